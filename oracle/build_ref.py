@@ -1,0 +1,194 @@
+"""Build recipe for the reference interpreter used as the CPU oracle.
+
+Compiles the reference's own C++ sources (the same object lists its per-directory
+Makefiles name, e.g. runtime/Makefile, interp/Makefile) where they lie under the
+reference checkout, with g++ -O2 as Makefile.common:5-6 does, against the
+declaration-only OpenCL header in oracle/clshim and the failing stubs in
+oracle/clstub.c.  The OpenCL back end therefore finds no platform and every
+trace runs on the reference's CPU interpreter device.
+
+Outputs go only to oracle/_ref/ (git-ignored):
+  oracle/_ref/libchai_ref.so   the reference library (interpreter path)
+  oracle/_ref/include/chai/    symlinks to the reference's public headers
+  oracle/_ref/ref_driver       the trace driver built from oracle/ref_driver.cpp
+  oracle/_ref/libr123_jit.so   the Random123 bijections exactly as the reference
+                               JIT prints them (oracle/r123_gen.cpp), as C++
+  oracle/_ref/libr123_upstream.so  the vendored upstream Random123 OpenCL text
+                               (Random123/r123*.i) compiled as C++
+
+Test infrastructure only: the product never links or runs anything built here.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import re
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+REF = Path(os.environ.get("CHAI_REFERENCE", "/root/reference"))
+
+# Directory order of the reference's top-level Makefile `all` target
+# (Makefile:3-24), minus tools_ (CLI programs) and with vendor built from
+# Makefile.NVIDIA's object list.
+DIRS = ["misc", "Random123", "vendor", "autotune", "kernel", "bytecode", "common",
+        "memmgr", "interp", "jitast", "jitbc", "jitstmt", "jitkrnl", "enqueue",
+        "runtime", "api", "applib"]
+PUBLIC_HEADERS = {"chai.h": "api", "BC.hpp": "bytecode", "RefCnt.hpp": "bytecode",
+                  "Stak.hpp": "bytecode", "Visit.hpp": "bytecode"}
+
+
+def _objects(d: Path) -> list[str]:
+    mk = d / ("Makefile.NVIDIA" if d.name == "vendor" else "Makefile")
+    text = mk.read_text()
+    m = re.search(r"LIBRARY_OBJECT_CODE\s*=\s*((?:.*\\\n)*.*)", text)
+    if not m:
+        return []
+    names = re.findall(r"([A-Za-z0-9_]+)\.o", m.group(1))
+    return [n + ".cpp" for n in names]
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("command failed: %s\n%s" % (" ".join(cmd), r.stderr[-4000:]))
+
+
+def available() -> bool:
+    return (REF / "api" / "chai.h").exists()
+
+
+def build(force: bool = False) -> Path:
+    """Compile the reference interpreter library and the trace driver."""
+    if not available():
+        raise FileNotFoundError("reference sources not found at %s" % REF)
+    lib = OUT / "libchai_ref.so"
+    drv = OUT / "ref_driver"
+    drv_src = HERE / "ref_driver.cpp"
+    if not force and lib.exists() and drv.exists() and drv.stat().st_mtime >= drv_src.stat().st_mtime:
+        return OUT
+    objdir = OUT / "obj"
+    objdir.mkdir(parents=True, exist_ok=True)
+    inc = OUT / "include" / "chai"
+    inc.mkdir(parents=True, exist_ok=True)
+    for name, d in PUBLIC_HEADERS.items():
+        link = inc / name
+        if link.is_symlink() or link.exists():
+            link.unlink()
+        link.symlink_to(REF / d / name)
+    incs = ["-I" + str(HERE / "clshim"), "-I" + str(OUT / "include")]
+    incs += ["-I" + str(REF / d) for d in DIRS]
+    flags = ["-O2", "-fPIC", "-fopenmp", "-w", "-std=gnu++98", "-include", "cstddef",
+             "-D_VENDOR_IS_NVIDIA_", "-D__STDC_LIMIT_MACROS"]
+    jobs = []
+    for d in DIRS:
+        for src in _objects(REF / d):
+            obj = objdir / (d + "__" + src.replace(".cpp", ".o"))
+            if force or not obj.exists():
+                jobs.append(["g++", "-c", *flags, *incs, str(REF / d / src), "-o", str(obj)])
+            else:
+                pass
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        list(ex.map(_run, jobs))
+    stub = objdir / "clstub.o"
+    _run(["gcc", "-c", "-O2", "-fPIC", "-I" + str(HERE / "clshim"), str(HERE / "clstub.c"), "-o", str(stub)])
+    objs = sorted(str(p) for p in objdir.glob("*.o"))
+    _run(["g++", "-shared", "-fopenmp", "-o", str(lib), *objs, "-lpthread"])
+    _run(["g++", "-O2", "-fopenmp", "-std=gnu++11", "-I" + str(OUT / "include"), str(drv_src),
+          "-o", str(drv), "-L" + str(OUT), "-lchai_ref", "-Wl,-rpath,$ORIGIN", "-lpthread"])
+    return OUT
+
+
+# C++ spellings of the OpenCL built-ins the Random123 text uses.
+_R123_PRELUDE = """#include <stdint.h>
+typedef uint64_t ulong;
+static inline uint64_t mul_hi(uint64_t a, uint64_t b)
+{ return (uint64_t)(((unsigned __int128)a * (unsigned __int128)b) >> 64); }
+"""
+
+# extern "C" entry points over the generated / upstream generator functions.
+_R123_EXPORTS = """
+extern "C" {
+#define EXP2(NAME, W, KW) void PFX_##NAME(const W* c, const W* k, W* o) { \\
+    NAME##_ctr_t C; NAME##_key_t K; for (int i = 0; i < 2; i++) C.v[i] = c[i]; \\
+    for (int i = 0; i < KW; i++) K.v[i] = k[i]; NAME##_ctr_t R = NAME##_R(NAME##_rounds, C, K); \\
+    for (int i = 0; i < 2; i++) o[i] = R.v[i]; }
+#define EXP4(NAME, W, KW) void PFX_##NAME(const W* c, const W* k, W* o) { \\
+    NAME##_ctr_t C; NAME##_key_t K; for (int i = 0; i < 4; i++) C.v[i] = c[i]; \\
+    for (int i = 0; i < KW; i++) K.v[i] = k[i]; NAME##_ctr_t R = NAME##_R(NAME##_rounds, C, K); \\
+    for (int i = 0; i < 4; i++) o[i] = R.v[i]; }
+EXP2(philox2x32, uint32_t, 1)
+EXP4(philox4x32, uint32_t, 2)
+EXP2(philox2x64, uint64_t, 1)
+EXP2(threefry2x32, uint32_t, 2)
+EXP4(threefry4x32, uint32_t, 4)
+EXP2(threefry2x64, uint64_t, 2)
+}
+"""
+
+
+def _strip_wrappers(text: str) -> str:
+    """Keep the bijections of the JIT's Random123 text: drop the OpenCL
+    integer typedefs and the *_uniform_* / *_normal_* wrappers, which use
+    OpenCL vector types (R123Philox.cpp:288-523, R123Threefry.cpp:289-535)."""
+    out, skipping = [], False
+    wrapper = re.compile(r"^inline \S+ (philox|threefry)_(uniform|normal)_\d+_\d+\(")
+    for line in text.splitlines():
+        if skipping:
+            if line.strip() == "}":
+                skipping = False
+            continue
+        if line.startswith("typedef ulong") or line.startswith("typedef uint ") or \
+                line.startswith("typedef uchar"):
+            continue
+        if wrapper.match(line):
+            if line.rstrip().endswith("{"):
+                skipping = True
+            continue
+        out.append(line)
+    return "\n".join(out) + "\n"
+
+
+def build_r123_pins(force: bool = False) -> None:
+    """Compile the reference JIT's generated Random123 text and the vendored
+    upstream Random123 OpenCL text as C++ libraries (oracle/_ref)."""
+    jit_so, up_so = OUT / "libr123_jit.so", OUT / "libr123_upstream.so"
+    if not force and jit_so.exists() and up_so.exists():
+        return
+    gen = OUT / "r123_gen"
+    _run(["g++", "-O1", "-std=gnu++98", "-include", "cstddef", "-I" + str(REF / "Random123"),
+          "-I" + str(REF / "misc"), str(HERE / "r123_gen.cpp"), "-o", str(gen), "-L" + str(OUT),
+          "-lchai_ref", "-Wl,-rpath,$ORIGIN", "-fopenmp"])
+    text = subprocess.run([str(gen)], capture_output=True, text=True, check=True).stdout
+    (OUT / "r123_jit.cl").write_text(text)
+    src = _R123_PRELUDE + _strip_wrappers(text) + _R123_EXPORTS.replace("PFX_", "jit_")
+    (OUT / "r123_jit.cpp").write_text(src)
+    _run(["g++", "-O2", "-fPIC", "-shared", "-w", str(OUT / "r123_jit.cpp"), "-o", str(jit_so)])
+    up = OUT / "r123_upstream.cpp"
+    up.write_text(_R123_PRELUDE + "\n".join(
+        '#include "%s"' % (REF / "Random123" / n) for n in ("r123array.i", "r123philox.i", "r123threefry.i"))
+        + "\n" + _R123_EXPORTS.replace("PFX_", "up_"))
+    _run(["g++", "-O2", "-fPIC", "-shared", "-w", str(up), "-o", str(up_so)])
+
+
+def build_oracle() -> Path:
+    """Compile the oracle's own C restatement (always possible; no reference
+    sources needed) into oracle/_build/liboracle.so."""
+    bdir = HERE / "_build"
+    bdir.mkdir(exist_ok=True)
+    so = bdir / "liboracle.so"
+    srcs = [HERE / "r123.c", HERE / "ops.c"]
+    if not so.exists() or any(s.stat().st_mtime > so.stat().st_mtime for s in srcs):
+        _run(["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-std=gnu11", *map(str, srcs),
+              "-o", str(so), "-lm"])
+    return so
+
+
+if __name__ == "__main__":
+    build_oracle()
+    build(force="--force" in sys.argv)
+    build_r123_pins(force="--force" in sys.argv)
+    print(OUT)
