@@ -1,0 +1,80 @@
+// Hand-written template pieces of the fused trace kernel ("ID space" kernel,
+// the B200 counterpart of enqueue/EnqueueIdSpace.cpp:19-359).  The trace
+// translator (trace.cpp) emits one __global__ function per kernel group whose
+// body is built from these pieces:
+//   - a grid-stride loop in which each thread owns a chunk of 4 consecutive
+//     elements of one slot (128-bit ld.global.v4 / st.global.v4 for 32-bit
+//     arrays, two 128-bit accesses for f64), grid.y = slot;
+//   - register-resident Random123 calls (chai_rng.cuh), one generator call per
+//     chunk when the row width is a multiple of the vector length;
+//   - per-thread double accumulators for sum / mean / dot_product, reduced by
+//     warp shuffles and a shared-memory block tree; each block writes one
+//     partial per reduction and slot, and chai_combine_partials (reduce.cu)
+//     adds the partials in a fixed order in FP64, so results are
+//     deterministic and the final combine is FP64 for any length.
+// Embedded verbatim into every runtime-compiled trace kernel.
+#pragma once
+#ifndef CHAI_TRACE_PRELUDE_CUH
+#define CHAI_TRACE_PRELUDE_CUH
+
+namespace chai_k {
+
+typedef unsigned int u32;
+typedef long long i64;
+
+template <class T> struct V4 { T v[4]; };
+
+// 4 consecutive elements at p (16-byte aligned for 32-bit types).
+template <class T> __device__ __forceinline__ void ld4(const T* __restrict__ p, T (&o)[4])
+{
+    if constexpr (sizeof(T) == 4) {
+        const uint4 r = __ldg(reinterpret_cast<const uint4*>(p));
+        o[0] = __builtin_bit_cast(T, r.x); o[1] = __builtin_bit_cast(T, r.y);
+        o[2] = __builtin_bit_cast(T, r.z); o[3] = __builtin_bit_cast(T, r.w);
+    } else {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        o[0] = (T)a.x; o[1] = (T)a.y; o[2] = (T)b.x; o[3] = (T)b.y;
+    }
+}
+
+template <class T> __device__ __forceinline__ void st4(T* __restrict__ p, const T (&v)[4])
+{
+    if constexpr (sizeof(T) == 4) {
+        uint4 r;
+        r.x = __builtin_bit_cast(unsigned, v[0]); r.y = __builtin_bit_cast(unsigned, v[1]);
+        r.z = __builtin_bit_cast(unsigned, v[2]); r.w = __builtin_bit_cast(unsigned, v[3]);
+        *reinterpret_cast<uint4*>(p) = r;
+    } else {
+        reinterpret_cast<double2*>(p)[0] = make_double2((double)v[0], (double)v[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2((double)v[2], (double)v[3]);
+    }
+}
+
+// Block-wide sum of NRED doubles; thread 0 receives the totals.
+template <int NRED, int NT>
+__device__ __forceinline__ void block_sum(double (&v)[NRED])
+{
+    __shared__ double red_smem[NRED][NT / 32];
+#pragma unroll
+    for (int r = 0; r < NRED; r++) {
+        double x = v[r];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0) red_smem[r][threadIdx.x >> 5] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int r = 0; r < NRED; r++) {
+            double x = threadIdx.x < NT / 32 ? red_smem[r][threadIdx.x] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            v[r] = x;
+        }
+    }
+}
+
+}  // namespace chai_k
+
+#endif

@@ -1,0 +1,177 @@
+// GEMV (autotune/EvergreenMatmulMV.cpp; oracle interp/InterpMatmulBase.hpp:
+// 37-47) as an HBM-bound kernel, and the transpose used by `transpose()`.
+//
+//   y = alpha * A x + beta * y    (A m x n row-major): one warp per row,
+//       128-bit loads of A unrolled 4 deep, x through the read-only L1 path,
+//       FP64 accumulation for f64 and FP32 for f32, warp-shuffle row sum.
+//   y = alpha * A^T x + beta * y: each thread owns 4 (f32) / 2 (f64) adjacent
+//       columns; the rows are split over blockIdx.y and the per-split column
+//       partials (context scratch) are summed in split order by a second
+//       kernel, so the result does not depend on scheduling.
+// Algorithmic bytes per launch: m*n*sizeof(T) + (m+n)*sizeof(T) (+ y read
+// when beta != 0).
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace chai {
+
+template <class T>
+__global__ void __launch_bounds__(256) chai_gemv_n(const T* __restrict__ A, long long lda, const T* __restrict__ x,
+                                                   T* __restrict__ y, long long m, long long n, T alpha, T beta)
+{
+    typedef typename std::conditional<sizeof(T) == 4, float4, double2>::type V;
+    constexpr int VE = 16 / sizeof(T);
+    const int lane = threadIdx.x & 31;
+    const long long row = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (row >= m) return;
+    const T* a = A + row * lda;
+    T acc = 0;
+    const bool vec = ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(x)) & 15) == 0;
+    long long done = 0;
+    if (vec) {
+        const long long nv = n / VE;
+        const V* av = reinterpret_cast<const V*>(a);
+        const V* xv = reinterpret_cast<const V*>(x);
+        long long v = lane;
+        for (; v + 96 < nv; v += 128) {
+            V a0 = __ldg(av + v), a1 = __ldg(av + v + 32), a2 = __ldg(av + v + 64), a3 = __ldg(av + v + 96);
+            V x0 = __ldg(xv + v), x1 = __ldg(xv + v + 32), x2 = __ldg(xv + v + 64), x3 = __ldg(xv + v + 96);
+            const T* pa[4] = {reinterpret_cast<const T*>(&a0), reinterpret_cast<const T*>(&a1),
+                              reinterpret_cast<const T*>(&a2), reinterpret_cast<const T*>(&a3)};
+            const T* px[4] = {reinterpret_cast<const T*>(&x0), reinterpret_cast<const T*>(&x1),
+                              reinterpret_cast<const T*>(&x2), reinterpret_cast<const T*>(&x3)};
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int j = 0; j < VE; j++) acc = fma(pa[u][j], px[u][j], acc);
+        }
+        for (; v < nv; v += 32) {
+            V a0 = __ldg(av + v), x0 = __ldg(xv + v);
+            const T* pa = reinterpret_cast<const T*>(&a0);
+            const T* px = reinterpret_cast<const T*>(&x0);
+#pragma unroll
+            for (int j = 0; j < VE; j++) acc = fma(pa[j], px[j], acc);
+        }
+        done = nv * VE;
+    }
+    for (long long j = done + lane; j < n; j += 32) acc = fma(__ldg(a + j), __ldg(x + j), acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) y[row] = beta == (T)0 ? alpha * acc : alpha * acc + beta * y[row];
+}
+
+// partial[s][j] = sum over rows of split s of x[i] * A[i][j]
+template <class T>
+__global__ void __launch_bounds__(256) chai_gemv_t_partial(const T* __restrict__ A, long long lda,
+                                                           const T* __restrict__ x, T* __restrict__ partial,
+                                                           long long m, long long n, long long rows_per_split)
+{
+    constexpr int VE = 16 / sizeof(T);
+    const long long j0 = ((long long)blockIdx.x * 256 + threadIdx.x) * VE;
+    if (j0 >= n) return;
+    const long long r0 = (long long)blockIdx.y * rows_per_split;
+    const long long r1 = r0 + rows_per_split < m ? r0 + rows_per_split : m;
+    T acc[VE];
+#pragma unroll
+    for (int j = 0; j < VE; j++) acc[j] = 0;
+    const bool full = j0 + VE <= n && ((lda * sizeof(T)) % 16 == 0) && ((reinterpret_cast<uintptr_t>(A) & 15) == 0);
+    for (long long i = r0; i < r1; i++) {
+        const T xi = __ldg(x + i);
+        const T* a = A + i * lda + j0;
+        if (full) {
+            typedef typename std::conditional<sizeof(T) == 4, float4, double2>::type V;
+            V av = __ldg(reinterpret_cast<const V*>(a));
+            const T* pa = reinterpret_cast<const T*>(&av);
+#pragma unroll
+            for (int j = 0; j < VE; j++) acc[j] = fma(pa[j], xi, acc[j]);
+        } else {
+            for (int j = 0; j < VE && j0 + j < n; j++) acc[j] = fma(__ldg(a + j), xi, acc[j]);
+        }
+    }
+    T* p = partial + (long long)blockIdx.y * n + j0;
+    for (int j = 0; j < VE && j0 + j < n; j++) p[j] = acc[j];
+}
+
+template <class T>
+__global__ void chai_gemv_t_finish(const T* __restrict__ partial, int splits, T* __restrict__ y, long long n,
+                                   T alpha, T beta)
+{
+    const long long j = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (j >= n) return;
+    T acc = 0;
+    for (int s = 0; s < splits; s++) acc += partial[(long long)s * n + j];
+    y[j] = beta == (T)0 ? alpha * acc : alpha * acc + beta * y[j];
+}
+
+template <class T>
+static int gemv_t(chai_cuda_ctx* ctx, int trans, int64_t m, int64_t n, double alpha, const void* a, int64_t lda,
+                  const void* x, double beta, void* y)
+{
+    if (!trans) {
+        const unsigned blocks = (unsigned)((m + 7) / 8);
+        if (blocks) chai_gemv_n<T><<<blocks, 256, 0, ctx->stream>>>((const T*)a, lda, (const T*)x, (T*)y, m, n,
+                                                                    (T)alpha, (T)beta);
+        CHAI_CUDA_TRY(ctx, cudaGetLastError());
+        return CHAI_OK;
+    }
+    constexpr int VE = 16 / sizeof(T);
+    const long long colblocks = (n + 256 * VE - 1) / (256 * VE);
+    long long splits = std::max<long long>(1, (long long)ctx->sm_count * 6 / std::max<long long>(1, colblocks));
+    splits = std::min<long long>(splits, std::max<long long>(1, m / 16));
+    const long long rps = (m + splits - 1) / splits;
+    splits = (m + rps - 1) / rps;
+    if (splits < 1) splits = 1;
+    int st = ensure_scratch(ctx, (size_t)splits * n * sizeof(T));
+    if (st) return st;
+    T* partial = static_cast<T*>(ctx->scratch);
+    if (m > 0 && n > 0) {
+        chai_gemv_t_partial<T><<<dim3((unsigned)colblocks, (unsigned)splits), 256, 0, ctx->stream>>>(
+            (const T*)a, lda, (const T*)x, partial, m, n, rps);
+        chai_gemv_t_finish<T><<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(partial, (int)splits, (T*)y, n,
+                                                                                     (T)alpha, (T)beta);
+    }
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    return CHAI_OK;
+}
+
+int launch_gemv(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha, const void* a,
+                int64_t lda, const void* x, double beta, void* y)
+{
+    if (prec == CHAI_F32) return gemv_t<float>(ctx, trans, m, n, alpha, a, lda, x, beta, y);
+    if (prec == CHAI_F64) return gemv_t<double>(ctx, trans, m, n, alpha, a, lda, x, beta, y);
+    return set_error(ctx, CHAI_ERR_UNSUPPORTED, "gemv precision");
+}
+
+// 32x32 tiled transpose through shared memory, per slot.
+template <class T>
+__global__ void chai_transpose(const T* __restrict__ in, T* __restrict__ out, long long w, long long h)
+{
+    __shared__ T tile[32][33];
+    const long long s = blockIdx.z;
+    in += s * w * h;
+    out += s * w * h;
+    const long long x = (long long)blockIdx.x * 32 + threadIdx.x;
+    for (int k = threadIdx.y; k < 32; k += 8) {
+        const long long y = (long long)blockIdx.y * 32 + k;
+        if (x < w && y < h) tile[k][threadIdx.x] = in[y * w + x];
+    }
+    __syncthreads();
+    const long long ox = (long long)blockIdx.y * 32 + threadIdx.x;
+    for (int k = threadIdx.y; k < 32; k += 8) {
+        const long long oy = (long long)blockIdx.x * 32 + k;
+        if (ox < h && oy < w) out[oy * h + ox] = tile[threadIdx.x][k];
+    }
+}
+
+int launch_transpose(chai_cuda_ctx* ctx, uint32_t prec, const void* in, void* out, int64_t w, int64_t h,
+                     int64_t slots)
+{
+    dim3 grid((unsigned)((w + 31) / 32), (unsigned)((h + 31) / 32), (unsigned)slots);
+    if (prec_bytes(prec) == 8) chai_transpose<double><<<grid, dim3(32, 8), 0, ctx->stream>>>((const double*)in, (double*)out, w, h);
+    else chai_transpose<float><<<grid, dim3(32, 8), 0, ctx->stream>>>((const float*)in, (float*)out, w, h);
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    return CHAI_OK;
+}
+
+}  // namespace chai

@@ -1,0 +1,86 @@
+// Internal state of a chai_b200 context (host side, C++17).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "chai_b200.h"
+
+namespace chai {
+
+struct Buffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    bool owned = true;
+};
+
+struct Config {
+    int gemm_precision = CHAI_GEMM_FP32;     // f32 matmul arithmetic
+    double rng_pi = 3.14159;                 // M_PI as the reference JIT prints it
+    int rng_layout = 0;                      // 0 chai, 1 counter
+    int tuner_mode = CHAI_TUNE_LEARNED;
+    std::string tune_db;
+    std::string jit_cache;
+};
+
+class Jit;      // runtime compilation cache (jit.cpp)
+class Tuner;    // learned / exhaustive GEMM tuner (tuner.cpp)
+
+}  // namespace chai
+
+struct chai_cuda_ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::mutex mem_mutex;                                   // buffer table
+    std::unordered_map<uint64_t, chai::Buffer> buffers;
+    std::mutex err_mutex;
+    std::string last_error;
+    chai::Config cfg;
+    // scratch for reduction partials and split-precision GEMM operands
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    double* pinned = nullptr;                               // pinned host results
+    size_t pinned_count = 0;
+    int* status_word = nullptr;                             // device error word for bounded waits
+    std::unique_ptr<chai::Jit> jit;
+    std::unique_ptr<chai::Tuner> tuner;
+    uint64_t next_temp_id = 1ull << 62;                     // ids of library-owned temporaries
+};
+
+namespace chai {
+
+int set_error(chai_cuda_ctx* ctx, int status, const std::string& msg);
+int cuda_status(chai_cuda_ctx* ctx, cudaError_t e, const char* what);
+// Grow the context scratch to at least `bytes` (stream-ordered).
+int ensure_scratch(chai_cuda_ctx* ctx, size_t bytes);
+Buffer* find_buffer(chai_cuda_ctx* ctx, uint64_t id);
+int alloc_buffer(chai_cuda_ctx* ctx, uint64_t id, size_t bytes);
+bool fault_injected(const char* site);
+
+size_t prec_bytes(uint32_t prec);
+
+// kernels with host launchers (each .cu file)
+int launch_rng_fill(chai_cuda_ctx* ctx, const chai_rng_desc* d, void* out);
+int launch_reduce(chai_cuda_ctx* ctx, uint32_t op, uint32_t prec, const void* a, const void* b, uint64_t n,
+                  uint32_t slots, double* dev_out);
+int launch_gemv(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha,
+                const void* a, int64_t lda, const void* x, double beta, void* y);
+int launch_gemm(chai_cuda_ctx* ctx, const chai_gemm_desc* d);
+int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_problem* p, int32_t count);
+
+}  // namespace chai
+
+#define CHAI_CUDA_TRY(ctx, expr)                                              \
+    do {                                                                      \
+        cudaError_t _e = (expr);                                              \
+        if (_e != cudaSuccess) return chai::cuda_status((ctx), _e, #expr);    \
+    } while (0)

@@ -1,0 +1,133 @@
+// Reductions: sum / mean / dot_product (enqueue/EnqueueReduce.cpp:21-222 runs
+// one serial work item per array; interp/InterpAccum.cpp:13-70 and
+// interp/InterpDotprod.cpp accumulate in double).
+//
+// Combine order, stated: each thread accumulates its grid-stride elements in
+// FP64, a warp-shuffle tree and a shared-memory tree reduce each block to one
+// partial, and chai_combine_partials adds a slot's partials in FP64 with a
+// fixed block-tree order.  The grid size is a function of the array size and
+// the SM count only, so a result is bit-reproducible on a given GPU model.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace chai {
+
+template <int NT>
+__device__ __forceinline__ double block_sum_d(double x)
+{
+    __shared__ double sm[NT / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = x;
+    __syncthreads();
+    x = threadIdx.x < NT / 32 ? sm[threadIdx.x] : 0.0;
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    }
+    return x;
+}
+
+struct CombineArgs {
+    void* outs[16];
+    int precs[16];
+    double scales[16];
+};
+
+// grid: (slots, nred); one block sums one (reduction, slot) row of partials
+__global__ void __launch_bounds__(256) chai_combine_partials(const double* __restrict__ partials, int nblocks,
+                                                             int slots, CombineArgs a)
+{
+    const int slot = blockIdx.x, r = blockIdx.y;
+    const double* p = partials + ((long long)r * slots + slot) * nblocks;
+    double x = 0.0;
+    for (int i = threadIdx.x; i < nblocks; i += 256) x += p[i];
+    x = block_sum_d<256>(x);
+    if (threadIdx.x == 0) {
+        x *= a.scales[r];
+        switch (a.precs[r]) {
+            case CHAI_F32: static_cast<float*>(a.outs[r])[slot] = (float)x; break;
+            case CHAI_F64: static_cast<double*>(a.outs[r])[slot] = x; break;
+            case CHAI_I32: static_cast<int*>(a.outs[r])[slot] = (int)(long long)x; break;
+            case CHAI_U32: static_cast<unsigned*>(a.outs[r])[slot] = (unsigned)(long long)x; break;
+        }
+    }
+}
+
+int launch_combine(chai_cuda_ctx* ctx, const double* partials, int nblocks, int nred, int slots,
+                   void* const* outs, const int* precs, const double* scales)
+{
+    if (nred > 16) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "more than 16 reductions in one kernel");
+    CombineArgs a;
+    for (int r = 0; r < nred; r++) {
+        a.outs[r] = outs[r];
+        a.precs[r] = precs[r];
+        a.scales[r] = scales[r];
+    }
+    chai_combine_partials<<<dim3(slots, nred), 256, 0, ctx->stream>>>(partials, nblocks, slots, a);
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    return CHAI_OK;
+}
+
+// Per-slot partial sums of a (op 0/1) or a*b (op 2); T is the array type.
+template <class T, bool DOT>
+__global__ void __launch_bounds__(256) chai_reduce_partials(const T* __restrict__ a, const T* __restrict__ b,
+                                                            unsigned long long n, double* __restrict__ partials)
+{
+    const int slot = blockIdx.y;
+    const T* pa = a + (unsigned long long)slot * n;
+    const T* pb = DOT ? b + (unsigned long long)slot * n : nullptr;
+    double acc = 0.0;
+    const unsigned long long stride = (unsigned long long)gridDim.x * 256;
+    // 16-byte vector loads when the slot base is aligned
+    const bool vec = ((reinterpret_cast<uintptr_t>(pa) | (DOT ? reinterpret_cast<uintptr_t>(pb) : 0)) & 15) == 0;
+    constexpr int VE = 16 / sizeof(T);
+    unsigned long long done = 0;
+    if (vec) {
+        const unsigned long long nv = n / VE;
+        for (unsigned long long v = blockIdx.x * 256ull + threadIdx.x; v < nv; v += stride) {
+            T x[VE], y[VE];
+            *reinterpret_cast<uint4*>(x) = __ldg(reinterpret_cast<const uint4*>(pa) + v);
+            if (DOT) *reinterpret_cast<uint4*>(y) = __ldg(reinterpret_cast<const uint4*>(pb) + v);
+#pragma unroll
+            for (int j = 0; j < VE; j++) acc += DOT ? (double)(x[j] * y[j]) : (double)x[j];
+        }
+        done = nv * VE;
+    }
+    for (unsigned long long i = done + blockIdx.x * 256ull + threadIdx.x; i < n; i += stride)
+        acc += DOT ? (double)(pa[i] * pb[i]) : (double)pa[i];
+    acc = block_sum_d<256>(acc);
+    if (threadIdx.x == 0) partials[(unsigned long long)slot * gridDim.x + blockIdx.x] = acc;
+}
+
+int launch_reduce(chai_cuda_ctx* ctx, uint32_t op, uint32_t prec, const void* a, const void* b, uint64_t n,
+                  uint32_t slots, double* dev_out)
+{
+    const size_t eb = prec_bytes(prec);
+    if (!eb) return set_error(ctx, CHAI_ERR_INVALID, "reduce precision");
+    const unsigned long long nv = (n * eb + 15) / 16;
+    unsigned gx = (unsigned)std::max<unsigned long long>(1, std::min<unsigned long long>((nv + 255) / 256,
+                                                         (unsigned long long)ctx->sm_count * 8 / slots + 1));
+    int st = ensure_scratch(ctx, (size_t)gx * slots * sizeof(double));
+    if (st) return st;
+    double* partials = static_cast<double*>(ctx->scratch);
+    dim3 grid(gx, slots);
+    const bool dot = op == 2;
+#define R(T) (dot ? chai_reduce_partials<T, true><<<grid, 256, 0, ctx->stream>>>((const T*)a, (const T*)b, n, partials) \
+                  : chai_reduce_partials<T, false><<<grid, 256, 0, ctx->stream>>>((const T*)a, (const T*)b, n, partials))
+    switch (prec) {
+        case CHAI_F32: R(float); break;
+        case CHAI_F64: R(double); break;
+        case CHAI_I32: R(int); break;
+        case CHAI_U32: R(unsigned); break;
+    }
+#undef R
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    void* outs[1] = {dev_out};
+    int precs[1] = {CHAI_F64};
+    double scales[1] = {op == 1 ? 1.0 / (double)n : 1.0};
+    return launch_combine(ctx, partials, (int)gx, 1, (int)slots, outs, precs, scales);
+}
+
+}  // namespace chai

@@ -1,0 +1,59 @@
+// Entry points whose specialised kernels live in later files of this build.
+#include "internal.h"
+#include "tuner.h"
+
+namespace chai {
+
+int launch_gemm_tc(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision)
+{
+    (void)d; (void)precision;
+    return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tensor-core gemm not built");
+}
+
+int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_problem* p, int32_t count)
+{
+    (void)precision; (void)p; (void)count;
+    return set_error(ctx, CHAI_ERR_UNSUPPORTED, "grouped gemm not built");
+}
+
+int Tuner::tune(const chai_gemm_key* key, int mode, chai_gemm_cfg* out)
+{
+    (void)key; (void)mode; (void)out;
+    return CHAI_ERR_UNSUPPORTED;
+}
+int Tuner::load(const std::string& path) { (void)path; return CHAI_OK; }
+int Tuner::save(const std::string& path) const { (void)path; return CHAI_OK; }
+bool Tuner::lookup(const chai_gemm_key* key, chai_gemm_cfg* out) const { (void)key; (void)out; return false; }
+
+}  // namespace chai
+
+using namespace chai;
+
+extern "C" {
+
+int chai_cuda_evaluate_many(chai_cuda_ctx* ctx, const chai_trace_desc* const* traces, size_t n, double* results)
+{
+    (void)traces; (void)n; (void)results;
+    if (!ctx) return CHAI_ERR_INVALID;
+    return set_error(ctx, CHAI_ERR_UNSUPPORTED, "evaluate_many not built");
+}
+
+int chai_cuda_tune(chai_cuda_ctx* ctx, const chai_gemm_key* key, int mode, chai_gemm_cfg* out)
+{
+    if (!ctx || !key || !out) return CHAI_ERR_INVALID;
+    return ctx->tuner->tune(key, mode, out);
+}
+
+int chai_cuda_tune_db_load(chai_cuda_ctx* ctx, const char* path)
+{
+    if (!ctx || !path) return CHAI_ERR_INVALID;
+    return ctx->tuner->load(path);
+}
+
+int chai_cuda_tune_db_save(chai_cuda_ctx* ctx, const char* path)
+{
+    if (!ctx || !path) return CHAI_ERR_INVALID;
+    return ctx->tuner->save(path);
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+// Trace translator internals (see trace.cpp).
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "chai_b200.h"
+
+struct chai_cuda_ctx;
+
+namespace chai {
+
+struct Node {
+    enum Kind { VAR, INPUT, SCALAR, OP, CONVERT, RNG, INDEX, FILL, MAKE, READ, MATMUL, MATMULG, TRANSPOSE,
+                REDUCE, GATHER } kind = OP;
+    uint32_t op = 0;
+    int prec = CHAI_F32;
+    uint64_t W = 1, H = 1;
+    uint32_t slots = 1;
+    std::vector<int> kids;
+    double scalar = 0;
+    uint32_t var = 0, ver = 0;
+    uint64_t buffer = 0;            // MAKE / READ / INPUT buffer id
+    int read_kind = 0;              // 0 read_scalar, 1 read1, 2 read2
+    // RNG
+    uint32_t variant = CHAI_RNG_PHILOX, dist = 0;
+    uint64_t seed = 0;
+    bool limits = false;
+    double lo = 0, hi = 1;
+    // INDEX
+    int dim = 0;
+    // MATMULG
+    double alpha = 1, beta = 0;
+    // storage when materialised
+    void* dev = nullptr;
+    uint64_t storage_buffer = 0;
+};
+
+class Translator {
+public:
+    // dry: plan and compile every kernel, allocate and launch nothing
+    explicit Translator(chai_cuda_ctx* ctx, bool dry = false) : ctx_(ctx), dry_(dry) {}
+    ~Translator();
+    int run(const chai_trace_desc* t, const chai_buffer_binding* b, size_t nb);
+    // scalar results of reductions that are statement roots (for evaluate_many)
+    const std::vector<Node>& nodes() const { return nodes_; }
+    // generated source of the last element kernel (diagnostics / tests)
+    std::string last_source;
+    std::string all_sources;
+    size_t kernels_launched = 0;
+
+private:
+    chai_cuda_ctx* ctx_;
+    bool dry_ = false;
+    std::vector<Node> nodes_;
+    std::map<uint32_t, chai_buffer_binding> bindings_;
+    std::map<std::pair<uint32_t, uint32_t>, int> assigned_;
+    std::map<uint32_t, int> latest_;
+    std::map<uint32_t, int> inputs_;
+    std::map<std::string, int> cse_;
+    std::vector<std::pair<uint32_t, int>> stmt_roots_;
+    std::vector<int> reads_;
+    std::vector<bool> materialize_;
+    std::vector<void*> temps_;
+    uint32_t slots_ = 1;
+    uint32_t unsupported_op_ = 0;
+
+    int fail(int st, const std::string& msg);
+    int add(Node n);
+    double scalar_cell(const chai_stmt& s, int& pos, bool& ok);
+    int parse(const chai_stmt& s, int& pos);
+    int resolve_var(const Node& v);
+    size_t node_bytes(const Node& n) const;
+    int assign_storage(int i);
+    int schedule(const std::vector<int>& order);
+    int emit_group(const std::vector<int>& roots);
+    int emit_linalg(int i);
+    int do_read(int i);
+};
+
+}  // namespace chai

@@ -1,0 +1,250 @@
+/* chai_b200 -- C ABI of the B200 back end for chai traced array programs.
+ *
+ * This library replaces the reference's OpenCL "Translator" device: the code
+ * that turns a recorded trace (a VectorTrace of bytecode stacks) into kernels
+ * and runs them, together with the device memory manager and the GEMM
+ * autotuner it calls.  The host side that records traces (api/, bytecode/,
+ * common/, runtime/ Scheduler) stays the reference's; it reaches this library
+ * through a DeviceBase subclass whose sub_evaluate flattens the VectorTrace
+ * into a chai_trace_desc and calls chai_cuda_evaluate.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: 0 (CHAI_OK) or a negative
+ *     chai_status code.  No C++ exception crosses this boundary.  A non-zero
+ *     status maps to DeviceBase::evaluate() == false, which the reference's
+ *     scheduler turns into DEVICE_FAILURE and a fall back to another device
+ *     (runtime/Executor.cpp:15,56-59; runtime/Scheduler.cpp:221-252).
+ *   - Arrays are row-major: W is the number of columns, H the number of rows
+ *     (api/ArrayFun.cpp:74-90).  Vectorised traces stack `slots` arrays of
+ *     W x H elements back to back.
+ *   - Device buffers are owned by the context and named by a 64-bit id the
+ *     host chooses (the reference keys them by trace hash and variable,
+ *     memmgr/MemTrans.hpp:48-51).  Host memory stays the caller's.
+ *   - chai_cuda_evaluate is called from one thread per context (one CUDA
+ *     stream per context); readback / release may come from any thread
+ *     (memmgr/MemTrans.hpp:43-47 guards the same way with _memMutex).
+ *   - There is no CPU fallback inside this library: without a usable B200
+ *     every entry point that would compute returns CHAI_ERR_NO_DEVICE.
+ */
+#ifndef CHAI_B200_H
+#define CHAI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHAI_B200_ABI_VERSION 1
+
+typedef enum chai_status {
+    CHAI_OK = 0,
+    CHAI_ERR_INVALID = -1,      /* bad argument or malformed trace */
+    CHAI_ERR_UNSUPPORTED = -2,  /* opcode / shape / precision not handled */
+    CHAI_ERR_OOM = -3,          /* device allocation failed */
+    CHAI_ERR_LAUNCH = -4,       /* kernel launch or execution failed */
+    CHAI_ERR_TIMEOUT = -5,      /* a bounded device wait gave up (status word set) */
+    CHAI_ERR_NOT_FOUND = -6,    /* unknown buffer id */
+    CHAI_ERR_NO_DEVICE = -7,    /* no CUDA device / not an sm_100 part */
+    CHAI_ERR_JIT = -8,          /* runtime compilation of a trace kernel failed */
+    CHAI_ERR_INJECTED = -9      /* failure forced by CHAI_FAULT_INJECT (testing) */
+} chai_status;
+
+/* Precision codes, as misc/PrecType.hpp numbers them. */
+enum { CHAI_U32 = 0, CHAI_I32 = 1, CHAI_F32 = 4, CHAI_F64 = 8 };
+
+/* RNG variants, as api/chai.h:412-417 numbers them. */
+enum { CHAI_RNG_PHILOX = 1230, CHAI_RNG_THREEFRY = 1231 };
+
+typedef struct chai_cuda_ctx chai_cuda_ctx;
+
+/* ------------------------------------------------------------------ life */
+
+/* Replaces Translator::initDevice / DeviceBase::initDevice
+ * (runtime/DeviceBase.hpp:22-61, runtime/Translator.cpp:353-364).
+ * `config` is the text of a device spec (devspec.cfg keywords are accepted and
+ * ignored where meaningless on CUDA); recognised keys, one per line or
+ * space-separated, `Key=Value`:
+ *   GemmPrecision=fp32|tf32|bf16|bf16x3|bf16x6|fp8   f32 matmul arithmetic
+ *   RngPi=<double>        constant inside Box-Muller (default 3.14159, the
+ *                         value the reference JIT prints)
+ *   RngLayout=chai|counter   key/counter placement (default chai)
+ *   TunerMode=learned|exhaustive|off, TuneDB=<path>
+ *   JitCache=<dir>        on-disk cache of compiled trace kernels
+ * May be NULL. */
+int chai_cuda_init(int device, const char* config, chai_cuda_ctx** out);
+/* Clean shutdown: frees every buffer, module and stream (no ShutdownNOP). */
+int chai_cuda_shutdown(chai_cuda_ctx* ctx);
+int chai_cuda_synchronize(chai_cuda_ctx* ctx);
+const char* chai_cuda_error_string(int status);
+/* Human-readable detail of the last failure on this context. */
+const char* chai_cuda_last_error(chai_cuda_ctx* ctx);
+/* Run subsequent work on an external cudaStream_t (NULL = the context's own). */
+int chai_cuda_set_stream(chai_cuda_ctx* ctx, void* cuda_stream);
+
+/* ---------------------------------------------------------------- memory */
+
+/* Replace MemTrans::memalloc / MemCallback::swizzle / untrackMem
+ * (memmgr/MemTrans.hpp:31-235, common/MemCallback.hpp:13-21). */
+int chai_cuda_buffer_alloc(chai_cuda_ctx* ctx, uint64_t id, size_t bytes);
+/* Register caller-owned device memory under `id` (never freed by the library). */
+int chai_cuda_buffer_wrap(chai_cuda_ctx* ctx, uint64_t id, void* device_ptr, size_t bytes);
+int chai_cuda_buffer_info(chai_cuda_ctx* ctx, uint64_t id, void** device_ptr, size_t* bytes);
+/* Host -> device copy of `bytes` at offset 0; the host buffer may be pageable. */
+int chai_cuda_upload(chai_cuda_ctx* ctx, uint64_t id, const void* host, size_t bytes);
+/* Device -> host copy; waits for all work on the context that writes `id`. */
+int chai_cuda_readback(chai_cuda_ctx* ctx, uint64_t id, void* host, size_t bytes);
+int chai_cuda_release(chai_cuda_ctx* ctx, uint64_t id);
+
+/* ----------------------------------------------------------------- trace */
+
+/* One bytecode cell, mirroring chai_internal::BC (bytecode/BC.hpp:15-36). */
+enum { CHAI_BC_OPCODE = 0, CHAI_BC_VARIABLE = 1, CHAI_BC_SCALAR = 2, CHAI_BC_MEMORY = 3 };
+typedef struct chai_bc {
+    uint32_t kind;      /* CHAI_BC_* */
+    uint32_t code;      /* opcode (ByteCodes.hpp numbers) or variable number */
+    uint32_t version;   /* variable version */
+    uint32_t reserved;
+    double   scalar;    /* CHAI_BC_SCALAR payload */
+    uint64_t buffer;    /* CHAI_BC_MEMORY: buffer id standing for a FrontMem box */
+} chai_bc;
+
+/* One statement: the bytecode stack of an assignment, in push order (operands
+ * are pushed last-argument first, the opcode last: api/ArrayFun.cpp:44-52). */
+typedef struct chai_stmt {
+    uint32_t lhs_variable;
+    uint32_t lhs_version;
+    uint32_t n_cells;
+    uint32_t reserved;
+    const chai_bc* cells;
+} chai_stmt;
+
+/* A vectorised trace (common/VectorTrace.hpp:28-119). */
+typedef struct chai_trace_desc {
+    uint32_t num_traces;        /* slots: identical traces batched together */
+    uint32_t n_stmts;
+    const chai_stmt* stmts;
+    uint64_t hash;              /* front-end trace hash (0: computed here) */
+} chai_trace_desc;
+
+/* Variables that live outside the trace: inputs computed by earlier traces and
+ * outputs later traces or the host read (the reference's liveVariables and
+ * BackMem boxes, common/VectorTrace.hpp:33-76). */
+typedef struct chai_buffer_binding {
+    uint32_t variable;
+    uint32_t prec;              /* CHAI_U32 .. CHAI_F64 */
+    uint64_t width, height;
+    uint32_t slots;
+    uint32_t reserved;
+    uint64_t buffer;            /* buffer id holding slots*height*width elements */
+} chai_buffer_binding;
+
+/* Replaces Translator::sub_evaluate (runtime/Translator.cpp:366-411). */
+int chai_cuda_evaluate(chai_cuda_ctx* ctx, const chai_trace_desc* trace,
+                       const chai_buffer_binding* bindings, size_t n_bindings);
+
+/* Diagnostic counterpart of the reference's logged kernel source
+ * (kernel/KernelCache.cpp:82-89 prints generated OpenCL under --log): plans
+ * the trace, emits every fused element kernel as CUDA C and compiles each with
+ * NVRTC for sm_100a.  Needs no device; allocates and launches nothing.  The
+ * generated source (or the error text on failure) is copied to `out`
+ * (NUL-terminated, truncated to `cap`); `needed` receives its full size. */
+int chai_cuda_trace_source(const chai_trace_desc* trace, const chai_buffer_binding* bindings,
+                           size_t n_bindings, const char* config, char* out, size_t cap, size_t* needed);
+
+/* Many traces of uneven length in one persistent launch captured in a CUDA
+ * graph.  All traces share one bytecode program (same hash, different W/H);
+ * trace i reads/writes buffers bindings[i*n_per .. ]; scalar results land in
+ * results[i] (host memory).  Replaces the per-hash VectorTrace batching of
+ * runtime/Scheduler.cpp:48-89, which only batches equal shapes. */
+int chai_cuda_evaluate_many(chai_cuda_ctx* ctx, const chai_trace_desc* const* traces, size_t n_traces,
+                            double* results);
+
+/* --------------------------------------------------------- direct kernels */
+
+/* Chai random array fill (Random123/R123Philox.cpp:288-523 and
+ * R123Threefry.cpp:289-535 as called from kernel/Function.cpp:433-503). */
+typedef struct chai_rng_desc {
+    uint32_t variant;           /* CHAI_RNG_PHILOX / CHAI_RNG_THREEFRY */
+    uint32_t prec;              /* CHAI_U32, CHAI_I32, CHAI_F32, CHAI_F64 */
+    uint32_t dist;              /* 0 uniform, 1 normal */
+    uint32_t vec_len;           /* 4 (32-bit default), 2 (f64 default) or 1 */
+    uint64_t seed;              /* generator seed at the call (counter word 0) */
+    uint64_t width, height;
+    uint32_t slots;
+    uint32_t has_limits;        /* uniform f32/f64: u*(max-min)+min */
+    double   min_limit, max_limit;
+} chai_rng_desc;
+int chai_cuda_rng_fill(chai_cuda_ctx* ctx, const chai_rng_desc* d, void* device_out);
+
+/* GEMM C = alpha * op(A) op(B) + beta * C  (EnqueueMatmulAuto.cpp:21-404,
+ * autotune/EvergreenMatmulMM.cpp).  Row-major, lda/ldb/ldc in elements. */
+enum {
+    CHAI_GEMM_FP32 = 0,     /* CUDA-core FFMA, f32 accumulate */
+    CHAI_GEMM_TF32 = 1,     /* tcgen05 kind::tf32 */
+    CHAI_GEMM_BF16 = 2,     /* operands rounded to bf16, tcgen05 kind::f16 */
+    CHAI_GEMM_BF16X3 = 3,   /* fp32 split hi+lo bf16, 3 products */
+    CHAI_GEMM_BF16X6 = 4,   /* fp32 split hi+mid+lo bf16, 6 products */
+    CHAI_GEMM_FP8 = 5,      /* e4m3 with per-128x128-tile scales */
+    CHAI_GEMM_FP64 = 6,     /* f64 operands (Arrayd64), CUDA-core DFMA */
+    CHAI_GEMM_AUTO = 7      /* context default (GemmPrecision) */
+};
+typedef struct chai_gemm_desc {
+    int32_t  precision;         /* CHAI_GEMM_* */
+    int32_t  trans_a, trans_b;
+    int32_t  reserved;
+    int64_t  m, n, k;
+    const void* a; int64_t lda;
+    const void* b; int64_t ldb;
+    void*    c;    int64_t ldc;
+    double   alpha, beta;
+    int64_t  batch;             /* >= 1: strided batch (traces / slots) */
+    int64_t  stride_a, stride_b, stride_c;
+} chai_gemm_desc;
+int chai_cuda_gemm(chai_cuda_ctx* ctx, const chai_gemm_desc* d);
+
+/* y = alpha * op(A) x + beta * y, f32 or f64 (autotune/EvergreenMatmulMV.cpp). */
+int chai_cuda_gemv(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha,
+                   const void* a, int64_t lda, const void* x, double beta, void* y);
+
+/* Many independent f32 GEMMs of different shapes in one persistent
+ * tensor-core launch (C_i = A_i B_i, row-major, packed). */
+typedef struct chai_gemm_problem {
+    int32_t m, n, k, reserved;
+    const float* a; const float* b; float* c;
+} chai_gemm_problem;
+int chai_cuda_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_problem* problems,
+                           int32_t count);
+
+/* sum / mean / dot_product over `slots` arrays of n elements each
+ * (enqueue/EnqueueReduce.cpp:21-222; interp/InterpAccum.cpp:13-70).
+ * op: 0 sum, 1 mean, 2 dot_product (b used).  Results (one per slot) are
+ * written as doubles to host memory `out`. */
+int chai_cuda_reduce(chai_cuda_ctx* ctx, uint32_t op, uint32_t prec, const void* a, const void* b,
+                     uint64_t n, uint32_t slots, double* out);
+
+/* ------------------------------------------------------------------ tuner */
+
+/* Replace StandardEM / AutoTuneEM / AutoTuneBench (autotune/StandardEM.cpp:69-147,
+ * autotune/AutoTuneBench.cpp:17-251) and the journal (autotune/AutoTuneMemo.hpp). */
+typedef struct chai_gemm_key {
+    int64_t m, n, k;
+    int32_t precision;          /* CHAI_GEMM_* */
+    int32_t is_gemv;
+} chai_gemm_key;
+typedef struct chai_gemm_cfg {
+    int32_t block_m, block_n, block_k, stages;
+    int32_t vec_width, cluster_m, cluster_n, reserved;
+    double  measured_us;        /* timing of the chosen config (0 if not timed) */
+} chai_gemm_cfg;
+enum { CHAI_TUNE_LEARNED = 0, CHAI_TUNE_EXHAUSTIVE = 1 };
+int chai_cuda_tune(chai_cuda_ctx* ctx, const chai_gemm_key* key, int mode, chai_gemm_cfg* out);
+int chai_cuda_tune_db_load(chai_cuda_ctx* ctx, const char* path);
+int chai_cuda_tune_db_save(chai_cuda_ctx* ctx, const char* path);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
