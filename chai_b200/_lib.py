@@ -99,6 +99,7 @@ SIGNATURES = {
     "chai_cuda_gemm_grouped": (C.c_int, [P, C.c_int32, C.POINTER(chai_gemm_problem), C.c_int32]),
     "chai_cuda_reduce": (C.c_int, [P, C.c_uint32, C.c_uint32, P, P, C.c_uint64, C.c_uint32,
                                    C.POINTER(C.c_double)]),
+    "chai_cuda_reduce_noalloc": (C.c_int, [C.c_uint32, C.c_uint32, P, P, C.c_uint64, C.c_uint32, P, P]),
     "chai_cuda_tune": (C.c_int, [P, C.POINTER(chai_gemm_key), C.c_int, C.POINTER(chai_gemm_cfg)]),
     "chai_cuda_tune_db_load": (C.c_int, [P, C.c_char_p]),
     "chai_cuda_tune_db_save": (C.c_int, [P, C.c_char_p]),

@@ -131,3 +131,84 @@ int launch_reduce(chai_cuda_ctx* ctx, uint32_t op, uint32_t prec, const void* a,
 }
 
 }  // namespace chai
+
+// ---------------------------------------------------------------------------
+// Allocation-free reduction entry point.
+//
+// Some callers cannot allocate device memory at the moment they need a
+// reduction: code that runs while another component owns the allocator (a
+// pre-sized arena, a memory pool that must not grow), or callbacks where an
+// allocation could block or fail late.  chai_cuda_reduce_noalloc serves them:
+// it needs no context, calls no allocator, and keeps its per-block partial
+// sums in the fixed array below, which the library reserves on every GPU that
+// loads it, for as long as the process runs.
+//
+// Limits and sharing:
+//   - at most CHAI_NOALLOC_PARTIALS partial sums per call (blocks x slots);
+//     a call with more slots than that is rejected;
+//   - every call uses the same array, which keeps whatever the previous call
+//     left in it.  Each partial is written before it is read, so nothing has
+//     to start at zero -- but two calls whose kernels overlap on the GPU (on
+//     different streams without ordering between them) race on the array;
+//   - the first call on a device looks up the array's device address (once
+//     per device, with that device current); make that first call before any
+//     stream capture begins.
+#include <mutex>
+
+#define CHAI_NOALLOC_PARTIALS 8192
+
+static __device__ __align__(256) double chai_noalloc_partials[CHAI_NOALLOC_PARTIALS];
+
+namespace {
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[256] = {nullptr};
+}  // namespace
+
+extern "C" int chai_cuda_reduce_noalloc(uint32_t op, uint32_t prec, const void* a, const void* b, uint64_t n,
+                                        uint32_t slots, double* device_out, void* cuda_stream)
+{
+    using namespace chai;
+    if (!a || !device_out || op > 2 || (op == 2 && !b) || slots == 0) return CHAI_ERR_INVALID;
+    const size_t eb = prec_bytes(prec);
+    if (!eb) return CHAI_ERR_INVALID;
+    if (slots > CHAI_NOALLOC_PARTIALS) return CHAI_ERR_UNSUPPORTED;   // more partials than the fixed array holds
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return CHAI_ERR_NO_DEVICE;
+    double* partials = nullptr;
+    {
+        std::lock_guard<std::mutex> g(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, chai_noalloc_partials) != cudaSuccess || !p) {
+                cudaGetLastError();
+                return CHAI_ERR_NO_DEVICE;
+            }
+            g_noalloc_ptr[dev] = static_cast<double*>(p);
+        }
+        partials = g_noalloc_ptr[dev];
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned long long nv = (n * eb + 15) / 16;
+    unsigned long long gx = std::min<unsigned long long>((nv + 255) / 256, (unsigned long long)sms * 8 / slots + 1);
+    gx = std::min<unsigned long long>(gx, CHAI_NOALLOC_PARTIALS / slots);
+    if (gx < 1) gx = 1;
+    cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+    dim3 grid((unsigned)gx, slots);
+    const bool dot = op == 2;
+#define RNA(T) (dot ? chai_reduce_partials<T, true><<<grid, 256, 0, s>>>((const T*)a, (const T*)b, n, partials) \
+                    : chai_reduce_partials<T, false><<<grid, 256, 0, s>>>((const T*)a, (const T*)b, n, partials))
+    switch (prec) {
+        case CHAI_F32: RNA(float); break;
+        case CHAI_F64: RNA(double); break;
+        case CHAI_I32: RNA(int); break;
+        case CHAI_U32: RNA(unsigned); break;
+    }
+#undef RNA
+    CombineArgs ca;
+    ca.outs[0] = device_out;
+    ca.precs[0] = CHAI_F64;
+    ca.scales[0] = op == 1 ? 1.0 / (double)n : 1.0;
+    chai_combine_partials<<<dim3(slots, 1), 256, 0, s>>>(partials, (int)gx, (int)slots, ca);
+    return cudaGetLastError() == cudaSuccess ? CHAI_OK : CHAI_ERR_LAUNCH;
+}

@@ -224,6 +224,20 @@ int chai_cuda_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gem
 int chai_cuda_reduce(chai_cuda_ctx* ctx, uint32_t op, uint32_t prec, const void* a, const void* b,
                      uint64_t n, uint32_t slots, double* out);
 
+/* Allocation-free variant of chai_cuda_reduce.  No counterpart in the
+ * reference: it exists for callers that must not allocate device memory at
+ * call time (a fixed arena owns the GPU, or an allocation could block or fail
+ * late).  It needs no context and calls no allocator; the caller passes the
+ * inputs and a device output of `slots` doubles, and the kernels run on
+ * `cuda_stream` (NULL: the legacy default stream).  Partial sums live in a
+ * fixed device array of 8192 doubles that every GPU loading the library keeps
+ * until exit, so at most 8192 slots are accepted (CHAI_ERR_UNSUPPORTED
+ * beyond).  All calls share that array: calls whose kernels overlap on the GPU
+ * race.  The first call on a device looks up the array's address; make it
+ * before any stream capture. */
+int chai_cuda_reduce_noalloc(uint32_t op, uint32_t prec, const void* a, const void* b, uint64_t n,
+                             uint32_t slots, double* device_out, void* cuda_stream);
+
 /* ------------------------------------------------------------------ tuner */
 
 /* Replace StandardEM / AutoTuneEM / AutoTuneBench (autotune/StandardEM.cpp:69-147,
