@@ -139,14 +139,35 @@ def l2_flusher():
 
 # ---------------------------------------------------------------- workloads
 
+def kstats(L, ctx, name, reset=True):
+    ms, n = C.c_double(), C.c_uint64()
+    L.check(L.lib().chai_cuda_kernel_stats(ctx, name.encode(), C.byref(ms), C.byref(n), 1 if reset else 0), ctx)
+    return ms.value, n.value
+
+
+def traffic(name):
+    """Per-launch DRAM bytes from the committed ncu summary (profiles/ncu_traffic.json)."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if p.exists():
+        return json.loads(p.read_text()).get(name)
+    return None
+
+
+GEMM_PREC = {"fp32": 0, "tf32": 1, "bf16": 2, "bf16x3": 3, "bf16x6": 4}
+TENSOR_MULT = {0: 0, 1: 1, 2: 1, 3: 3, 4: 6}
+
+
 def run_gemm(args, L, ctx, stream):
     import torch
-    n = args.size or 8192
-    prec = {"fp32": 0, "tf32": 1, "bf16": 2, "bf16x3": 3, "bf16x6": 4, "fp8": 5}[args.precision]
-    g = torch.Generator(device="cuda").manual_seed(1)
-    A = torch.rand((n, n), device="cuda", generator=g, dtype=torch.float32) * 2 - 1
-    B = torch.rand((n, n), device="cuda", generator=g, dtype=torch.float32) * 2 - 1
+    n = args.size or 16384
+    prec = GEMM_PREC[args.precision]
+    # seeded uniform[-1, 1) operands from the library's own Philox fill (chai layout, seeds 1 and 2)
+    A = torch.empty((n, n), device="cuda", dtype=torch.float32)
+    B = torch.empty((n, n), device="cuda", dtype=torch.float32)
     Cm = torch.empty((n, n), device="cuda", dtype=torch.float32)
+    for t, seed in ((A, 1), (B, 2)):
+        rd = L.chai_rng_desc(1230, 4, 0, 4, seed, n, n, 1, 1, -1.0, 1.0)
+        L.check(L.lib().chai_cuda_rng_fill(ctx, C.byref(rd), C.c_void_p(t.data_ptr())), ctx)
     d = L.chai_gemm_desc(prec, 0, 0, 0, n, n, n, A.data_ptr(), n, B.data_ptr(), n, Cm.data_ptr(), n, 1.0, 0.0, 1,
                          0, 0, 0)
 
@@ -156,29 +177,33 @@ def run_gemm(args, L, ctx, stream):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    kstats(L, ctx, "gemm_tc")
     flops = 2.0 * n ** 3
     with Clocks(torch.cuda.current_device()) as clk:
         ts = time_events(step, args.steps, stream)
     ms = sum(ts) / len(ts)
-    # e2e: host buffers in, result out, through the public entry point
-    Ah, Bh = A.cpu().numpy(), B.cpu().numpy()
-    Ch = np.empty((n, n), dtype=np.float32)
+    k_ms, k_n = kstats(L, ctx, "gemm_tc")
+    kern_ms = k_ms / k_n if k_n else None
+    # e2e through the public entry points: pinned host A, B in, C out each step
+    Ah = A.cpu().pin_memory()
+    Bh = B.cpu().pin_memory()
+    Ch = torch.empty((n, n), dtype=torch.float32).pin_memory()
     ids = (901, 902, 903)
-    for i, arr in zip(ids, (Ah, Bh)):
-        L.check(L.lib().chai_cuda_buffer_alloc(ctx, i, arr.nbytes), ctx)
-    L.check(L.lib().chai_cuda_buffer_alloc(ctx, ids[2], Ch.nbytes), ctx)
+    for i in ids:
+        L.check(L.lib().chai_cuda_buffer_alloc(ctx, i, n * n * 4), ctx)
     ptrs = []
     for i in ids:
         p = C.c_void_p()
         L.lib().chai_cuda_buffer_info(ctx, i, C.byref(p), None)
         ptrs.append(p.value)
     de = L.chai_gemm_desc(prec, 0, 0, 0, n, n, n, ptrs[0], n, ptrs[1], n, ptrs[2], n, 1.0, 0.0, 1, 0, 0, 0)
+    del A, B, Cm
 
     def e2e():
-        L.check(L.lib().chai_cuda_upload(ctx, ids[0], Ah.ctypes.data_as(C.c_void_p), Ah.nbytes), ctx)
-        L.check(L.lib().chai_cuda_upload(ctx, ids[1], Bh.ctypes.data_as(C.c_void_p), Bh.nbytes), ctx)
+        L.check(L.lib().chai_cuda_upload(ctx, ids[0], C.c_void_p(Ah.data_ptr()), n * n * 4), ctx)
+        L.check(L.lib().chai_cuda_upload(ctx, ids[1], C.c_void_p(Bh.data_ptr()), n * n * 4), ctx)
         L.check(L.lib().chai_cuda_gemm(ctx, C.byref(de)), ctx)
-        L.check(L.lib().chai_cuda_readback(ctx, ids[2], Ch.ctypes.data_as(C.c_void_p), Ch.nbytes), ctx)
+        L.check(L.lib().chai_cuda_readback(ctx, ids[2], C.c_void_p(Ch.data_ptr()), n * n * 4), ctx)
 
     e2e()
     torch.cuda.synchronize()
@@ -188,21 +213,27 @@ def run_gemm(args, L, ctx, stream):
         e2e()
     torch.cuda.synchronize()
     e_ms = (time.perf_counter() - t0) * 1e3 / esteps
+    for i in ids:
+        L.lib().chai_cuda_release(ctx, i)
     P, kind = peaks()
-    tensor_mult = {0: 0, 1: 1, 2: 1, 3: 3, 4: 6, 5: 1}[prec]
-    achieved = flops * max(1, tensor_mult) / (ms * 1e-3) / 1e12
+    tensor_flops = flops * TENSOR_MULT[prec]
+    roof = None
+    if prec and kern_ms:
+        achieved = tensor_flops / (kern_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": P["bf16_tflops"], "unit": "TFLOP/s",
+                "frac": achieved / P["bf16_tflops"], "traffic": traffic("gemm_tc_%s_%d" % (args.precision, n)),
+                "peak_source": "%s (bf16 dense, burst)" % kind, "kernel": "chai_gemm_tc_kernel",
+                "kernel_ms": kern_ms, "algorithmic_flops": tensor_flops}
     return {
         "metric": "GEMM TFLOP/s at err vs FP32", "unit": "TFLOP/s", "value": flops / (ms * 1e-3) / 1e12,
         "ms_per_step": ms, "dtype": args.precision, "higher_is_better": True,
-        "config": {"workload": "gemm M=N=K=%d f32 in, %s" % (n, args.precision), "m": n, "n": n, "k": n,
-                   "l2": "inputs (%d MiB each) larger than L2" % (n * n * 4 >> 20)},
+        "config": {"workload": "square GEMM M=N=K=%d, f32 operands uniform[-1,1) (chai Philox seeds 1,2), %s"
+                   % (n, args.precision), "m": n, "n": n, "k": n,
+                   "l2": "operands (%d MiB each) larger than L2" % (n * n * 4 >> 20),
+                   "includes": "operand split/transposition prepass + tcgen05 GEMM"},
         "e2e": {"value": flops / (e_ms * 1e-3) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": 2 * n * n * 4,
                 "d2h_bytes_per_step": n * n * 4},
-        "roofline": {"bound": "tensor" if prec else "fp32-simt", "achieved": achieved,
-                     "peak": P["bf16_tflops"] if prec else None, "unit": "TFLOP/s",
-                     "frac": (achieved / P["bf16_tflops"]) if prec else None, "traffic": None,
-                     "peak_source": kind},
-        "clocks": clk.summary(), "gpu_launches": args.steps * (2 if prec in (3, 4, 5) else 1),
+        "roofline": roof, "clocks": clk.summary(), "gpu_launches": args.steps * (1 if prec in (0, 2) else 3),
     }
 
 
@@ -212,22 +243,24 @@ def mc_expr(ch, g, W, H):
                           - f(100), f(0)))
 
 
+def record(ch, build):
+    ch._Client.pending = []
+    out = build()
+    stmts = [(v, ver, cells) for v, ver, cells, _ in ch._Client.pending]
+    ch._Client.pending = []
+    return stmts, out
+
+
 def run_mc(args, L, ctx, stream):
     import torch
     import chai_b200.api as ch
     W, H = 8192, 16384                 # 2^27 normals from 2^26 Box-Muller pairs
-    dev = ch.init()
+    dev = ch.vm()
     n = W * H
-    g = ch.RNGf32(ch.RNG_PHILOX, 42)
-    # record the trace once (as the scheduler does for a repeated hash)
-    ch._Client.pending = []
-    p = ch.Arrayf32(mc_expr(ch, g, W, H))
-    stmts = [(v, ver, cells) for v, ver, cells, _ in ch._Client.pending]
-    ch._Client.pending = []
+    stmts, p = record(ch, lambda: ch.Arrayf32(mc_expr(ch, ch.RNGf32(ch.RNG_PHILOX, 42), W, H)))
     bid = 77001
-    binds = [(p.var, L.F32 if hasattr(L, "F32") else 4, 1, 1, 1, 0, bid)]
     desc, keep = ch.build_desc(stmts)
-    barr = (L.chai_buffer_binding * 1)(L.chai_buffer_binding(*binds[0]))
+    barr = (L.chai_buffer_binding * 1)(L.chai_buffer_binding(p.var, 4, 1, 1, 1, 0, bid))
 
     def step():
         L.check(L.lib().chai_cuda_evaluate(dev.ctx, C.byref(desc), barr, 1), dev.ctx)
@@ -235,84 +268,226 @@ def run_mc(args, L, ctx, stream):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    kstats(L, ctx, "trace")
     with Clocks(torch.cuda.current_device()) as clk:
         ts = time_events(step, args.steps, stream)
     ms = sum(ts) / len(ts)
-    out = np.zeros(1, dtype=np.float32)
-    L.check(L.lib().chai_cuda_readback(dev.ctx, bid, out.ctypes.data_as(C.c_void_p), 4), dev.ctx)
+    k_ms, k_n = kstats(L, ctx, "trace")
 
-    # e2e through the public API: record + evaluate + read_scalar each step
     def e2e():
-        g2 = ch.RNGf32(ch.RNG_PHILOX, 42)
-        return float(ch.Arrayf32(mc_expr(ch, g2, W, H)).read_scalar())
+        return float(ch.Arrayf32(mc_expr(ch, ch.RNGf32(ch.RNG_PHILOX, 42), W, H)).read_scalar())
 
-    e2e()
+    payoff = e2e()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    esteps = max(1, args.steps)
-    for _ in range(esteps):
+    for _ in range(max(1, args.steps)):
         payoff = e2e()
-    e_ms = (time.perf_counter() - t0) * 1e3 / esteps
+    e_ms = (time.perf_counter() - t0) * 1e3 / max(1, args.steps)
     return {
         "metric": "trace throughput (MC: Philox normals -> exp -> mean)", "unit": "Gnormals/s",
         "value": n / (ms * 1e-3) / 1e9, "ms_per_step": ms, "dtype": "f32", "higher_is_better": True,
-        "config": {"workload": "mc 2^27 normals fused", "normals": n, "payoff": payoff,
-                   "l2": "no HBM inputs (RNG in registers)"},
+        "config": {"workload": "Monte Carlo trace, 2^27 Philox4x32-10 Box-Muller normals, fused", "normals": n,
+                   "payoff": payoff, "l2": "no HBM inputs (RNG in registers)",
+                   "kernel_ms": (k_ms / k_n) if k_n else None},
         "e2e": {"value": n / (e_ms * 1e-3) / 1e9, "unit": "Gnormals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 16},
         "roofline": None, "clocks": clk.summary(), "gpu_launches": args.steps * 2,
     }
 
 
-WORKLOADS = {"gemm": run_gemm, "mc": run_mc}
+def kirsch_expr(ch, A, W, H):
+    f = np.float32
+    X, Y = ch.index_f32(0, W, H), ch.index_f32(1, W, H)
+    one = f(1)
+    nb = [ch.gather2_floor(A, X - one, Y - one), ch.gather2_floor(A, X, Y - one),
+          ch.gather2_floor(A, X + one, Y - one), ch.gather2_floor(A, X + one, Y),
+          ch.gather2_floor(A, X + one, Y + one), ch.gather2_floor(A, X, Y + one),
+          ch.gather2_floor(A, X - one, Y + one), ch.gather2_floor(A, X - one, Y)]
+    total = nb[0] + nb[1] + nb[2] + nb[3] + nb[4] + nb[5] + nb[6] + nb[7]
+    r = [f(8) * ((nb[k] + nb[(k + 1) % 8]) + nb[(k + 2) % 8]) - f(3) * total for k in range(8)]
+    return ch.max(ch.max(ch.max(r[0], r[1]), ch.max(r[2], r[3])), ch.max(ch.max(r[4], r[5]), ch.max(r[6], r[7])))
+
+
+def run_kirsch(args, L, ctx, stream):
+    import torch
+    import chai_b200.api as ch
+    W = H = args.size or 8192
+    dev = ch.vm()
+    img = torch.empty((H, W), device="cuda", dtype=torch.float32)
+    rd = L.chai_rng_desc(1230, 4, 0, 4, 5, W, H, 1, 1, 0.0, 1.0)
+    L.check(L.lib().chai_cuda_rng_fill(ctx, C.byref(rd), C.c_void_p(img.data_ptr())), ctx)
+    out = torch.empty_like(img)
+    in_id, out_id = 88001, 88002
+    L.check(L.lib().chai_cuda_buffer_wrap(ctx, in_id, C.c_void_p(img.data_ptr()), img.numel() * 4), ctx)
+    L.check(L.lib().chai_cuda_buffer_wrap(ctx, out_id, C.c_void_p(out.data_ptr()), out.numel() * 4), ctx)
+
+    def build():
+        A = ch._ARR[4](_raw=([ch._bc(0, 0), ], W, H, 1))
+        return A
+    # trace: A bound as an input variable, K bound as an output variable
+    ch._Client.pending = []
+    a_var = next(ch._Client.vars)
+    A = ch._Raw([ch._bc(1, a_var, 0)], 4, W, H)
+    K = ch.Arrayf32(kirsch_expr(ch, A, W, H))
+    stmts = [(v, ver, cells) for v, ver, cells, _ in ch._Client.pending]
+    ch._Client.pending = []
+    desc, keep = ch.build_desc(stmts)
+    barr = (L.chai_buffer_binding * 2)(L.chai_buffer_binding(a_var, 4, W, H, 1, 0, in_id),
+                                       L.chai_buffer_binding(K.var, 4, W, H, 1, 0, out_id))
+
+    def step():
+        L.check(L.lib().chai_cuda_evaluate(dev.ctx, C.byref(desc), barr, 2), dev.ctx)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    kstats(L, ctx, "trace")
+    with Clocks(torch.cuda.current_device()) as clk:
+        ts = time_events(step, args.steps, stream)
+    ms = sum(ts) / len(ts)
+    k_ms, k_n = kstats(L, ctx, "trace")
+    nbytes = 2 * 4 * W * H
+    # e2e: host image in (pinned), edge map out, through the public API
+    hin = img.cpu().pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    e_in, e_out = 88003, 88004
+    L.check(L.lib().chai_cuda_buffer_alloc(ctx, e_in, W * H * 4), ctx)
+    barr2 = (L.chai_buffer_binding * 2)(L.chai_buffer_binding(a_var, 4, W, H, 1, 0, e_in),
+                                        L.chai_buffer_binding(K.var, 4, W, H, 1, 0, e_out))
+
+    def e2e():
+        L.check(L.lib().chai_cuda_upload(ctx, e_in, C.c_void_p(hin.data_ptr()), W * H * 4), ctx)
+        L.check(L.lib().chai_cuda_evaluate(dev.ctx, C.byref(desc), barr2, 2), dev.ctx)
+        L.check(L.lib().chai_cuda_readback(ctx, e_out, C.c_void_p(hout.data_ptr()), W * H * 4), ctx)
+
+    e2e()
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.steps, 5))):
+        e2e()
+    e_ms = (time.perf_counter() - t0) * 1e3 / max(1, min(args.steps, 5))
+    P, kind = peaks()
+    kern_ms = k_ms / k_n if k_n else None
+    roof = None
+    if kern_ms:
+        ach = nbytes / (kern_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": ach, "peak": P["hbm_gbs"], "unit": "GB/s", "frac": ach / P["hbm_gbs"],
+                "traffic": traffic("trace_kirsch_%d" % W), "peak_source": "%s (copy)" % kind,
+                "kernel": "chai_group (Kirsch trace)", "kernel_ms": kern_ms, "algorithmic_bytes": nbytes}
+    return {
+        "metric": "trace HBM GB/s", "unit": "GB/s", "value": nbytes / (ms * 1e-3) / 1e9, "ms_per_step": ms,
+        "dtype": "f32", "higher_is_better": True,
+        "config": {"workload": "Kirsch 8-direction compass filter via gather2_floor, %dx%d f32 uniform[0,1)"
+                   % (W, H), "l2": "image (%d MiB) larger than L2" % (W * H * 4 >> 20)},
+        "e2e": {"value": nbytes / (e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": W * H * 4,
+                "d2h_bytes_per_step": W * H * 4},
+        "roofline": roof, "clocks": clk.summary(), "gpu_launches": args.steps,
+    }
+
+
+def run_gemv(args, L, ctx, stream):
+    import torch
+    m = n = args.size or 8192
+    dt = torch.float64 if args.precision == "f64" else torch.float32
+    prec = 8 if dt == torch.float64 else 4
+    eb = 8 if prec == 8 else 4
+    A = torch.rand((m, n), device="cuda", dtype=dt) * 2 - 1
+    x = torch.rand(n, device="cuda", dtype=dt) * 2 - 1
+    y = torch.empty(m, device="cuda", dtype=dt)
+
+    def step():
+        L.check(L.lib().chai_cuda_gemv(ctx, prec, 0, m, n, 1.0, C.c_void_p(A.data_ptr()), n,
+                                       C.c_void_p(x.data_ptr()), 0.0, C.c_void_p(y.data_ptr())), ctx)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    kstats(L, ctx, "gemv")
+    flush = l2_flusher()
+    with Clocks(torch.cuda.current_device()) as clk:
+        ts = time_events(step, args.steps, stream, flush=flush)
+    ms = sum(ts) / len(ts)
+    k_ms, k_n = kstats(L, ctx, "gemv")
+    nbytes = (m * n + m + n) * eb
+    P, kind = peaks()
+    kern_ms = k_ms / k_n if k_n else ms
+    ach = nbytes / (kern_ms * 1e-3) / 1e9
+    return {
+        "metric": "GEMV GB/s", "unit": "GB/s", "value": nbytes / (ms * 1e-3) / 1e9, "ms_per_step": ms,
+        "dtype": "f64" if prec == 8 else "f32", "higher_is_better": True,
+        "config": {"workload": "GEMV y = A x, %dx%d %s" % (m, n, "f64" if prec == 8 else "f32"),
+                   "l2": "flushed between steps"},
+        "e2e": None,
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": P["hbm_gbs"], "unit": "GB/s",
+                     "frac": ach / P["hbm_gbs"], "traffic": traffic("gemv_%d" % m), "peak_source": kind,
+                     "kernel": "chai_gemv_n", "kernel_ms": kern_ms, "algorithmic_bytes": nbytes},
+        "clocks": clk.summary(), "gpu_launches": args.steps,
+    }
+
+
+WORKLOADS = {"gemm": run_gemm, "mc": run_mc, "kirsch": run_kirsch, "gemv": run_gemv}
 
 
 # ---------------------------------------------------------------- reference arm
 
-def run_reference(args):
-    """The reference's own CPU interpreter (oracle/_ref/ref_driver), on a
-    bounded sample of the same workload."""
+def run_reference(args, steps=None):
+    """The reference's own CPU implementation of the path -- its bytecode
+    interpreter (runtime/Interpreter.cpp), built from the reference sources into
+    oracle/_ref -- timed on this host on a bounded sample of the same workload.
+    The interpreter is one device thread (runtime/DeviceMap.cpp:17-23), so it
+    uses one core whatever the host offers."""
     drv = ROOT / "oracle" / "_ref" / "ref_driver"
-    cores = 1   # the interpreter device is one thread (runtime/DeviceMap.cpp:17-23)
     if not drv.exists():
-        return {"impl": "reference", "unavailable": "oracle/_ref/ref_driver not built"}
+        return {"impl": "reference", "unavailable": "oracle/_ref/ref_driver not built (reference sources absent)"}
+    steps = steps or max(1, args.steps)
     wl = args.workload
+    times = []
     with tempfile.TemporaryDirectory() as td:
+        rng = np.random.default_rng(1)
         if wl == "gemm":
-            n = 1024
-            rng = np.random.default_rng(1)
-            A = rng.uniform(-1, 1, (n, n)).astype(np.float32)
-            A.tofile(td + "/A")
-            A.tofile(td + "/B")
-            times = []
-            for _ in range(max(1, min(args.steps, 3))):
-                r = subprocess.run([str(drv), "gemm_f32", str(n), str(n), str(n), td + "/A", td + "/B", td + "/C"],
-                                   capture_output=True, text=True, timeout=600)
-                times.append(float(r.stdout.split("ms=")[1].split()[0]))
-            ms = statistics.median(times)
-            v = 2.0 * n ** 3 / (ms * 1e-3) / 1e12
+            n = 512      # the reference's own CPU-runnable matmul size; 1024^3 takes ~18 s per run
+            rng.uniform(-1, 1, (n, n)).astype(np.float32).tofile(td + "/A")
+            rng.uniform(-1, 1, (n, n)).astype(np.float32).tofile(td + "/B")
+            cmd = [str(drv), "gemm_f32", str(n), str(n), str(n), td + "/A", td + "/B", td + "/C"]
             unit, metric = "TFLOP/s", "GEMM TFLOP/s at err vs FP32"
-            sample = "interpreter matmul 1024^3 f32 (double accumulation), make2 inputs"
-        else:
-            W, H = 1024, 1024
-            times = []
-            for _ in range(max(1, min(args.steps, 3))):
-                r = subprocess.run([str(drv), "mc_rng", str(W), str(H)], capture_output=True, text=True,
-                                   timeout=600)
-                times.append(float(r.stdout.split("ms=")[1].split()[0]))
-            ms = statistics.median(times)
-            v = W * H / (ms * 1e-3) / 1e9
+            conv = lambda ms: 2.0 * n ** 3 / (ms * 1e-3) / 1e12
+            sample = "interpreter matmul 512^3 f32 (double accumulation), inputs via make2"
+        elif wl == "mc":
+            W, H = 1024, 512
+            cmd = [str(drv), "mc_rng", str(W), str(H)]
             unit, metric = "Gnormals/s", "trace throughput (MC: Philox normals -> exp -> mean)"
-            sample = "interpreter MC trace over 2^20 normals (its own RNG)"
+            conv = lambda ms: W * H / (ms * 1e-3) / 1e9
+            sample = "interpreter MC trace over 2^19 normals (its own RNG)"
+        elif wl == "kirsch":
+            W = H = 1024
+            rng.uniform(0, 1, (H, W)).astype(np.float32).tofile(td + "/img")
+            cmd = [str(drv), "kirsch", str(W), str(H), td + "/img", td + "/out"]
+            unit, metric = "GB/s", "trace HBM GB/s"
+            conv = lambda ms: 2 * 4 * W * H / (ms * 1e-3) / 1e9
+            sample = "interpreter Kirsch trace (8 gather2_floor + max) over 1024x1024"
+        else:
+            m = n = 4096
+            rng.uniform(-1, 1, (m, n)).astype(np.float32).tofile(td + "/A")
+            rng.uniform(-1, 1, n).astype(np.float32).tofile(td + "/x")
+            cmd = [str(drv), "gemv_f32", str(m), str(n), td + "/A", td + "/x", td + "/y"]
+            unit, metric = "GB/s", "GEMV GB/s"
+            conv = lambda ms: (m * n + m + n) * 4 / (ms * 1e-3) / 1e9
+            sample = "interpreter matmul(matrix, vector) 4096x4096 f32"
+        for _ in range(steps):
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+            if r.returncode != 0:
+                return {"impl": "reference", "unavailable": "ref_driver failed: " + r.stderr[-200:]}
+            times.append(float(r.stdout.split("ms=")[1].split()[0]))
+    ms = statistics.median(times)
+    v = conv(ms)
     return {"impl": "reference", "metric": metric, "value": v, "unit": unit, "ms_per_step": ms,
-            "higher_is_better": True, "cpu_baseline": {"value": v, "unit": unit, "cores": cores,
-                                                      "kind": "reference", "sample": sample},
+            "higher_is_better": True,
+            "cpu_baseline": {"value": v, "unit": unit, "cores": 1, "kind": "reference", "sample": sample},
             "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def cpu_baseline(args):
-    r = run_reference(args)
-    return r.get("cpu_baseline") if "cpu_baseline" in r else None
+    r = run_reference(args, steps=2)
+    return r.get("cpu_baseline") if "cpu_baseline" in r else {"unavailable": r.get("unavailable")}
 
 
 # ---------------------------------------------------------------- main
@@ -323,6 +498,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="gemm", choices=sorted(WORKLOADS))
+    ap.add_argument("--sweep", default="", help="gemm only: write the precision/error sweep JSON here")
     ap.add_argument("--precision", default="bf16x3")
     ap.add_argument("--size", type=int, default=0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -337,6 +513,7 @@ def main():
             line.update({"n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup})
             print(json.dumps(line))
         return
+    os.environ.setdefault("CHAI_KERNEL_TIMING", "1")
     import torch
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)

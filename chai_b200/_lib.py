@@ -81,6 +81,7 @@ SIGNATURES = {
     "chai_cuda_error_string": (C.c_char_p, [C.c_int]),
     "chai_cuda_last_error": (C.c_char_p, [P]),
     "chai_cuda_set_stream": (C.c_int, [P, P]),
+    "chai_cuda_kernel_stats": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int]),
     "chai_cuda_buffer_alloc": (C.c_int, [P, C.c_uint64, C.c_size_t]),
     "chai_cuda_buffer_wrap": (C.c_int, [P, C.c_uint64, P, C.c_size_t]),
     "chai_cuda_buffer_info": (C.c_int, [P, C.c_uint64, C.POINTER(P), C.POINTER(C.c_size_t)]),

@@ -64,6 +64,23 @@ bool fault_injected(const char* site)
     return false;
 }
 
+void ktime_begin(chai_cuda_ctx* ctx, const char* name, cudaEvent_t* ev)
+{
+    (void)name;
+    ev[0] = ev[1] = nullptr;
+    if (!ctx->kernel_timing) return;
+    cudaEventCreate(&ev[0]);
+    cudaEventCreate(&ev[1]);
+    cudaEventRecord(ev[0], ctx->stream);
+}
+
+void ktime_end(chai_cuda_ctx* ctx, const char* name, cudaEvent_t* ev)
+{
+    if (!ctx->kernel_timing || !ev[0]) return;
+    cudaEventRecord(ev[1], ctx->stream);
+    ctx->kstats[name].pending.push_back(std::make_pair(ev[0], ev[1]));
+}
+
 Buffer* find_buffer(chai_cuda_ctx* ctx, uint64_t id)
 {
     std::lock_guard<std::mutex> g(ctx->mem_mutex);
@@ -187,6 +204,7 @@ int chai_cuda_init(int device, const char* config, chai_cuda_ctx** out)
         return CHAI_ERR_OOM;
     }
     ctx->pinned_count = 4096;
+    ctx->kernel_timing = getenv("CHAI_KERNEL_TIMING") && atoi(getenv("CHAI_KERNEL_TIMING")) != 0;
     ctx->jit.reset(new Jit(ctx));
     ctx->tuner.reset(new Tuner(ctx));
     if (!ctx->cfg.tune_db.empty()) ctx->tuner->load(ctx->cfg.tune_db);
@@ -209,6 +227,29 @@ int chai_cuda_shutdown(chai_cuda_ctx* ctx)
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
+    return CHAI_OK;
+}
+
+// Device time of the library's hot kernels, recorded with CUDA events on the
+// context stream when CHAI_KERNEL_TIMING=1 (the counterpart of the reference's
+// per-dispatch timing in Scheduler::_workStat, runtime/Scheduler.cpp:198-220).
+int chai_cuda_kernel_stats(chai_cuda_ctx* ctx, const char* name, double* total_ms, uint64_t* launches, int reset)
+{
+    if (!ctx || !name) return CHAI_ERR_INVALID;
+    CHAI_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    auto& st = ctx->kstats[name];
+    for (auto& p : st.pending) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.first, p.second);
+        st.ms += ms;
+        st.launches++;
+        cudaEventDestroy(p.first);
+        cudaEventDestroy(p.second);
+    }
+    st.pending.clear();
+    if (total_ms) *total_ms = st.ms;
+    if (launches) *launches = st.launches;
+    if (reset) { st.ms = 0; st.launches = 0; }
     return CHAI_OK;
 }
 

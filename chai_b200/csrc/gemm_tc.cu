@@ -1,0 +1,680 @@
+// Tensor-core GEMM for sm_100a: TMA -> shared memory -> tcgen05.mma with the
+// accumulator in TMEM -> tcgen05.ld epilogue.  The only dense contraction of
+// the back end (the reference's counterpart is the auto-tuned OpenCL GEMM,
+// autotune/EvergreenMatmulMM.cpp, driven by enqueue/EnqueueMatmulAuto.cpp).
+//
+// Operand preparation ("planes").  C = alpha * A B + beta * C with f32 A (M x K,
+// row-major) and B (K x N, row-major).  A prepass writes the operands in the
+// tensor-core type, K-major, with rows padded to whole 128-byte K blocks:
+//   A'  M x K'   and   B'  N x K'  (B transposed),
+// where each 128-byte block of the original K range is expanded into S blocks
+// of "planes" of the split value:
+//   bf16     S = 1  [a0]                     x [b0]
+//   bf16x3   S = 3  [a0 a0 a1]               x [b0 b1 b0]
+//   bf16x6   S = 6  [a0 a0 a1 a0 a1 a2]      x [b0 b1 b0 b2 b1 b0]
+//   tf32     S = 1  [a] (f32 bits, kind::tf32)
+// with a0 = bf16(a), a1 = bf16(a - a0), a2 = bf16(a - a0 - a1).  A split
+// precision is therefore one bf16 GEMM over K' = S * K_pad: the products
+// a_i b_j with i + j <= 1 (x3) or <= 2 (x6) are accumulated in FP32 in TMEM,
+// interleaved block by block.  Dropped terms are O(2^-24) (x6) and O(2^-16)
+// (x3) relative to |a||b|.
+//
+// Kernel.  One 128 x 256 output tile per CTA, 6 warps:
+//   warp 0    TMA producer: 4-stage ring of {A 128x128B, B 256x128B} tiles,
+//             SWIZZLE_128B, mbarrier complete_tx;
+//   warp 1    allocates 256 TMEM columns; one elected thread issues
+//             4 x tcgen05.mma (M=128, N=256, K=32 bytes) per stage and
+//             tcgen05.commit frees the stage;
+//   warps 2-5 epilogue: tcgen05.ld 32x32b.x16 (TMEM lane quarter = warp % 4),
+//             alpha/beta, 128-bit stores.
+// Every mbarrier wait is bounded: on timeout the kernel records an error code
+// in the context status word, stops issuing, waits (bounded) for its own TMA
+// copies, releases TMEM and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "internal.h"
+
+namespace chai {
+
+int launch_transpose(chai_cuda_ctx* ctx, uint32_t prec, const void* in, void* out, int64_t w, int64_t h,
+                     int64_t slots);
+
+namespace tc {
+
+constexpr int BM = 128;
+constexpr int BN = 256;
+constexpr int KB_BYTES = 128;            // one swizzle row: 64 bf16 / 32 tf32 / 128 fp8
+constexpr int STAGES = 4;
+constexpr int A_STAGE = BM * KB_BYTES;   // 16 KiB
+constexpr int B_STAGE = BN * KB_BYTES;   // 32 KiB
+constexpr int SMEM_BYTES = STAGES * (A_STAGE + B_STAGE) + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int THREADS = 192;
+constexpr unsigned TMEM_COLS = 512;                       // two 128 x 256 FP32 accumulators
+constexpr unsigned long long WAIT_NS = 2000000000ull;      // a wait gives up after 2 s
+constexpr int GROUP_M = 16;                                // tile raster: 16 M-tiles per group
+
+enum Kind { KIND_BF16 = 0, KIND_TF32 = 1 };
+
+__device__ __forceinline__ unsigned smem_u32(const void* p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// try_wait with an explicit suspend-time hint, so one poll lasts at most ~1 us
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(bar), "r"(parity), "r"(1000u)
+                 : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: false (and the status word set) once WAIT_NS has passed.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int* status, int code)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > WAIT_NS) {
+            atomicExch(status, code);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap* map, unsigned bar, int x, int y, int z)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+                 ::"r"(dst), "l"(map), "r"(bar), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
+// K-major, SWIZZLE_128B shared-memory matrix descriptor: rows of 128 bytes,
+// 8-row groups 1024 bytes apart (SBO), descriptor version 1, base offset 0.
+__device__ __forceinline__ unsigned long long smem_desc(unsigned addr)
+{
+    unsigned long long d = 0;
+    d |= (unsigned long long)((addr & 0x3FFFF) >> 4);          // start address
+    d |= (unsigned long long)1 << 16;                          // LBO (unused for swizzled K-major)
+    d |= (unsigned long long)(1024 >> 4) << 32;                // SBO
+    d |= (unsigned long long)1 << 46;                          // version
+    d |= (unsigned long long)2 << 61;                          // SWIZZLE_128B
+    return d;
+}
+
+// Instruction descriptor: FP32 accumulate, K-major A and B, M = 128, N = 256.
+template <int KIND>
+__device__ __forceinline__ unsigned instr_desc()
+{
+    unsigned d = 0;
+    d |= 1u << 4;                                   // C format F32
+    const unsigned fmt = KIND == KIND_TF32 ? 2u : 1u;   // BF16 = 1, TF32 = 2
+    d |= fmt << 7;                                  // A format
+    d |= fmt << 10;                                 // B format
+    d |= (unsigned)(BN >> 3) << 17;                 // N / 8
+    d |= (unsigned)(BM >> 4) << 24;                 // M / 16
+    return d;
+}
+
+template <int KIND>
+__device__ __forceinline__ void mma(unsigned tmem, unsigned long long a, unsigned long long b, unsigned idesc,
+                                    unsigned accumulate)
+{
+    if (KIND == KIND_TF32)
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+                     ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    else
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                     ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(unsigned bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16])
+{
+    unsigned r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// 32 consecutive TMEM columns of this warp's 32 lanes; no wait (see tmem_wait)
+__device__ __forceinline__ void tmem_ld32_nowait(unsigned taddr, unsigned (&r)[32])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                 "[%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                   "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                   "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+struct EpiArgs {
+    float* c;
+    long long ldc, stride_c;
+    int m, n;
+    float alpha, beta;
+    int vec_ok;        // 16-byte aligned rows of C
+};
+
+struct TileGrid {
+    int tiles_m, tiles_n, batch;
+};
+
+// tile t -> (m, n, batch) in GROUP_M-high column strips, so the CTAs running
+// at one time share a small set of A and B panels in L2
+__device__ __forceinline__ void tile_coords(const TileGrid& g, int t, int& tm, int& tn, int& tb)
+{
+    const int per_batch = g.tiles_m * g.tiles_n;
+    tb = t / per_batch;
+    t -= tb * per_batch;
+    const int group = t / (GROUP_M * g.tiles_n);
+    const int first_m = group * GROUP_M;
+    const int rows = min(GROUP_M, g.tiles_m - first_m);
+    const int r = t - group * GROUP_M * g.tiles_n;
+    tm = first_m + r % rows;
+    tn = r / rows;
+}
+
+// Persistent: CTA b handles tiles b, b + G, b + 2G, ...  Barriers:
+//   full[s] / empty[s]      TMA ring (count 1 / committed by tcgen05)
+//   tfull[a] / tempty[a]    accumulator a in TMEM columns 256*a (MMA commit /
+//                           4 epilogue warps)
+template <int KIND, bool SPLIT>
+__global__ void __launch_bounds__(THREADS, 1)
+chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                    int kblocks, int split_s, TileGrid tg, EpiArgs ep, int* status)
+{
+    // Split precisions keep two accumulators per tile -- the a0*b0 blocks in
+    // one, every correction block in the other -- so the large running sum
+    // sees only the a0*b0 accumulation steps; they are added in FP32 in the
+    // epilogue.  That uses all 512 TMEM columns, so split tiles are single
+    // buffered (NB = 1); plain bf16 / tf32 tiles double-buffer (NB = 2).
+    constexpr int NB = SPLIT ? 1 : 2;
+    constexpr unsigned BUF_COLS = SPLIT ? 2 * BN : BN;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* sa = smem;
+    unsigned char* sb = smem + STAGES * A_STAGE;
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(sb + STAGES * B_STAGE);
+    unsigned long long* full = bars;
+    unsigned long long* empty = bars + STAGES;
+    unsigned long long* tfull = bars + 2 * STAGES;
+    unsigned long long* tempty = bars + 2 * STAGES + 2;
+    unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * STAGES + 4);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntiles = tg.tiles_m * tg.tiles_n * tg.batch;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(smem_u32(&tfull[a]), 1);
+            mbar_init(smem_u32(&tempty[a]), 4);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            long long it = 0, issued = 0;
+            const int kx_mul = KB_BYTES / (KIND == KIND_TF32 ? 4 : 2);
+            for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
+                int tm, tn, tb;
+                tile_coords(tg, t, tm, tn, tb);
+                for (int kb = 0; kb < kblocks; kb++, it++) {
+                    const int s = (int)(it % STAGES);
+                    const long long r = it / STAGES;
+                    if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (unsigned)((r - 1) & 1), status, 101)) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    const unsigned fb = smem_u32(&full[s]);
+                    mbar_expect_tx(fb, A_STAGE + B_STAGE);
+                    tma_load_3d(smem_u32(sa + s * A_STAGE), &map_a, fb, kb * kx_mul, tm * BM, tb);
+                    tma_load_3d(smem_u32(sb + s * B_STAGE), &map_b, fb, kb * kx_mul, tn * BN, tb);
+                    issued = it + 1;
+                }
+            }
+            // wait (bounded) until every copy this thread issued has landed
+            for (long long j = issued - STAGES < 0 ? 0 : issued - STAGES; j < issued; j++)
+                mbar_wait(smem_u32(&full[j % STAGES]), (unsigned)((j / STAGES) & 1), status, 102);
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------------------- MMA
+        if (lane == 0) {
+            const unsigned idesc = instr_desc<KIND>();
+            long long it = 0;
+            int lt = 0;
+            for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, lt++) {
+                const int ab = lt % NB;
+                const int use = lt / NB;
+                if (use >= 1 && !mbar_wait(smem_u32(&tempty[ab]), (unsigned)((use - 1) & 1), status, 105)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const unsigned acc_main = tmem + (unsigned)ab * BUF_COLS;
+                const unsigned acc_corr = acc_main + BN;
+                for (int kb = 0; kb < kblocks; kb++, it++) {
+                    const int s = (int)(it % STAGES);
+                    if (!mbar_wait(smem_u32(&full[s]), (unsigned)((it / STAGES) & 1), status, 103)) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const unsigned a0 = smem_u32(sa + s * A_STAGE), b0 = smem_u32(sb + s * B_STAGE);
+                    const int blk = SPLIT ? kb % split_s : 0;
+                    const unsigned acc = blk == 0 ? acc_main : acc_corr;
+                    const bool first = SPLIT ? (blk == 0 ? kb == 0 : kb == 1) : kb == 0;
+#pragma unroll
+                    for (int k = 0; k < KB_BYTES / 32; k++)
+                        mma<KIND>(acc, smem_desc(a0 + 32 * k), smem_desc(b0 + 32 * k), idesc, !(first && k == 0));
+                    mma_commit(smem_u32(&empty[s]));   // stage free once these MMAs finish
+                }
+                mma_commit(smem_u32(&tfull[ab]));      // accumulator ab complete
+            }
+        }
+    } else {
+        // ----------------------------------------------------------- epilogue
+        const int quarter = warp & 3;                  // TMEM lanes 32*quarter .. +31
+        int lt = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
+            const int ab = lt % NB;
+            const bool ok = mbar_wait(smem_u32(&tfull[ab]), (unsigned)((lt / NB) & 1), status, 104);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            int tm, tn, tb;
+            tile_coords(tg, t, tm, tn, tb);
+            const int row = tm * BM + quarter * 32 + lane;
+            float* crow = ep.c + (long long)tb * ep.stride_c + (long long)row * ep.ldc;
+            const bool do_store = ok && !*abort_flag && kblocks > 0;
+            const unsigned tbase = tmem + ((unsigned)(quarter * 32) << 16) + (unsigned)ab * BUF_COLS;
+            // 64 columns per step: two (four when split) 32-column TMEM loads in
+            // flight, one wait, then 16 x 16-byte stores of this lane's row
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 64) {
+                unsigned r0[32], r1[32];
+                tmem_ld32_nowait(tbase + (unsigned)c0, r0);          // warp-wide, always executed
+                tmem_ld32_nowait(tbase + (unsigned)(c0 + 32), r1);
+                float v[64];
+                if (SPLIT && split_s > 1) {
+                    unsigned q0[32], q1[32];
+                    tmem_ld32_nowait(tbase + (unsigned)(BN + c0), q0);
+                    tmem_ld32_nowait(tbase + (unsigned)(BN + c0 + 32), q1);
+                    tmem_wait();
+#pragma unroll
+                    for (int i = 0; i < 32; i++) {
+                        v[i] = __uint_as_float(r0[i]) + __uint_as_float(q0[i]);
+                        v[32 + i] = __uint_as_float(r1[i]) + __uint_as_float(q1[i]);
+                    }
+                } else {
+                    tmem_wait();
+#pragma unroll
+                    for (int i = 0; i < 32; i++) {
+                        v[i] = __uint_as_float(r0[i]);
+                        v[32 + i] = __uint_as_float(r1[i]);
+                    }
+                }
+                const int col = tn * BN + c0;
+                if (!do_store || row >= ep.m || col >= ep.n) continue;
+#pragma unroll
+                for (int i = 0; i < 64; i++) v[i] *= ep.alpha;
+                if (ep.vec_ok && col + 64 <= ep.n) {
+                    float4* p = reinterpret_cast<float4*>(crow + col);
+#pragma unroll
+                    for (int q = 0; q < 16; q++) {
+                        float4 o = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                        if (ep.beta != 0.0f) {
+                            const float4 old = p[q];
+                            o.x += ep.beta * old.x; o.y += ep.beta * old.y;
+                            o.z += ep.beta * old.z; o.w += ep.beta * old.w;
+                        }
+                        p[q] = o;
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 64; i++)
+                        if (col + i < ep.n) crow[col + i] = ep.beta != 0.0f ? v[i] + ep.beta * crow[col + i] : v[i];
+                }
+            }
+            // accumulator ab may be overwritten once all four warps have read it
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&tempty[ab]));
+            if (!ok || *abort_flag) break;
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+// ------------------------------------------------------------------ prepass
+
+__device__ __forceinline__ void split3(float a, __nv_bfloat16 (&p)[3])
+{
+    p[0] = __float2bfloat16_rn(a);
+    const float r1 = a - __bfloat162float(p[0]);
+    p[1] = __float2bfloat16_rn(r1);
+    const float r2 = r1 - __bfloat162float(p[1]);
+    p[2] = __float2bfloat16_rn(r2);
+}
+
+// plane index of K-block s for the A and B sides of a split precision
+__constant__ unsigned char kSelA[3][6] = {{0}, {0, 0, 1}, {0, 0, 1, 0, 1, 2}};
+__constant__ unsigned char kSelB[3][6] = {{0}, {0, 1, 0}, {0, 1, 0, 2, 1, 0}};
+
+// 8 consecutive values -> 16-byte chunks of plane p0/p1/p2
+__device__ __forceinline__ void split8(const float (&a)[8], uint4 (&q)[3])
+{
+    __nv_bfloat16 h[3][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        __nv_bfloat16 p[3];
+        split3(a[i], p);
+        h[0][i] = p[0]; h[1][i] = p[1]; h[2][i] = p[2];
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++) q[j] = *reinterpret_cast<const uint4*>(h[j]);
+}
+
+// A (rows x k, row-major, leading dim ld) -> A' (rows x S*kpad bf16); each
+// thread splits 8 consecutive elements and writes one 16-byte chunk per block
+template <int S, int MODE>
+__global__ void __launch_bounds__(256) split_rows_bf16(const float* __restrict__ x, long long ld, long long sx,
+                                                       int rows, int k, int kpad, __nv_bfloat16* __restrict__ out,
+                                                       long long so)
+{
+    const int batch = blockIdx.z;
+    const int row = blockIdx.y;
+    x += batch * sx + (long long)row * ld;
+    out += batch * so + (long long)row * S * kpad;
+    const int sel = S == 1 ? 0 : (S == 3 ? 1 : 2);
+    const bool vec = ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+    for (int k8 = blockIdx.x * blockDim.x + threadIdx.x; k8 * 8 < kpad; k8 += gridDim.x * blockDim.x) {
+        const int kk = k8 * 8;
+        float a[8];
+        if (vec && kk + 8 <= k) {
+            const float4 u = __ldg(reinterpret_cast<const float4*>(x + kk));
+            const float4 w = __ldg(reinterpret_cast<const float4*>(x + kk) + 1);
+            a[0] = u.x; a[1] = u.y; a[2] = u.z; a[3] = u.w; a[4] = w.x; a[5] = w.y; a[6] = w.z; a[7] = w.w;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; i++) a[i] = kk + i < k ? __ldg(x + kk + i) : 0.0f;
+        }
+        uint4 q[3];
+        split8(a, q);
+        const int kb = kk >> 6, j = kk & 63;
+#pragma unroll
+        for (int s = 0; s < S; s++)
+            *reinterpret_cast<uint4*>(out + (long long)(kb * S + s) * 64 + j) =
+                q[MODE == 0 ? kSelA[sel][s] : kSelB[sel][s]];
+    }
+}
+
+// B (k x cols, row-major) -> B' (cols x S*kpad bf16) through a 64 x 64 tile:
+// float4 loads along cols, 16-byte stores of 8 consecutive k per column
+template <int S>
+__global__ void __launch_bounds__(256) split_cols_bf16(const float* __restrict__ x, long long ld, long long sx, int k,
+                                                       int cols, int kpad, __nv_bfloat16* __restrict__ out,
+                                                       long long so)
+{
+    __shared__ float tile[64][65];
+    const int batch = blockIdx.z;
+    x += batch * sx;
+    out += batch * so;
+    const int k0 = blockIdx.y * 64, c0 = blockIdx.x * 64;
+    const bool vec = ((reinterpret_cast<uintptr_t>(x) & 15) == 0) && (ld % 4 == 0);
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // 16 float4 per tile row, 16 rows per pass
+    for (int i = ty; i < 64; i += 16) {
+        const int kk = k0 + i, cc = c0 + tx * 4;
+        float v[4];
+        if (vec && kk < k && cc + 4 <= cols) {
+            const float4 u = __ldg(reinterpret_cast<const float4*>(x + (long long)kk * ld + cc));
+            v[0] = u.x; v[1] = u.y; v[2] = u.z; v[3] = u.w;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; q++) v[q] = (kk < k && cc + q < cols) ? x[(long long)kk * ld + cc + q] : 0.0f;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) tile[i][tx * 4 + q] = v[q];
+    }
+    __syncthreads();
+    const int sel = S == 1 ? 0 : (S == 3 ? 1 : 2);
+    // 64 columns x 8 runs of 8 k = 512 items, two per thread
+    for (int item = threadIdx.x; item < 512; item += 256) {
+        const int c = item >> 3, r = item & 7;
+        const int cc = c0 + c, kk = k0 + r * 8;
+        if (cc >= cols || kk >= kpad) continue;
+        float a[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) a[i] = tile[r * 8 + i][c];
+        uint4 q[3];
+        split8(a, q);
+        const int kb = kk >> 6, j = kk & 63;
+        __nv_bfloat16* o = out + (long long)cc * S * kpad;
+#pragma unroll
+        for (int s = 0; s < S; s++) *reinterpret_cast<uint4*>(o + (long long)(kb * S + s) * 64 + j) = q[kSelB[sel][s]];
+    }
+}
+
+// f32 rows padded to kpad (tf32 operands), optionally transposing
+__global__ void pad_rows_f32(const float* __restrict__ x, long long ld, long long sx, int rows, int k, int kpad,
+                             float* __restrict__ out, long long so)
+{
+    const int batch = blockIdx.z, row = blockIdx.y;
+    x += batch * sx + (long long)row * ld;
+    out += batch * so + (long long)row * kpad;
+    for (int kk = blockIdx.x * blockDim.x + threadIdx.x; kk < kpad; kk += gridDim.x * blockDim.x)
+        out[kk] = kk < k ? x[kk] : 0.0f;
+}
+
+__global__ void transpose_pad_f32(const float* __restrict__ x, long long ld, long long sx, int k, int cols, int kpad,
+                                  float* __restrict__ out, long long so)
+{
+    __shared__ float tile[32][33];
+    const int batch = blockIdx.z;
+    x += batch * sx;
+    out += batch * so;
+    const int k0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int i = threadIdx.y; i < 32; i += 8) {
+        const int kk = k0 + i, cc = c0 + threadIdx.x;
+        tile[i][threadIdx.x] = (kk < k && cc < cols) ? x[(long long)kk * ld + cc] : 0.0f;
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += 8) {
+        const int cc = c0 + i, kk = k0 + threadIdx.x;
+        if (cc < cols && kk < kpad) out[(long long)cc * kpad + kk] = tile[threadIdx.x][i];
+    }
+}
+
+}  // namespace tc
+
+// ---------------------------------------------------------------- host side
+
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                     const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                     CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled encode_fn(chai_cuda_ctx* ctx)
+{
+    static PFN_encodeTiled fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_encodeTiled>(p);
+        else
+            set_error(ctx, CHAI_ERR_NO_DEVICE, "cuTensorMapEncodeTiled unavailable");
+    }
+    return fn;
+}
+
+// rows x kelems (row-major, per batch `batch_stride` elements), box kbox x rbox
+static int make_map(chai_cuda_ctx* ctx, CUtensorMap* map, const void* base, CUtensorMapDataType dt, int esize,
+                    long long kelems, long long rows, long long batch, long long batch_stride, int kbox, int rbox)
+{
+    PFN_encodeTiled enc = encode_fn(ctx);
+    if (!enc) return CHAI_ERR_NO_DEVICE;
+    cuuint64_t dims[3] = {(cuuint64_t)kelems, (cuuint64_t)rows, (cuuint64_t)batch};
+    cuuint64_t strides[2] = {(cuuint64_t)(kelems * esize), (cuuint64_t)(batch_stride * esize)};
+    cuuint32_t box[3] = {(cuuint32_t)kbox, (cuuint32_t)rbox, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, dt, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(ctx, CHAI_ERR_INVALID, "cuTensorMapEncodeTiled failed");
+    return CHAI_OK;
+}
+
+int launch_gemm_tc(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision)
+{
+    using namespace tc;
+    if (d->trans_a || d->trans_b) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: transposed operands");
+    if (precision == CHAI_GEMM_FP8) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "fp8 gemm not built");
+    const long long M = d->m, N = d->n, K = d->k, batch = d->batch > 0 ? d->batch : 1;
+    if (M == 0 || N == 0) return CHAI_OK;
+    if (K == 0) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: K = 0");
+    if (M > 65535 || batch > 65535) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: M or batch above 65535");
+    if (M > (1ll << 31) || N > (1ll << 31)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: size");
+    const bool tf32 = precision == CHAI_GEMM_TF32;
+    const int S = precision == CHAI_GEMM_BF16X3 ? 3 : precision == CHAI_GEMM_BF16X6 ? 6 : 1;
+    const int kblk = tf32 ? 32 : 64;                       // elements per 128-byte K block
+    const long long kpad = (K + kblk - 1) / kblk * kblk;
+    const long long kp = S * kpad;                         // K' of the planes
+    const size_t esz = tf32 ? 4 : 2;
+    const size_t a_bytes = (size_t)batch * M * kp * esz, b_bytes = (size_t)batch * N * kp * esz;
+    int st = ensure_scratch(ctx, a_bytes + b_bytes + 1024);
+    if (st) return st;
+    char* base = static_cast<char*>(ctx->scratch);
+    void* Ap = base;
+    void* Bp = base + ((a_bytes + 1023) & ~size_t(1023));
+    const float* A = static_cast<const float*>(d->a);
+    const float* B = static_cast<const float*>(d->b);
+    cudaStream_t s = ctx->stream;
+    // prepass
+    if (K > 0) {
+        dim3 rgrid((unsigned)std::min<long long>((kpad / 8 + 255) / 256, 64), (unsigned)M, (unsigned)batch);
+        dim3 tgrid((unsigned)((N + 31) / 32), (unsigned)((kpad + 31) / 32), (unsigned)batch);
+        dim3 sgrid((unsigned)((N + 63) / 64), (unsigned)(kpad / 64), (unsigned)batch);
+        if (tf32) {
+            pad_rows_f32<<<rgrid, 256, 0, s>>>(A, d->lda, d->stride_a, (int)M, (int)K, (int)kpad, (float*)Ap, M * kp);
+            transpose_pad_f32<<<tgrid, dim3(32, 8), 0, s>>>(B, d->ldb, d->stride_b, (int)K, (int)N, (int)kpad,
+                                                            (float*)Bp, N * kp);
+        } else {
+            __nv_bfloat16* a2 = (__nv_bfloat16*)Ap;
+            __nv_bfloat16* b2 = (__nv_bfloat16*)Bp;
+#define SPLIT(SS)                                                                                                   \
+    split_rows_bf16<SS, 0><<<rgrid, 256, 0, s>>>(A, d->lda, d->stride_a, (int)M, (int)K, (int)kpad, a2, M * kp);    \
+    split_cols_bf16<SS><<<sgrid, 256, 0, s>>>(B, d->ldb, d->stride_b, (int)K, (int)N, (int)kpad, b2, N * kp)
+            if (S == 1) { SPLIT(1); } else if (S == 3) { SPLIT(3); } else { SPLIT(6); }
+#undef SPLIT
+        }
+        CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    }
+    CUtensorMap ma, mb;
+    const CUtensorMapDataType dt = tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    st = make_map(ctx, &ma, Ap, dt, (int)esz, kp, M, batch, M * kp, kblk, BM);
+    if (st) return st;
+    st = make_map(ctx, &mb, Bp, dt, (int)esz, kp, N, batch, N * kp, kblk, BN);
+    if (st) return st;
+    EpiArgs ep;
+    ep.c = static_cast<float*>(d->c);
+    ep.ldc = d->ldc;
+    ep.stride_c = d->stride_c;
+    ep.m = (int)M;
+    ep.n = (int)N;
+    ep.alpha = (float)d->alpha;
+    ep.beta = (float)d->beta;
+    ep.vec_ok = ((reinterpret_cast<uintptr_t>(d->c) & 15) == 0 && d->ldc % 4 == 0 && d->stride_c % 4 == 0) ? 1 : 0;
+    const int kblocks = (int)(kp / kblk);
+    TileGrid tg;
+    tg.tiles_m = (int)((M + BM - 1) / BM);
+    tg.tiles_n = (int)((N + BN - 1) / BN);
+    tg.batch = (int)batch;
+    const long long ntiles = (long long)tg.tiles_m * tg.tiles_n * tg.batch;
+    if (ntiles > (1ll << 30)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: too many tiles");
+    const unsigned grid = (unsigned)std::min<long long>(ntiles, ctx->sm_count);
+#define LAUNCH_TC(KD, SP)                                                                                      \
+    do {                                                                                                       \
+        cudaFuncSetAttribute(chai_gemm_tc_kernel<KD, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES); \
+        chai_gemm_tc_kernel<KD, SP><<<grid, THREADS, SMEM_BYTES, s>>>(ma, mb, kblocks, S, tg, ep, ctx->status_word); \
+    } while (0)
+    cudaEvent_t ev[2];
+    ktime_begin(ctx, "gemm_tc", ev);
+    if (tf32) LAUNCH_TC(KIND_TF32, false);
+    else if (S == 1) LAUNCH_TC(KIND_BF16, false);
+    else LAUNCH_TC(KIND_BF16, true);
+#undef LAUNCH_TC
+    ktime_end(ctx, "gemm_tc", ev);
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    return CHAI_OK;
+}
+
+}  // namespace chai

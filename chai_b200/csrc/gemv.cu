@@ -110,8 +110,11 @@ static int gemv_t(chai_cuda_ctx* ctx, int trans, int64_t m, int64_t n, double al
 {
     if (!trans) {
         const unsigned blocks = (unsigned)((m + 7) / 8);
+        cudaEvent_t ev[2];
+        ktime_begin(ctx, "gemv", ev);
         if (blocks) chai_gemv_n<T><<<blocks, 256, 0, ctx->stream>>>((const T*)a, lda, (const T*)x, (T*)y, m, n,
                                                                     (T)alpha, (T)beta);
+        ktime_end(ctx, "gemv", ev);
         CHAI_CUDA_TRY(ctx, cudaGetLastError());
         return CHAI_OK;
     }

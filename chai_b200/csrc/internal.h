@@ -54,6 +54,10 @@ struct chai_cuda_ctx {
     std::unique_ptr<chai::Jit> jit;
     std::unique_ptr<chai::Tuner> tuner;
     uint64_t next_temp_id = 1ull << 62;                     // ids of library-owned temporaries
+    // per-kernel device time (CHAI_KERNEL_TIMING=1): name -> events in flight / totals
+    bool kernel_timing = false;
+    struct KStat { double ms = 0; uint64_t launches = 0; std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending; };
+    std::map<std::string, KStat> kstats;
 };
 
 namespace chai {
@@ -65,6 +69,9 @@ int ensure_scratch(chai_cuda_ctx* ctx, size_t bytes);
 Buffer* find_buffer(chai_cuda_ctx* ctx, uint64_t id);
 int alloc_buffer(chai_cuda_ctx* ctx, uint64_t id, size_t bytes);
 bool fault_injected(const char* site);
+// bracket a kernel launch with events when kernel timing is on
+void ktime_begin(chai_cuda_ctx* ctx, const char* name, cudaEvent_t* ev);
+void ktime_end(chai_cuda_ctx* ctx, const char* name, cudaEvent_t* ev);
 
 size_t prec_bytes(uint32_t prec);
 

@@ -4,12 +4,6 @@
 
 namespace chai {
 
-int launch_gemm_tc(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision)
-{
-    (void)d; (void)precision;
-    return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tensor-core gemm not built");
-}
-
 int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_problem* p, int32_t count)
 {
     (void)precision; (void)p; (void)count;

@@ -367,8 +367,11 @@ int Translator::emit_group(const std::vector<int>& roots)
     std::vector<void*> ptrs(args.size());
     for (size_t k = 0; k < args.size(); k++)
         ptrs[k] = args[k].kind == KArg::PTR ? (void*)&args[k].ptr : (void*)&args[k].v;
+    cudaEvent_t kev[2];
+    ktime_begin(ctx_, "trace", kev);
     st = ctx_->jit->launch(fn, dim3((unsigned)gx, S, 1), dim3(256, 1, 1), 0, ptrs.data());
     if (st) return st;
+    ktime_end(ctx_, "trace", kev);
     kernels_launched++;
     if (nred) {
         std::vector<void*> outs;

@@ -80,6 +80,12 @@ int chai_cuda_synchronize(chai_cuda_ctx* ctx);
 const char* chai_cuda_error_string(int status);
 /* Human-readable detail of the last failure on this context. */
 const char* chai_cuda_last_error(chai_cuda_ctx* ctx);
+/* Device time of a hot kernel ("gemm_tc", "trace", "gemv") accumulated over
+ * its launches, measured with CUDA events on the context stream when the
+ * process runs with CHAI_KERNEL_TIMING=1 (the counterpart of the reference's
+ * per-dispatch timing, runtime/Scheduler.cpp:198-220). */
+int chai_cuda_kernel_stats(chai_cuda_ctx* ctx, const char* name, double* total_ms, uint64_t* launches,
+                           int reset);
 /* Run subsequent work on an external cudaStream_t (NULL = the context's own). */
 int chai_cuda_set_stream(chai_cuda_ctx* ctx, void* cuda_stream);
 

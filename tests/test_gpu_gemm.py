@@ -1,0 +1,102 @@
+"""GEMM precision sweep parity: every arithmetic of chai_cuda_gemm against the
+FP64 oracle (oracle/ops.c, pinned to the reference interpreter's matmul).
+
+Error metric (stated per precision): max |C - C64| / (|A| |B|)_ij, the
+componentwise-bound-normalised error, and the reference autotuner's two
+self-checks (autotune/EvergreenMatmulMM.cpp:905-1000): the sentinel (A = B = 1
+gives C = K) and the "paranoid" L1 check against a CPU double reference.
+
+Bounds: bf16 2^-7, tf32 2^-9 (operands keep 10 mantissa bits), bf16x3 2^-14
+(dropped a1*b1 and residual terms ~2^-16), bf16x6 within 4x the FP32 SIMT
+GEMM's own error plus 2^-22 (FP32 accumulation dominates), fp32 SIMT 2^-18."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from chai_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+BOUND = {L.GEMM_BF16: 2.0 ** -7, L.GEMM_TF32: 2.0 ** -9, L.GEMM_BF16X3: 2.0 ** -14, L.GEMM_FP32: 2.0 ** -18}
+
+
+def run_gemm(dev, A, B, prec, alpha=1.0, beta=0.0, C0=None):
+    import torch
+    batch = A.shape[0] if A.ndim == 3 else 1
+    A3 = A.reshape(batch, *A.shape[-2:])
+    B3 = B.reshape(batch, *B.shape[-2:])
+    M, K = A3.shape[1:]
+    N = B3.shape[2]
+    a = torch.from_numpy(np.ascontiguousarray(A3)).cuda()
+    b = torch.from_numpy(np.ascontiguousarray(B3)).cuda()
+    c = torch.from_numpy(np.ascontiguousarray(C0.reshape(batch, M, N))).cuda() if C0 is not None else \
+        torch.full((batch, M, N), float("nan"), device="cuda")
+    d = L.chai_gemm_desc(prec, 0, 0, 0, M, N, K, a.data_ptr(), K, b.data_ptr(), N, c.data_ptr(), N, alpha, beta,
+                         batch, M * K, K * N, M * N)
+    L.check(L.lib().chai_cuda_gemm(dev.ctx, C.byref(d)), dev.ctx)
+    L.check(L.lib().chai_cuda_synchronize(dev.ctx), dev.ctx)
+    return c.cpu().numpy().reshape(A.shape[:-2] + (M, N))
+
+
+def norm_err(Cg, A, B):
+    C64 = oracle.gemm_f64(A, B)
+    bound = np.abs(A).astype(np.float64) @ np.abs(B).astype(np.float64)
+    return float(np.max(np.abs(Cg.astype(np.float64) - C64) / np.maximum(bound, 1e-300)))
+
+
+SHAPES = [(128, 256, 64), (200, 300, 100), (512, 512, 512), (256, 384, 2048), (1, 17, 9)]
+
+
+@pytest.mark.parametrize("prec", [L.GEMM_FP32, L.GEMM_BF16, L.GEMM_TF32, L.GEMM_BF16X3, L.GEMM_BF16X6])
+@pytest.mark.parametrize("shape", SHAPES)
+def test_gemm_precision_vs_fp64(chai_dev, prec, shape):
+    M, N, K = shape
+    A = oracle.rng_fill(M * K, seed=1, limits=(-1.0, 1.0)).reshape(M, K)
+    B = oracle.rng_fill(K * N, seed=2, limits=(-1.0, 1.0)).reshape(K, N)
+    Cg = run_gemm(chai_dev, A, B, prec)
+    e = norm_err(Cg, A, B)
+    if prec == L.GEMM_BF16X6:
+        e32 = norm_err(run_gemm(chai_dev, A, B, L.GEMM_FP32), A, B)
+        assert e <= 4 * e32 + 2.0 ** -22, (e, e32)
+    else:
+        assert e <= BOUND[prec], e
+
+
+@pytest.mark.parametrize("prec", [L.GEMM_BF16, L.GEMM_TF32, L.GEMM_BF16X3, L.GEMM_BF16X6])
+def test_gemm_sentinel(chai_dev, prec):
+    """A = B = 1: every entry of C equals K exactly (sentinel check)."""
+    M, N, K = 256, 512, 768
+    Cg = run_gemm(chai_dev, np.ones((M, K), np.float32), np.ones((K, N), np.float32), prec)
+    assert np.all(Cg == K)
+
+
+@pytest.mark.parametrize("prec", [L.GEMM_BF16X3, L.GEMM_TF32])
+def test_gemm_alpha_beta_batch(chai_dev, prec):
+    """C = alpha A B + beta C over a strided batch (matmulG over vector slots)."""
+    rng = np.random.default_rng(9)
+    batch, M, N, K = 3, 130, 260, 96
+    A = rng.uniform(-1, 1, (batch, M, K)).astype(np.float32)
+    B = rng.uniform(-1, 1, (batch, K, N)).astype(np.float32)
+    C0 = rng.uniform(-1, 1, (batch, M, N)).astype(np.float32)
+    Cg = run_gemm(chai_dev, A, B, prec, alpha=0.5, beta=-2.0, C0=C0)
+    for i in range(batch):
+        want = 0.5 * oracle.gemm_f64(A[i], B[i]) - 2.0 * C0[i].astype(np.float64)
+        bound = 0.5 * (np.abs(A[i]).astype(np.float64) @ np.abs(B[i])) + 2.0 * np.abs(C0[i])
+        assert np.max(np.abs(Cg[i] - want) / bound) <= BOUND[prec]
+
+
+@pytest.mark.parametrize("prec", [L.GEMM_FP32, L.GEMM_BF16X6])
+def test_gemm_paranoid_l1(chai_dev, prec):
+    """The reference autotuner's paranoid check (EvergreenMatmulMM.cpp:
+    945-1040): inputs uniform on [0, 1), L1 distance to the CPU double result
+    below 1 (devspec.cfg Paranoid=1 on GPUs) and the mean of C within 10% of
+    K/4.  An FP32-level check, so it applies to fp32 and bf16x6."""
+    rng = np.random.default_rng(3)
+    n = 128
+    A = rng.uniform(0, 1, (n, n)).astype(np.float32)
+    B = rng.uniform(0, 1, (n, n)).astype(np.float32)
+    Cg = run_gemm(chai_dev, A, B, prec)
+    assert np.abs(Cg - oracle.gemm_f64(A, B)).sum() < 1.0
+    assert abs(Cg.mean() - 0.25 * n) / (0.25 * n) < 0.1
