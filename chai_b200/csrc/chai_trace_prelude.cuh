@@ -75,6 +75,66 @@ __device__ __forceinline__ void block_sum(double (&v)[NRED])
     }
 }
 
+// --------------------------------------------------------- stencil tiles
+// Tensor map passed by value to a stencil kernel (layout of CUtensorMap).
+struct __align__(64) Tmap { unsigned long long opaque[16]; };
+
+__device__ __forceinline__ unsigned smem_u32(const void* p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// 3-D tiled TMA load (x = innermost, 16-byte aligned) into shared memory
+__device__ __forceinline__ void tma_load_3d(void* dst, const Tmap* map, unsigned long long* bar, int x, int y, int z)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+                 ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
+// Bounded wait for phase `parity`: gives up after 2 s, sets *status and
+// returns false (the tile is then skipped; nothing waits forever).
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, int* status)
+{
+    unsigned long long t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (;;) {
+        unsigned ok;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(ok)
+                     : "r"(smem_u32(bar)), "r"(parity), "r"(1000u)
+                     : "memory");
+        if (ok) return true;
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > 2000000000ull) {
+            atomicExch(status, 201);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ long long wrapi(long long v, long long n)
+{
+    v %= n;
+    return v < 0 ? v + n : v;
+}
+
 }  // namespace chai_k
 
 #endif

@@ -69,8 +69,14 @@ void ktime_begin(chai_cuda_ctx* ctx, const char* name, cudaEvent_t* ev)
     (void)name;
     ev[0] = ev[1] = nullptr;
     if (!ctx->kernel_timing) return;
-    cudaEventCreate(&ev[0]);
-    cudaEventCreate(&ev[1]);
+    for (int k = 0; k < 2; k++) {
+        if (!ctx->event_pool.empty()) {
+            ev[k] = ctx->event_pool.back();
+            ctx->event_pool.pop_back();
+        } else {
+            cudaEventCreate(&ev[k]);
+        }
+    }
     cudaEventRecord(ev[0], ctx->stream);
 }
 
@@ -219,6 +225,9 @@ int chai_cuda_shutdown(chai_cuda_ctx* ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->tuner.reset();
     ctx->jit.reset();
+    for (auto& kv : ctx->kstats)
+        for (auto& p : kv.second.pending) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
+    for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     for (auto& kv : ctx->buffers)
         if (kv.second.owned && kv.second.ptr) cudaFree(kv.second.ptr);
     ctx->buffers.clear();
@@ -243,8 +252,8 @@ int chai_cuda_kernel_stats(chai_cuda_ctx* ctx, const char* name, double* total_m
         cudaEventElapsedTime(&ms, p.first, p.second);
         st.ms += ms;
         st.launches++;
-        cudaEventDestroy(p.first);
-        cudaEventDestroy(p.second);
+        ctx->event_pool.push_back(p.first);
+        ctx->event_pool.push_back(p.second);
     }
     st.pending.clear();
     if (total_ms) *total_ms = st.ms;

@@ -58,6 +58,7 @@ struct chai_cuda_ctx {
     bool kernel_timing = false;
     struct KStat { double ms = 0; uint64_t launches = 0; std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending; };
     std::map<std::string, KStat> kstats;
+    std::vector<cudaEvent_t> event_pool;
 };
 
 namespace chai {

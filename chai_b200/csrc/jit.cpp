@@ -66,6 +66,15 @@ int Jit::get(const std::string& body, const char* name, void** fn)
 {
     int st = compile_only_ ? CHAI_OK : resolve();
     if (st) return st;
+    // the prelude is fixed for the life of the library: key on the body only
+    uint64_t h = fnv1a64(body.data(), body.size());
+    h = fnv1a64(name, strlen(name), h);
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = functions_.find(h);
+    if (it != functions_.end()) {
+        *fn = it->second;
+        return CHAI_OK;
+    }
     std::string src;
     src.reserve(body.size() + 32768);
     src += kChaiRngSrc;
@@ -75,18 +84,12 @@ int Jit::get(const std::string& body, const char* name, void** fn)
     src += kChaiTracePreludeSrc;
     src += "\n";
     src += body;
-    uint64_t h = fnv1a64(src.data(), src.size());
-    h = fnv1a64(name, strlen(name), h);
-    std::lock_guard<std::mutex> g(mu_);
-    auto it = functions_.find(h);
-    if (it != functions_.end()) {
-        *fn = it->second;
-        return CHAI_OK;
-    }
+    // on-disk cache entries are keyed by the whole source (prelude included)
+    const uint64_t hdisk = fnv1a64(name, strlen(name), fnv1a64(src.data(), src.size()));
     std::vector<char> cubin;
     const char* dir = compile_only_ ? nullptr : ctx_->cfg.jit_cache.empty() ? getenv("CHAI_JIT_CACHE") : ctx_->cfg.jit_cache.c_str();
     if (dir && *dir) {
-        std::ifstream f(cache_path(dir, h), std::ios::binary);
+        std::ifstream f(cache_path(dir, hdisk), std::ios::binary);
         if (f) cubin.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
     }
     if (cubin.empty()) {
@@ -117,7 +120,7 @@ int Jit::get(const std::string& body, const char* name, void** fn)
             return CHAI_OK;
         }
         if (dir && *dir) {
-            std::ofstream f(cache_path(dir, h), std::ios::binary);
+            std::ofstream f(cache_path(dir, hdisk), std::ios::binary);
             if (f) f.write(cubin.data(), (std::streamsize)cubin.size());
         }
     }

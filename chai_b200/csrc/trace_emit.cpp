@@ -1,5 +1,6 @@
 // Code emission for trace kernel groups, linear-algebra lowering and
 // read-backs (second half of the trace translator, see trace.cpp).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -59,10 +60,30 @@ static std::string literal(double v, int prec)
 }
 
 struct KArg {
-    enum { PTR, I64 } kind;
-    void* ptr;
+    enum { PTR, I64, REF } kind;
+    void* ptr;        // PTR: the device pointer passed; REF: address of the by-value argument
     long long v;
 };
+
+typedef CUresult (*PFN_encodeTiledT)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                      const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiledT tensor_map_encoder()
+{
+    static PFN_encodeTiledT fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_encodeTiledT>(p);
+    }
+    return fn;
+}
+
+// stencil tile geometry (outputs per CTA: TX x TY; halo: PX columns, R rows)
+constexpr int ST_TX = 128, ST_TY = 16, ST_PX = 4;
 
 int Translator::emit_group(const std::vector<int>& roots)
 {
@@ -75,7 +96,7 @@ int Translator::emit_group(const std::vector<int>& roots)
     }
     const long long n = (long long)(W * H);
     if (n == 0) return CHAI_OK;
-    const bool vec = (n % 4) == 0;
+    bool vec = (n % 4) == 0;
     std::set<int> root_set(roots.begin(), roots.end());
 
     // body nodes in dependency order; loads for values computed elsewhere
@@ -100,6 +121,67 @@ int Translator::emit_group(const std::vector<int>& roots)
         body.push_back(i);
     };
     for (int r : roots) dfs(r);
+
+    // Constant-offset stencil gathers -- the reference's "eligible gather"
+    // (jitast/AstGather.cpp:90-195), which it reads through image2d_t:
+    // gather{1,2}_floor(A, X + cx [, Y + cy]) where X, Y are the iteration's own
+    // index arrays (f32, f64 or i32) and A has the iteration's shape.  When every
+    // gather of the group is one, the group runs as 2-D tiles of TX x TY outputs
+    // whose source tile plus halo is staged in shared memory: by one TMA load for
+    // interior tiles, by wrapped (periodic) loads for border tiles.
+    struct Sten { int src, cx, cy; };
+    std::map<int, Sten> sten;
+    std::vector<int> srcs;
+    int R = 0;
+    bool mode2d = W >= 16 && H >= 4 && W < (1u << 24) && H < (1u << 24) && S <= 65535;
+    bool any_gather = false;
+    std::function<bool(int, int, long long&)> offset_of = [&](int x, int dim, long long& off) -> bool {
+        const Node& nx = nodes_[x];
+        if (nx.prec != CHAI_F32 && nx.prec != CHAI_F64 && nx.prec != CHAI_I32) return false;
+        if (nx.kind == Node::CONVERT) return offset_of(nx.kids[0], dim, off);
+        if (nx.kind == Node::INDEX) {
+            off = 0;
+            return nx.dim == dim && nx.W == W && nx.H == H;
+        }
+        if (nx.kind == Node::OP && (nx.op == 11 || nx.op == 14) && nx.kids.size() == 2) {
+            auto ilit = [&](int k, long long& c) {
+                const Node& sn = nodes_[k];
+                if (sn.kind != Node::SCALAR || sn.scalar != std::floor(sn.scalar) || std::fabs(sn.scalar) > 4) return false;
+                c = (long long)sn.scalar;
+                return true;
+            };
+            long long c, o;
+            if (ilit(nx.kids[1], c) && offset_of(nx.kids[0], dim, o)) {
+                off = nx.op == 11 ? o + c : o - c;
+                return true;
+            }
+            if (nx.op == 11 && ilit(nx.kids[0], c) && offset_of(nx.kids[1], dim, o)) {
+                off = o + c;
+                return true;
+            }
+        }
+        return false;
+    };
+    size_t tile_bytes = 0;
+    for (int i : body) {
+        const Node& nd = nodes_[i];
+        if (nd.kind != Node::GATHER) continue;
+        any_gather = true;
+        const Node& a = nodes_[nd.kids[0]];
+        long long cx = 0, cy = 0;
+        bool ok = a.W == W && a.H == H && offset_of(nd.kids[1], 0, cx) &&
+                  (nd.op == 40 || offset_of(nd.kids[2], 1, cy)) && std::llabs(cx) <= ST_PX && std::llabs(cy) <= 4;
+        if (!ok) { mode2d = false; break; }
+        sten[i] = Sten{nd.kids[0], (int)cx, (int)cy};
+        if (std::find(srcs.begin(), srcs.end(), nd.kids[0]) == srcs.end()) srcs.push_back(nd.kids[0]);
+        R = std::max(R, (int)std::llabs(cy));
+    }
+    for (int src : srcs) tile_bytes += (size_t)(ST_TY + 2 * R) * (ST_TX + 2 * ST_PX) * prec_bytes(nodes_[src].prec);
+    mode2d = mode2d && any_gather && srcs.size() <= 2 && tile_bytes <= 40 * 1024;
+    if (!mode2d) sten.clear();
+    const int SH = ST_TY + 2 * R, SW = ST_TX + 2 * ST_PX;
+    const bool use_tma = mode2d && (W % 4) == 0;
+    std::vector<CUtensorMap> maps(srcs.size());
 
     std::ostringstream os;
     std::vector<KArg> args;
@@ -139,19 +221,67 @@ int Translator::emit_group(const std::vector<int>& roots)
             args.push_back({KArg::PTR, nd.dev, 0});
         }
     }
-    os << ", double* __restrict__ partials)\n{\n";
+    os << ", double* __restrict__ partials";
+    if (mode2d) {
+        os << ", int* __restrict__ status";
+        for (size_t k = 0; k < srcs.size(); k++) os << ", const __grid_constant__ chai_k::Tmap tm" << k;
+    }
+    os << ")\n{\n";
     os << "  using namespace chai_ops; using namespace chai_rng;\n";
-    os << "  const int slot = blockIdx.y;\n";
     if (nred) os << "  double red[" << nred << "] = {0};\n";
-    os << "  const long long nchunk = (n + 3) >> 2;\n";
-    os << "  for (long long c = (long long)blockIdx.x * 256 + threadIdx.x; c < nchunk; "
-          "c += (long long)gridDim.x * 256) {\n";
-    os << "    const long long e0 = c << 2;\n";
-    if (!vec) os << "    bool ok[4]; for (int j = 0; j < 4; j++) ok[j] = e0 + j < n;\n";
-    if (need_xy)
-        os << "    long long xx[4], yy[4]; { const long long y0 = e0 / W, x0 = e0 - y0 * W; "
-              "for (int j = 0; j < 4; j++) { long long x = x0 + j, y = y0; while (x >= W) { x -= W; y++; } "
-              "xx[j] = x; yy[j] = y; } }\n";
+    if (!mode2d) {
+        os << "  const int slot = blockIdx.y;\n";
+        os << "  const long long nchunk = (n + 3) >> 2;\n";
+        os << "  for (long long c = (long long)blockIdx.x * 256 + threadIdx.x; c < nchunk; "
+              "c += (long long)gridDim.x * 256) {\n";
+        os << "    const long long e0 = c << 2;\n";
+        if (!vec) os << "    bool ok[4]; for (int j = 0; j < 4; j++) ok[j] = e0 + j < n;\n";
+        if (need_xy)
+            os << "    long long xx[4], yy[4]; { const long long y0 = e0 / W, x0 = e0 - y0 * W; "
+                  "for (int j = 0; j < 4; j++) { long long x = x0 + j, y = y0; while (x >= W) { x -= W; y++; } "
+                  "xx[j] = x; yy[j] = y; } }\n";
+    } else {
+        vec = (W % 4) == 0;
+        os << "  const int slot = blockIdx.z;\n";
+        os << "  const long long tx0 = (long long)blockIdx.x * " << ST_TX << ", ty0 = (long long)blockIdx.y * " << ST_TY
+           << ";\n";
+        for (size_t k = 0; k < srcs.size(); k++)
+            os << "  __shared__ __align__(128) " << ctype_of(nodes_[srcs[k]].prec) << " tile" << k << "[" << SH * SW
+               << "];\n";
+        os << "  __shared__ __align__(8) unsigned long long tbar;\n";
+        os << "  bool tile_ok = true;\n";
+        os << "  {\n    const bool interior = " << (use_tma ? "true" : "false") << " && tx0 - " << ST_PX
+           << " >= 0 && tx0 + " << ST_TX + ST_PX << " <= W && ty0 - " << R << " >= 0 && ty0 + " << ST_TY + R
+           << " <= H;\n";
+        os << "    if (interior) {\n      if (threadIdx.x == 0) chai_k::mbar_init(&tbar, 1);\n      __syncthreads();\n"
+              "      if (threadIdx.x == 0) {\n        chai_k::mbar_expect_tx(&tbar, " << tile_bytes << "u);\n";
+        for (size_t k = 0; k < srcs.size(); k++) {
+            const Node& a = nodes_[srcs[k]];
+            os << "        chai_k::tma_load_3d(tile" << k << ", &tm" << k << ", &tbar, (int)(tx0 - " << ST_PX
+               << "), (int)(ty0 - " << R << "), slot % " << a.slots << ");\n";
+        }
+        os << "      }\n      tile_ok = chai_k::mbar_wait_bounded(&tbar, 0, status);\n    } else {\n";
+        for (size_t k = 0; k < srcs.size(); k++) {
+            const Node& a = nodes_[srcs[k]];
+            const long long sl = a.slots > 1 ? (long long)(a.W * a.H) : 0;
+            int gsrc = -1;   // the pointer parameter of a gather reading this source
+            for (auto& kv : sten)
+                if (kv.second.src == srcs[k]) { gsrc = kv.first; break; }
+            os << "      for (int idx = threadIdx.x; idx < " << SH * SW << "; idx += 256) { const int r = idx / " << SW
+               << ", c = idx - r * " << SW << "; tile" << k << "[idx] = g" << gsrc << "[(long long)(slot % "
+               << a.slots << ") * " << sl << " + chai_k::wrapi(ty0 - " << R << " + r, H) * W + chai_k::wrapi(tx0 - "
+               << ST_PX << " + c, W)]; }\n";
+        }
+        os << "    }\n    __syncthreads();\n  }\n";
+        os << "  const int lx = (threadIdx.x & 31) * 4;\n";
+        os << "  for (int rr = 0; rr < " << ST_TY / 8 << " && tile_ok; rr++) {\n";
+        os << "    const int ly = (threadIdx.x >> 5) + 8 * rr;\n";
+        os << "    const long long yv = ty0 + ly, xv = tx0 + lx;\n";
+        os << "    if (yv >= H || xv >= W) continue;\n";
+        os << "    const long long e0 = yv * W + xv;\n";
+        os << "    bool ok[4]; long long xx[4], yy[4];\n";
+        os << "    for (int j = 0; j < 4; j++) { ok[j] = xv + j < W; xx[j] = xv + j; yy[j] = yv; }\n";
+    }
     const double two_pi = 2.0 * ctx_->cfg.rng_pi;
     const int layout = ctx_->cfg.rng_layout;
     for (int i : body) {
@@ -206,6 +336,13 @@ int Translator::emit_group(const std::vector<int>& roots)
                 break;
             }
             case Node::GATHER: {
+                if (sten.count(i)) {
+                    const Sten& g = sten[i];
+                    const int k = (int)(std::find(srcs.begin(), srcs.end(), g.src) - srcs.begin());
+                    os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = tile" << k << "[(ly + " << R + g.cy << ") * "
+                       << SW << " + lx + j + " << ST_PX + g.cx << "];\n";
+                    break;
+                }
                 const Node& a = nodes_[nd.kids[0]];
                 const long long sl = a.slots > 1 ? (long long)(a.W * a.H) : 0;
                 os << "    for (int j = 0; j < 4; j++) { const long long base = (long long)(slot % " << a.slots
@@ -339,8 +476,12 @@ int Translator::emit_group(const std::vector<int>& roots)
     os << "  }\n";
     if (nred) {
         os << "  chai_k::block_sum<" << nred << ", 256>(red);\n";
-        os << "  if (threadIdx.x == 0) for (int k = 0; k < " << nred << "; k++) partials[((long long)k * gridDim.y + "
-              "slot) * gridDim.x + blockIdx.x] = red[k];\n";
+        if (!mode2d)
+            os << "  if (threadIdx.x == 0) for (int k = 0; k < " << nred << "; k++) partials[((long long)k * gridDim.y + "
+                  "slot) * gridDim.x + blockIdx.x] = red[k];\n";
+        else
+            os << "  if (threadIdx.x == 0) for (int k = 0; k < " << nred << "; k++) partials[((long long)k * gridDim.z + "
+                  "slot) * (gridDim.x * gridDim.y) + blockIdx.y * gridDim.x + blockIdx.x] = red[k];\n";
     }
     os << "}\n";
 
@@ -351,25 +492,61 @@ int Translator::emit_group(const std::vector<int>& roots)
     if (st) return st;
     if (dry_) return CHAI_OK;
     const long long nchunk = (n + 3) / 4;
-    long long gx = (nchunk + 255) / 256;
+    long long gx = (nchunk + 255) / 256, gy = 1;
     const long long cap = std::max<long long>(1, (long long)ctx_->sm_count * 8 / (long long)S);
     gx = std::min(gx, cap);
+    if (mode2d) {
+        gx = ((long long)W + ST_TX - 1) / ST_TX;
+        gy = ((long long)H + ST_TY - 1) / ST_TY;
+        if (gy > 65535) return fail(CHAI_ERR_UNSUPPORTED, "stencil grid too tall");
+    }
+    const long long nblocks = gx * gy;
     double* partials = nullptr;
     if (nred) {
-        st = ensure_scratch(ctx_, (size_t)nred * S * gx * sizeof(double));
+        st = ensure_scratch(ctx_, (size_t)nred * S * nblocks * sizeof(double));
         if (st) return st;
         partials = static_cast<double*>(ctx_->scratch);
     }
+    const size_t n_checked = args.size();
     args.push_back({KArg::PTR, partials, 0});
-    for (size_t k = 0; k + 1 < args.size(); k++)
+    if (mode2d) {
+        args.push_back({KArg::PTR, ctx_->status_word, 0});
+        for (size_t k = 0; k < srcs.size(); k++) {
+            memset(&maps[k], 0, sizeof(CUtensorMap));
+            if (use_tma) {
+                const Node& a = nodes_[srcs[k]];
+                PFN_encodeTiledT enc = tensor_map_encoder();
+                if (!enc) return fail(CHAI_ERR_NO_DEVICE, "cuTensorMapEncodeTiled unavailable");
+                const CUtensorMapDataType dt = a.prec == CHAI_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                               : a.prec == CHAI_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                               : a.prec == CHAI_I32 ? CU_TENSOR_MAP_DATA_TYPE_INT32
+                                                                    : CU_TENSOR_MAP_DATA_TYPE_UINT32;
+                const size_t eb = prec_bytes(a.prec);
+                cuuint64_t dims[3] = {(cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.slots};
+                cuuint64_t strides[2] = {(cuuint64_t)(a.W * eb), (cuuint64_t)(a.W * a.H * eb)};
+                cuuint32_t box[3] = {(cuuint32_t)SW, (cuuint32_t)SH, 1};
+                cuuint32_t estr[3] = {1, 1, 1};
+                if ((reinterpret_cast<uintptr_t>(a.dev) & 15) != 0)
+                    return fail(CHAI_ERR_INVALID, "stencil source not 16-byte aligned");
+                CUresult r = enc(&maps[k], dt, 3, a.dev, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                if (r != CUDA_SUCCESS) return fail(CHAI_ERR_INVALID, "stencil tensor map encoding failed");
+            }
+            args.push_back({KArg::REF, &maps[k], 0});
+        }
+    }
+    for (size_t k = 0; k < n_checked; k++)
         if (args[k].kind == KArg::PTR && !args[k].ptr)
             return fail(CHAI_ERR_INVALID, "trace kernel operand without storage");
     std::vector<void*> ptrs(args.size());
     for (size_t k = 0; k < args.size(); k++)
-        ptrs[k] = args[k].kind == KArg::PTR ? (void*)&args[k].ptr : (void*)&args[k].v;
+        ptrs[k] = args[k].kind == KArg::PTR ? (void*)&args[k].ptr
+                  : args[k].kind == KArg::REF ? args[k].ptr : (void*)&args[k].v;
     cudaEvent_t kev[2];
     ktime_begin(ctx_, "trace", kev);
-    st = ctx_->jit->launch(fn, dim3((unsigned)gx, S, 1), dim3(256, 1, 1), 0, ptrs.data());
+    const dim3 grid = mode2d ? dim3((unsigned)gx, (unsigned)gy, S) : dim3((unsigned)gx, S, 1);
+    st = ctx_->jit->launch(fn, grid, dim3(256, 1, 1), 0, ptrs.data());
     if (st) return st;
     ktime_end(ctx_, "trace", kev);
     kernels_launched++;
@@ -383,7 +560,7 @@ int Translator::emit_group(const std::vector<int>& roots)
             precs.push_back(nd.prec);
             scales.push_back(nd.op == 131 ? 1.0 / (double)n : 1.0);
         }
-        st = launch_combine(ctx_, partials, (int)gx, nred, (int)S, outs.data(), precs.data(), scales.data());
+        st = launch_combine(ctx_, partials, (int)nblocks, nred, (int)S, outs.data(), precs.data(), scales.data());
         if (st) return st;
         kernels_launched++;
     }

@@ -297,3 +297,31 @@ def test_kirsch_trace_bit_exact(ch):
     A = ch.make2(img)
     got = ch.Arrayf32(kirsch_expr(ch, A, W, H)).read2()
     assert np.array_equal(got, oracle.kirsch(img))
+
+
+@pytest.mark.parametrize("shape", [(96, 128), (130, 517), (16, 16), (300, 1024)])
+def test_stencil_tiles_bit_exact(ch, shape):
+    """Constant-offset gathers run as 2-D shared-memory tiles (TMA for
+    interior tiles when W % 4 == 0, wrapped loads at borders and otherwise);
+    the periodic wrap must match the interpreter exactly at every border."""
+    H, W = shape
+    rng = np.random.default_rng(W + H)
+    img = rng.standard_normal((H, W)).astype(np.float32)
+    A = ch.make2(img)
+    X, Y = ch.index_f32(0, W, H), ch.index_f32(1, W, H)
+    e = (ch.gather2_floor(A, X + f32(2), Y - f32(1)) * f32(3) - ch.gather2_floor(A, X - f32(1), Y + f32(3))
+         + ch.gather1_floor(A, X + f32(4)))
+    got = ch.Arrayf32(e).read2()
+    roll = lambda dx, dy: np.roll(np.roll(img, -dy, axis=0), -dx, axis=1)
+    want = roll(2, -1) * f32(3) - roll(-1, 3) + roll(4, 0)
+    assert np.array_equal(got, want)
+
+
+def test_stencil_with_reduction(ch):
+    H, W = 256, 512
+    img = oracle.rng_fill(W * H, seed=9).reshape(H, W)
+    A = ch.make2(img)
+    X, Y = ch.index_f32(0, W, H), ch.index_f32(1, W, H)
+    s = float(ch.Arrayf64(ch.sum(ch.convert_f64(ch.gather2_floor(A, X + f32(1), Y) - A))).read_scalar())
+    want = (np.roll(img, -1, axis=1).astype(np.float32) - img).astype(np.float64).sum()
+    assert abs(s - want) <= 1e-9 * max(1.0, np.abs(img).sum())

@@ -69,7 +69,21 @@ def test_kirsch_trace_is_one_kernel_with_gathers():
     stmts, (A, K) = record(build)
     st, src = source(stmts, [(K.var, 4, 64, 64, 1, 0, 8)])
     assert st == 0, src
-    assert src.count("__global__") == 1 and src.count("gather_index") == 16
+    # every gather is a constant-offset stencil: one 2-D tiled kernel, the
+    # source tile staged in shared memory by TMA (wrapped loads at borders)
+    assert src.count("__global__") == 1 and src.count("gather_index") == 0
+    assert "tma_load_3d(tile0" in src and src.count("tile0[(ly") == 8
+
+
+def test_data_dependent_gather_stays_generic():
+    def build():
+        A = ch._ARR[4](_raw=([ch._bc(L.BC_MEMORY, buffer=7), ch._sc(1), ch._sc(64), ch._sc(64), ch._op(66)], 64, 64, 1))
+        X = ch._ARR[4](_raw=([ch._bc(L.BC_MEMORY, buffer=9), ch._sc(1), ch._sc(64), ch._sc(64), ch._op(66)], 64, 64, 1))
+        return A, X, ch.Arrayf32(ch.gather2_floor(A, X, ch.index_f32(1, 64, 64)))
+    stmts, (A, X, G) = record(build)
+    st, src = source(stmts, [(G.var, 4, 64, 64, 1, 0, 8)])
+    assert st == 0, src
+    assert src.count("gather_index") == 2 and "tma_load_3d(" not in src.split("chai_group")[1]
 
 
 def test_gather_of_value_computed_in_trace_splits_kernels():
