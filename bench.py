@@ -424,7 +424,65 @@ def run_gemv(args, L, ctx, stream):
     }
 
 
-WORKLOADS = {"gemm": run_gemm, "mc": run_mc, "kirsch": run_kirsch, "gemv": run_gemv}
+def many_lengths(n=64, seed=7):
+    """Trace lengths log-uniform in [2^12, 2^22], rounded to multiples of 4."""
+    rng = np.random.default_rng(seed)
+    return [int(4 * round(2.0 ** u / 4)) for u in rng.uniform(12, 22, n)]
+
+
+def run_mc_many(args, L, ctx, stream):
+    import torch
+    import chai_b200.api as ch
+    Ls = many_lengths()
+    total = sum(Ls)
+
+    def mc1(seed, W):
+        return ch.Arrayf32(mc_expr(ch, ch.RNGf32(ch.RNG_PHILOX, seed), W, 1))
+    traces = [ch.record(lambda s=s, W=W: mc1(42 + s, W))[0] for s, W in enumerate(Ls)]
+    descs = []
+    ptrs = (C.POINTER(L.chai_trace_desc) * len(traces))()
+    for i, st in enumerate(traces):
+        d, k = ch.build_desc(st)
+        descs.append((d, k))
+        ptrs[i] = C.pointer(d)
+    res = (C.c_double * len(traces))()
+
+    def step():
+        L.check(L.lib().chai_cuda_evaluate_many(ctx, ptrs, len(traces), res), ctx)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    kstats(L, ctx, "many")
+    with Clocks(torch.cuda.current_device()) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+        wall = (time.perf_counter() - t0) * 1e3 / args.steps
+    k_ms, k_n = kstats(L, ctx, "many")
+    kern = k_ms / k_n if k_n else wall
+
+    def e2e():      # record 64 traces through the front end and evaluate them
+        tr = [ch.record(lambda s=s, W=W: mc1(42 + s, W))[0] for s, W in enumerate(Ls)]
+        return ch.evaluate_many(tr)
+    e2e()
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.steps, 5))):
+        e2e()
+    e_ms = (time.perf_counter() - t0) * 1e3 / max(1, min(args.steps, 5))
+    return {
+        "metric": "trace throughput (64 uneven MC traces, one persistent launch)", "unit": "Gnormals/s",
+        "value": total / (kern * 1e-3) / 1e9, "ms_per_step": kern, "dtype": "f32", "higher_is_better": True,
+        "config": {"workload": "64 MC traces, lengths log-uniform in [2^12, 2^22] (seed 7), one persistent kernel "
+                               "+ combine captured in a CUDA graph", "normals": total,
+                   "host_ms_per_call": wall, "l2": "no HBM inputs (RNG in registers)"},
+        "e2e": {"value": total / (e_ms * 1e-3) / 1e9, "unit": "Gnormals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8 * len(Ls)},
+        "roofline": None, "clocks": clk.summary(), "gpu_launches": args.steps * 2,
+    }
+
+
+WORKLOADS = {"gemm": run_gemm, "mc": run_mc, "kirsch": run_kirsch, "gemv": run_gemv, "mc-many": run_mc_many}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -451,6 +509,11 @@ def run_reference(args, steps=None):
             unit, metric = "TFLOP/s", "GEMM TFLOP/s at err vs FP32"
             conv = lambda ms: 2.0 * n ** 3 / (ms * 1e-3) / 1e12
             sample = "interpreter matmul 512^3 f32 (double accumulation), inputs via make2"
+        elif wl == "mc-many":
+            Ls = [max(4, L // 16) for L in many_lengths()]
+            cmd = None
+            unit, metric = "Gnormals/s", "trace throughput (64 uneven MC traces, one persistent launch)"
+            sample = "64 sequential interpreter MC traces, lengths 1/16 of the GPU workload's"
         elif wl == "mc":
             W, H = 1024, 512
             cmd = [str(drv), "mc_rng", str(W), str(H)]
@@ -473,6 +536,16 @@ def run_reference(args, steps=None):
             conv = lambda ms: (m * n + m + n) * 4 / (ms * 1e-3) / 1e9
             sample = "interpreter matmul(matrix, vector) 4096x4096 f32"
         for _ in range(steps):
+            if wl == "mc-many":     # the reference runs uneven traces one dispatch at a time
+                ms_sum = 0.0
+                for L in Ls:
+                    r = subprocess.run([str(drv), "mc_rng", str(L), "1"], capture_output=True, text=True, timeout=600)
+                    if r.returncode != 0:
+                        return {"impl": "reference", "unavailable": "ref_driver failed: " + r.stderr[-200:]}
+                    ms_sum += float(r.stdout.split("ms=")[1].split()[0])
+                times.append(ms_sum)
+                conv = lambda ms: sum(Ls) / (ms * 1e-3) / 1e9
+                continue
             r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
             if r.returncode != 0:
                 return {"impl": "reference", "unavailable": "ref_driver failed: " + r.stderr[-200:]}

@@ -596,3 +596,34 @@ def transpose(a):
 
 def matmul(a, b, c=None, alpha=1.0, beta=1.0):
     return _Matmul(a, b, c, alpha, beta)
+
+
+# ------------------------------------------------------------------ many traces
+
+def record(build):
+    """Record the statements `build()` creates without evaluating them; returns
+    (statements, value of build()).  The statements form one trace."""
+    saved = _Client.pending
+    _Client.pending = []
+    try:
+        out = build()
+        stmts = [(v, ver, cells) for v, ver, cells, _ in _Client.pending]
+    finally:
+        _Client.pending = saved
+    return stmts, out
+
+
+def evaluate_many(traces):
+    """Evaluate many recorded traces that share one program (same bytecode
+    up to scalar values: shapes, seeds, literals) and end in a reduction; one
+    result per trace (chai_cuda_evaluate_many)."""
+    dev = vm()
+    keep = []
+    ptrs = (C.POINTER(L.chai_trace_desc) * len(traces))()
+    for i, stmts in enumerate(traces):
+        desc, k = build_desc(stmts)
+        keep.append((desc, k))
+        ptrs[i] = C.pointer(desc)
+    res = (C.c_double * len(traces))()
+    L.check(L.lib().chai_cuda_evaluate_many(dev.ctx, ptrs, len(traces), res), dev.ctx)
+    return np.frombuffer(res, dtype=np.float64).copy()

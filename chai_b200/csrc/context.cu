@@ -17,6 +17,8 @@
 
 namespace chai {
 
+void many_release(chai_cuda_ctx* ctx);
+
 int set_error(chai_cuda_ctx* ctx, int status, const std::string& msg)
 {
     if (ctx) {
@@ -223,6 +225,7 @@ int chai_cuda_shutdown(chai_cuda_ctx* ctx)
     if (!ctx) return CHAI_ERR_INVALID;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    many_release(ctx);
     ctx->tuner.reset();
     ctx->jit.reset();
     for (auto& kv : ctx->kstats)

@@ -130,6 +130,36 @@ int launch_reduce(chai_cuda_ctx* ctx, uint32_t op, uint32_t prec, const void* a,
     return launch_combine(ctx, partials, (int)gx, 1, (int)slots, outs, precs, scales);
 }
 
+// One block per trace: add the trace's tile partials (tiles [first, next first))
+// in tile order in FP64; mean divides by n; the result is rounded to the
+// reduction's precision and returned as a double.
+__global__ void __launch_bounds__(256) chai_many_combine(const long long* __restrict__ tab, int stride,
+                                                         const double* __restrict__ partials,
+                                                         double* __restrict__ out, int mean, int prec)
+{
+    const int t = blockIdx.x;
+    const long long ntiles = tab[0];
+    const int ntr = (int)tab[1];
+    const long long* row = tab + 2 + (long long)t * stride;
+    const long long first = row[3];
+    const long long last = t + 1 < ntr ? row[stride + 3] : ntiles;
+    double x = 0.0;
+    for (long long i = first + threadIdx.x; i < last; i += 256) x += partials[i];
+    x = block_sum_d<256>(x);
+    if (threadIdx.x == 0) {
+        if (mean) x /= (double)row[0];
+        if (prec == CHAI_F32) x = (double)(float)x;
+        out[t] = x;
+    }
+}
+
+int launch_many_combine(chai_cuda_ctx* ctx, const long long* tab, int stride, const double* partials, double* out,
+                        int ntr, int mean, int prec)
+{
+    chai_many_combine<<<ntr, 256, 0, ctx->stream>>>(tab, stride, partials, out, mean, prec);
+    return cudaGetLastError() == cudaSuccess ? CHAI_OK : CHAI_ERR_LAUNCH;
+}
+
 }  // namespace chai
 
 // ---------------------------------------------------------------------------

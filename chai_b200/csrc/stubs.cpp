@@ -25,13 +25,6 @@ using namespace chai;
 
 extern "C" {
 
-int chai_cuda_evaluate_many(chai_cuda_ctx* ctx, const chai_trace_desc* const* traces, size_t n, double* results)
-{
-    (void)traces; (void)n; (void)results;
-    if (!ctx) return CHAI_ERR_INVALID;
-    return set_error(ctx, CHAI_ERR_UNSUPPORTED, "evaluate_many not built");
-}
-
 int chai_cuda_tune(chai_cuda_ctx* ctx, const chai_gemm_key* key, int mode, chai_gemm_cfg* out)
 {
     if (!ctx || !key || !out) return CHAI_ERR_INVALID;

@@ -342,6 +342,50 @@ int Translator::resolve_var(const Node& v)
 
 // ----------------------------------------------------------- evaluate
 
+int Translator::parse_only(const chai_trace_desc* t)
+{
+    slots_ = t->num_traces ? t->num_traces : 1;
+    for (uint32_t i = 0; i < t->n_stmts; i++) {
+        const chai_stmt& s = t->stmts[i];
+        if (!s.cells || s.n_cells == 0) return fail(CHAI_ERR_INVALID, "empty statement");
+        int pos = (int)s.n_cells - 1;
+        const int root = parse(s, pos);
+        if (root < 0 || pos != -1) return fail(CHAI_ERR_INVALID, "malformed statement");
+        if (nodes_[root].kind == Node::READ) {
+            reads_.push_back(root);
+        } else {
+            assigned_[std::make_pair(s.lhs_variable, s.lhs_version)] = root;
+            latest_[s.lhs_variable] = root;
+            stmt_roots_.push_back(std::make_pair(s.lhs_variable, root));
+        }
+    }
+    return CHAI_OK;
+}
+
+int Translator::result_root() const
+{
+    if (stmt_roots_.empty()) return -1;
+    const int r = stmt_roots_.back().second;
+    return nodes_[r].kind == Node::REDUCE ? r : -1;
+}
+
+int Translator::read_result(double* out)
+{
+    const int r = result_root();
+    if (r < 0 || !nodes_[r].dev) return fail(CHAI_ERR_UNSUPPORTED, "trace has no reduction result");
+    const Node& n = nodes_[r];
+    unsigned char buf[8] = {0};
+    CHAI_CUDA_TRY(ctx_, cudaMemcpyAsync(buf, n.dev, prec_bytes(n.prec), cudaMemcpyDeviceToHost, ctx_->stream));
+    CHAI_CUDA_TRY(ctx_, cudaStreamSynchronize(ctx_->stream));
+    switch (n.prec) {
+        case CHAI_F32: { float v; memcpy(&v, buf, 4); *out = v; break; }
+        case CHAI_F64: { double v; memcpy(&v, buf, 8); *out = v; break; }
+        case CHAI_I32: { int v; memcpy(&v, buf, 4); *out = v; break; }
+        default: { unsigned v; memcpy(&v, buf, 4); *out = v; break; }
+    }
+    return CHAI_OK;
+}
+
 int Translator::run(const chai_trace_desc* t, const chai_buffer_binding* binds, size_t nb)
 {
     for (size_t i = 0; i < nb; i++) bindings_[binds[i].variable] = binds[i];

@@ -45,6 +45,12 @@ public:
     explicit Translator(chai_cuda_ctx* ctx, bool dry = false) : ctx_(ctx), dry_(dry) {}
     ~Translator();
     int run(const chai_trace_desc* t, const chai_buffer_binding* b, size_t nb);
+    // parse the statements only (no bindings, storage or launches)
+    int parse_only(const chai_trace_desc* t);
+    // root node of the last assignment when it is a reduction, else -1
+    int result_root() const;
+    // after run(): value of result_root() as a double (host)
+    int read_result(double* out);
     // scalar results of reductions that are statement roots (for evaluate_many)
     const std::vector<Node>& nodes() const { return nodes_; }
     // generated source of the last element kernel (diagnostics / tests)

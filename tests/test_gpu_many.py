@@ -1,0 +1,59 @@
+"""Many uneven traces in one persistent launch under a CUDA graph
+(chai_cuda_evaluate_many) against the same traces evaluated one at a time.
+
+Tolerance: results are the reductions rounded to f32 (as read_scalar returns
+them); the two paths add FP64 partials in different orders, so they may
+differ by one f32 ulp."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+f32 = np.float32
+
+
+def mc(ch, seed, W, H=1):
+    g = ch.RNGf32(ch.RNG_PHILOX, seed)
+    return ch.Arrayf32(ch.mean(ch.max(f32(100) * ch.exp(f32(0.03) + f32(0.2) * ch.rng_normal_make(g, W, H))
+                                      - f32(100), f32(0))))
+
+
+def close(a, b):
+    """Equal (including the +inf a u0 = 0 draw gives in the reference's
+    Box-Muller) or within two f32 ulps."""
+    return a == b or abs(a - b) <= 2 * np.spacing(np.float32(abs(b)))
+
+
+def lengths(n, seed=7):
+    rng = np.random.default_rng(seed)
+    return [int(4 * round(2.0 ** u / 4)) for u in rng.uniform(12, 22, n)]
+
+
+def test_many_uneven_mc_traces_match_single(chai_dev):
+    import chai_b200.api as ch
+    Ls = lengths(64)
+    traces = [ch.record(lambda L=L, s=s: mc(ch, 1000 + s, L))[0] for s, L in enumerate(Ls)]
+    got = ch.evaluate_many(traces)
+    again = ch.evaluate_many(traces)          # graph replay
+    assert np.array_equal(got, again)
+    for s, L in enumerate(Ls[:8] + Ls[-4:]):
+        idx = Ls.index(L)
+        want = float(mc(ch, 1000 + idx, L).read_scalar())
+        assert close(got[idx], want), (idx, got[idx], want)
+
+
+def test_many_changes_lengths_between_calls(chai_dev):
+    import chai_b200.api as ch
+    a = [ch.record(lambda L=L: mc(ch, 5, L))[0] for L in (4096, 8192, 65536)]
+    b = [ch.record(lambda L=L: mc(ch, 5, L))[0] for L in (1 << 20, 4096, 12)]
+    ra, rb = ch.evaluate_many(a), ch.evaluate_many(b)
+    for L, r in zip((1 << 20, 4096, 12), rb):
+        assert close(r, float(mc(ch, 5, L).read_scalar()))
+    assert ra[0] == rb[1]
+
+
+def test_many_falls_back_for_other_programs(chai_dev):
+    import chai_b200.api as ch
+    x = np.arange(1000, dtype=np.float32)
+    traces = [ch.record(lambda s=s: ch.Arrayf32(ch.sum(ch.make1(x * s))))[0] for s in (1, 2)]
+    r = ch.evaluate_many(traces)
+    assert np.allclose(r, [x.sum(), 2 * x.sum()])
