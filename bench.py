@@ -482,7 +482,80 @@ def run_mc_many(args, L, ctx, stream):
     }
 
 
-WORKLOADS = {"gemm": run_gemm, "mc": run_mc, "kirsch": run_kirsch, "gemv": run_gemv, "mc-many": run_mc_many}
+def grouped_shapes(count=4096, seed=11):
+    """M, N, K uniform over the multiples of 8 in [32, 512] (seed 11)."""
+    rng = np.random.default_rng(seed)
+    return [tuple(int(v) for v in rng.integers(4, 65, 3) * 8) for _ in range(count)]
+
+
+def run_grouped(args, L, ctx, stream):
+    import torch
+    shapes = grouped_shapes()
+    prec = GEMM_PREC[args.precision] if args.precision in GEMM_PREC else 3
+    if prec in (0, 1):
+        prec = 3
+    g = torch.Generator(device="cuda").manual_seed(3)
+    sa = sum(m * k for m, n, k in shapes)
+    sb = sum(k * n for m, n, k in shapes)
+    sc = sum(m * n for m, n, k in shapes)
+    A = torch.rand(sa, device="cuda", generator=g) * 2 - 1
+    B = torch.rand(sb, device="cuda", generator=g) * 2 - 1
+    Cm = torch.empty(sc, device="cuda")
+    arr = (L.chai_gemm_problem * len(shapes))()
+    oa = ob = oc = 0
+    for i, (m, n, k) in enumerate(shapes):
+        arr[i] = L.chai_gemm_problem(m, n, k, 0, A.data_ptr() + 4 * oa, B.data_ptr() + 4 * ob, Cm.data_ptr() + 4 * oc)
+        oa += m * k
+        ob += k * n
+        oc += m * n
+    flops = sum(2.0 * m * n * k for m, n, k in shapes)
+
+    def step():
+        L.check(L.lib().chai_cuda_gemm_grouped(ctx, prec, arr, len(shapes)), ctx)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    kstats(L, ctx, "gemm_grouped")
+    with Clocks(torch.cuda.current_device()) as clk:
+        ts = time_events(step, args.steps, stream)
+    ms = sum(ts) / len(ts)
+    k_ms, k_n = kstats(L, ctx, "gemm_grouped")
+    kern = k_ms / k_n if k_n else ms
+    # e2e: host operands in, results out
+    Ah, Bh = A.cpu().pin_memory(), B.cpu().pin_memory()
+    Ch = torch.empty(sc).pin_memory()
+
+    def e2e():
+        A.copy_(Ah, non_blocking=True)
+        B.copy_(Bh, non_blocking=True)
+        step()
+        Ch.copy_(Cm, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+    e2e()
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.steps, 5))):
+        e2e()
+    e_ms = (time.perf_counter() - t0) * 1e3 / max(1, min(args.steps, 5))
+    P, kind = peaks()
+    tensor_mult = TENSOR_MULT[prec]
+    ach = flops * tensor_mult / (kern * 1e-3) / 1e12
+    return {
+        "metric": "GEMM TFLOP/s at err vs FP32", "unit": "TFLOP/s", "value": flops / (ms * 1e-3) / 1e12,
+        "ms_per_step": ms, "dtype": args.precision if prec != 3 else "bf16x3", "higher_is_better": True,
+        "config": {"workload": "4096 grouped f32 GEMMs, M,N,K multiples of 8 in [32,512] (seed 11), one persistent "
+                               "tcgen05 launch", "problems": len(shapes), "useful_gflop": flops / 1e9},
+        "e2e": {"value": flops / (e_ms * 1e-3) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": 4 * (sa + sb),
+                "d2h_bytes_per_step": 4 * sc},
+        "roofline": {"bound": "tensor", "achieved": ach, "peak": P["bf16_tflops"], "unit": "TFLOP/s",
+                     "frac": ach / P["bf16_tflops"], "traffic": traffic("gemm_grouped"), "peak_source": kind,
+                     "kernel": "chai_gemm_tc_kernel (grouped)", "kernel_ms": kern},
+        "clocks": clk.summary(), "gpu_launches": args.steps * 3,
+    }
+
+
+WORKLOADS = {"gemm": run_gemm, "mc": run_mc, "kirsch": run_kirsch, "gemv": run_gemv, "mc-many": run_mc_many,
+             "grouped": run_grouped}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -509,6 +582,15 @@ def run_reference(args, steps=None):
             unit, metric = "TFLOP/s", "GEMM TFLOP/s at err vs FP32"
             conv = lambda ms: 2.0 * n ** 3 / (ms * 1e-3) / 1e12
             sample = "interpreter matmul 512^3 f32 (double accumulation), inputs via make2"
+        elif wl == "grouped":
+            cmd = None
+            unit, metric = "TFLOP/s", "GEMM TFLOP/s at err vs FP32"
+            sample = "interpreter matmul loop over the first 16 of the 4096 grouped problems"
+            shapes = grouped_shapes()[:16]
+            files = []
+            for i, (m, n, k) in enumerate(shapes):
+                rng.uniform(-1, 1, (m, k)).astype(np.float32).tofile(td + "/A%d" % i)
+                rng.uniform(-1, 1, (k, n)).astype(np.float32).tofile(td + "/B%d" % i)
         elif wl == "mc-many":
             Ls = [max(4, L // 16) for L in many_lengths()]
             cmd = None
@@ -536,6 +618,17 @@ def run_reference(args, steps=None):
             conv = lambda ms: (m * n + m + n) * 4 / (ms * 1e-3) / 1e9
             sample = "interpreter matmul(matrix, vector) 4096x4096 f32"
         for _ in range(steps):
+            if wl == "grouped":     # one interpreter matmul per problem
+                ms_sum = 0.0
+                for i, (m, n, k) in enumerate(shapes):
+                    r = subprocess.run([str(drv), "gemm_f32", str(m), str(n), str(k), td + "/A%d" % i, td + "/B%d" % i,
+                                        td + "/C"], capture_output=True, text=True, timeout=600)
+                    if r.returncode != 0:
+                        return {"impl": "reference", "unavailable": "ref_driver failed: " + r.stderr[-200:]}
+                    ms_sum += float(r.stdout.split("ms=")[1].split()[0])
+                times.append(ms_sum)
+                conv = lambda ms: sum(2.0 * m * n * k for m, n, k in shapes) / (ms * 1e-3) / 1e12
+                continue
             if wl == "mc-many":     # the reference runs uneven traces one dispatch at a time
                 ms_sum = 0.0
                 for L in Ls:

@@ -35,6 +35,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstring>
+#include <vector>
 
 #include "internal.h"
 
@@ -224,14 +226,75 @@ __device__ __forceinline__ void tile_coords(const TileGrid& g, int t, int& tm, i
     tn = r / rows;
 }
 
+// One problem of a grouped GEMM: its operand planes are row ranges of the
+// stacked A' / B' arrays (one tensor map each for all problems).
+struct GroupEntry {
+    long long tile_start;   // first tile of the problem in the global tile list
+    int tiles_n;            // tiles along N
+    int kblocks;            // 128-byte K blocks of the problem's planes
+    int a_row0, b_row0;     // first row in the stacked A' / B'
+    int m, n;
+    int ldc, vec_ok;
+    float* c;
+};
+
+struct TileInfo {
+    int tm, tn, tb, kblocks, arow, brow, m, n, vec_ok;
+    long long ldc, coff;
+    float* c;
+};
+
+// Everything a role needs about tile t: single GEMM (tile raster over M, N,
+// batch) or grouped (problem found by binary search on tile_start).
+template <bool GROUPED>
+__device__ __forceinline__ TileInfo tile_info(int t, const TileGrid& tg, const EpiArgs& ep, int kblocks,
+                                              const GroupEntry* groups, int ngroups)
+{
+    TileInfo ti;
+    if (!GROUPED) {
+        tile_coords(tg, t, ti.tm, ti.tn, ti.tb);
+        ti.kblocks = kblocks;
+        ti.arow = ti.tm * BM;
+        ti.brow = ti.tn * BN;
+        ti.m = ep.m;
+        ti.n = ep.n;
+        ti.vec_ok = ep.vec_ok;
+        ti.ldc = ep.ldc;
+        ti.coff = (long long)ti.tb * ep.stride_c;
+        ti.c = ep.c;
+    } else {
+        int lo = 0, hi = ngroups - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (groups[mid].tile_start <= t) lo = mid; else hi = mid - 1;
+        }
+        const GroupEntry& g = groups[lo];
+        const int local = (int)(t - g.tile_start);
+        ti.tm = local / g.tiles_n;
+        ti.tn = local - ti.tm * g.tiles_n;
+        ti.tb = 0;
+        ti.kblocks = g.kblocks;
+        ti.arow = g.a_row0 + ti.tm * BM;
+        ti.brow = g.b_row0 + ti.tn * BN;
+        ti.m = g.m;
+        ti.n = g.n;
+        ti.vec_ok = g.vec_ok;
+        ti.ldc = g.ldc;
+        ti.coff = 0;
+        ti.c = g.c;
+    }
+    return ti;
+}
+
 // Persistent: CTA b handles tiles b, b + G, b + 2G, ...  Barriers:
 //   full[s] / empty[s]      TMA ring (count 1 / committed by tcgen05)
 //   tfull[a] / tempty[a]    accumulator a in TMEM columns 256*a (MMA commit /
 //                           4 epilogue warps)
-template <int KIND, bool SPLIT>
+template <int KIND, bool SPLIT, bool GROUPED>
 __global__ void __launch_bounds__(THREADS, 1)
 chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
-                    int kblocks, int split_s, TileGrid tg, EpiArgs ep, int* status)
+                    int kblocks, int split_s, TileGrid tg, EpiArgs ep, int* status, const GroupEntry* groups,
+                    int ngroups)
 {
     // Split precisions keep two accumulators per tile -- the a0*b0 blocks in
     // one, every correction block in the other -- so the large running sum
@@ -283,9 +346,8 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
             long long it = 0, issued = 0;
             const int kx_mul = KB_BYTES / (KIND == KIND_TF32 ? 4 : 2);
             for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
-                int tm, tn, tb;
-                tile_coords(tg, t, tm, tn, tb);
-                for (int kb = 0; kb < kblocks; kb++, it++) {
+                const TileInfo ti = tile_info<GROUPED>(t, tg, ep, kblocks, groups, ngroups);
+                for (int kb = 0; kb < ti.kblocks; kb++, it++) {
                     const int s = (int)(it % STAGES);
                     const long long r = it / STAGES;
                     if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (unsigned)((r - 1) & 1), status, 101)) {
@@ -294,8 +356,8 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
                     }
                     const unsigned fb = smem_u32(&full[s]);
                     mbar_expect_tx(fb, A_STAGE + B_STAGE);
-                    tma_load_3d(smem_u32(sa + s * A_STAGE), &map_a, fb, kb * kx_mul, tm * BM, tb);
-                    tma_load_3d(smem_u32(sb + s * B_STAGE), &map_b, fb, kb * kx_mul, tn * BN, tb);
+                    tma_load_3d(smem_u32(sa + s * A_STAGE), &map_a, fb, kb * kx_mul, ti.arow, ti.tb);
+                    tma_load_3d(smem_u32(sb + s * B_STAGE), &map_b, fb, kb * kx_mul, ti.brow, ti.tb);
                     issued = it + 1;
                 }
             }
@@ -319,7 +381,8 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const unsigned acc_main = tmem + (unsigned)ab * BUF_COLS;
                 const unsigned acc_corr = acc_main + BN;
-                for (int kb = 0; kb < kblocks; kb++, it++) {
+                const int tk = GROUPED ? tile_info<GROUPED>(t, tg, ep, kblocks, groups, ngroups).kblocks : kblocks;
+                for (int kb = 0; kb < tk; kb++, it++) {
                     const int s = (int)(it % STAGES);
                     if (!mbar_wait(smem_u32(&full[s]), (unsigned)((it / STAGES) & 1), status, 103)) {
                         *abort_flag = 1;
@@ -346,11 +409,11 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
             const int ab = lt % NB;
             const bool ok = mbar_wait(smem_u32(&tfull[ab]), (unsigned)((lt / NB) & 1), status, 104);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            int tm, tn, tb;
-            tile_coords(tg, t, tm, tn, tb);
-            const int row = tm * BM + quarter * 32 + lane;
-            float* crow = ep.c + (long long)tb * ep.stride_c + (long long)row * ep.ldc;
-            const bool do_store = ok && !*abort_flag && kblocks > 0;
+            const TileInfo ti = tile_info<GROUPED>(t, tg, ep, kblocks, groups, ngroups);
+            const int tn = ti.tn;
+            const int row = ti.tm * BM + quarter * 32 + lane;
+            float* crow = ti.c + ti.coff + (long long)row * ti.ldc;
+            const bool do_store = ok && !*abort_flag && ti.kblocks > 0;
             const unsigned tbase = tmem + ((unsigned)(quarter * 32) << 16) + (unsigned)ab * BUF_COLS;
             // 64 columns per step: two (four when split) 32-column TMEM loads in
             // flight, one wait, then 16 x 16-byte stores of this lane's row
@@ -379,10 +442,10 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
                     }
                 }
                 const int col = tn * BN + c0;
-                if (!do_store || row >= ep.m || col >= ep.n) continue;
+                if (!do_store || row >= ti.m || col >= ti.n) continue;
 #pragma unroll
                 for (int i = 0; i < 64; i++) v[i] *= ep.alpha;
-                if (ep.vec_ok && col + 64 <= ep.n) {
+                if (ti.vec_ok && col + 64 <= ti.n) {
                     float4* p = reinterpret_cast<float4*>(crow + col);
 #pragma unroll
                     for (int q = 0; q < 16; q++) {
@@ -397,7 +460,7 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
                 } else {
 #pragma unroll
                     for (int i = 0; i < 64; i++)
-                        if (col + i < ep.n) crow[col + i] = ep.beta != 0.0f ? v[i] + ep.beta * crow[col + i] : v[i];
+                        if (col + i < ti.n) crow[col + i] = ep.beta != 0.0f ? v[i] + ep.beta * crow[col + i] : v[i];
                 }
             }
             // accumulator ab may be overwritten once all four warps have read it
@@ -554,6 +617,102 @@ __global__ void transpose_pad_f32(const float* __restrict__ x, long long ld, lon
     }
 }
 
+// ----------------------------------------------------- grouped prepass
+
+// A-side job: rows [row0, row0 + rows) of the stacked A' come from `src`
+struct RowJob {
+    long long row0;
+    const float* src;
+    int rows, k, kpad, pad;
+};
+
+// B-side job: 64 x 64 tiles [tile0, tile0 + tiles) transpose-split `src` (k x cols)
+// into rows [row0, row0 + cols) of the stacked B'
+struct ColJob {
+    long long tile0, row0;
+    const float* src;
+    int tiles, tiles_n, k, kpad, cols, pad;
+};
+
+// 4 rows per 256-thread block (64 threads x 8 elements per row pass)
+template <int S>
+__global__ void __launch_bounds__(256) grouped_split_rows(const RowJob* __restrict__ jobs, int njobs, long long nrows,
+                                                          __nv_bfloat16* __restrict__ out, long long pitch)
+{
+    const long long row = (long long)blockIdx.x * 4 + (threadIdx.x >> 6);
+    if (row >= nrows) return;
+    const int lane = threadIdx.x & 63;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].row0 <= row) lo = mid; else hi = mid - 1;
+    }
+    const RowJob j = jobs[lo];
+    const float* x = j.src + (row - j.row0) * (long long)j.k;
+    __nv_bfloat16* o = out + row * pitch;
+    const int sel = S == 1 ? 0 : (S == 3 ? 1 : 2);
+    const bool vec = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+    for (int k8 = lane; k8 * 8 < j.kpad; k8 += 64) {
+        const int kk = k8 * 8;
+        float a[8];
+        if (vec && kk + 8 <= j.k) {
+            const float4 u = __ldg(reinterpret_cast<const float4*>(x + kk));
+            const float4 w = __ldg(reinterpret_cast<const float4*>(x + kk) + 1);
+            a[0] = u.x; a[1] = u.y; a[2] = u.z; a[3] = u.w; a[4] = w.x; a[5] = w.y; a[6] = w.z; a[7] = w.w;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; i++) a[i] = kk + i < j.k ? __ldg(x + kk + i) : 0.0f;
+        }
+        uint4 q[3];
+        split8(a, q);
+        const int kb = kk >> 6, jj = kk & 63;
+#pragma unroll
+        for (int s = 0; s < S; s++) *reinterpret_cast<uint4*>(o + (long long)(kb * S + s) * 64 + jj) = q[kSelA[sel][s]];
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) grouped_split_cols(const ColJob* __restrict__ jobs, int njobs,
+                                                          __nv_bfloat16* __restrict__ out, long long pitch)
+{
+    __shared__ float tile[64][65];
+    const long long t = blockIdx.x;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].tile0 <= t) lo = mid; else hi = mid - 1;
+    }
+    const ColJob j = jobs[lo];
+    const int local = (int)(t - j.tile0);
+    const int kt = local / j.tiles_n, nt = local - kt * j.tiles_n;
+    const int k0 = kt * 64, c0 = nt * 64;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    for (int i = ty; i < 64; i += 16) {
+        const int kk = k0 + i;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int cc = c0 + tx * 4 + q;
+            tile[i][tx * 4 + q] = (kk < j.k && cc < j.cols) ? __ldg(j.src + (long long)kk * j.cols + cc) : 0.0f;
+        }
+    }
+    __syncthreads();
+    const int sel = S == 1 ? 0 : (S == 3 ? 1 : 2);
+    for (int item = threadIdx.x; item < 512; item += 256) {
+        const int c = item >> 3, r = item & 7;
+        const int cc = c0 + c, kk = k0 + r * 8;
+        if (cc >= j.cols || kk >= j.kpad) continue;
+        float a[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) a[i] = tile[r * 8 + i][c];
+        uint4 q[3];
+        split8(a, q);
+        const int kb = kk >> 6, jj = kk & 63;
+        __nv_bfloat16* o = out + (j.row0 + cc) * pitch;
+#pragma unroll
+        for (int s = 0; s < S; s++) *reinterpret_cast<uint4*>(o + (long long)(kb * S + s) * 64 + jj) = q[kSelB[sel][s]];
+    }
+}
+
 }  // namespace tc
 
 // ---------------------------------------------------------------- host side
@@ -663,8 +822,10 @@ int launch_gemm_tc(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision)
     const unsigned grid = (unsigned)std::min<long long>(ntiles, ctx->sm_count);
 #define LAUNCH_TC(KD, SP)                                                                                      \
     do {                                                                                                       \
-        cudaFuncSetAttribute(chai_gemm_tc_kernel<KD, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES); \
-        chai_gemm_tc_kernel<KD, SP><<<grid, THREADS, SMEM_BYTES, s>>>(ma, mb, kblocks, S, tg, ep, ctx->status_word); \
+        cudaFuncSetAttribute(chai_gemm_tc_kernel<KD, SP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                             SMEM_BYTES);                                                                      \
+        chai_gemm_tc_kernel<KD, SP, false><<<grid, THREADS, SMEM_BYTES, s>>>(ma, mb, kblocks, S, tg, ep,       \
+                                                                              ctx->status_word, nullptr, 0);   \
     } while (0)
     cudaEvent_t ev[2];
     ktime_begin(ctx, "gemm_tc", ev);
@@ -673,6 +834,117 @@ int launch_gemm_tc(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision)
     else LAUNCH_TC(KIND_BF16, true);
 #undef LAUNCH_TC
     ktime_end(ctx, "gemm_tc", ev);
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    return CHAI_OK;
+}
+
+}  // namespace chai
+
+namespace chai {
+
+// Many independent f32 GEMMs C_i = A_i B_i in one persistent tensor-core launch.
+// Every problem's planes are written into one stacked A' (sum M_i rows) and
+// one stacked B' (sum N_i rows) with a common row pitch, so two tensor maps
+// serve all problems; the kernel finds a tile's problem by binary search on
+// its first tile.  A tile that overhangs a problem's M or N reads rows of the
+// next problem (or TMA zero fill past the end): they only reach accumulator
+// rows / columns that the epilogue does not store.
+int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_problem* p, int32_t count)
+{
+    using namespace tc;
+    if (count <= 0) return CHAI_OK;
+    int prec = precision == CHAI_GEMM_AUTO ? ctx->cfg.gemm_precision : precision;
+    if (prec == CHAI_GEMM_FP32) prec = CHAI_GEMM_BF16X3;   // f32 accuracy on the tensor cores
+    if (prec != CHAI_GEMM_BF16 && prec != CHAI_GEMM_BF16X3 && prec != CHAI_GEMM_BF16X6)
+        return set_error(ctx, CHAI_ERR_UNSUPPORTED, "grouped gemm: bf16, bf16x3 or bf16x6");
+    const int S = prec == CHAI_GEMM_BF16X3 ? 3 : prec == CHAI_GEMM_BF16X6 ? 6 : 1;
+    long long ra = 0, rb = 0, kmax = 0, tiles = 0, coltiles = 0;
+    std::vector<GroupEntry> groups(count);
+    std::vector<RowJob> rj(count);
+    std::vector<ColJob> cj(count);
+    for (int i = 0; i < count; i++) {
+        const chai_gemm_problem& q = p[i];
+        if (q.m <= 0 || q.n <= 0 || q.k <= 0 || !q.a || !q.b || !q.c || q.m > 65535 || q.n > 65535)
+            return set_error(ctx, CHAI_ERR_INVALID, "grouped gemm: bad problem " + std::to_string(i));
+        const int kpad = (q.k + 63) / 64 * 64;
+        kmax = std::max<long long>(kmax, kpad);
+        GroupEntry& g = groups[i];
+        g.tile_start = tiles;
+        g.tiles_n = (q.n + BN - 1) / BN;
+        g.kblocks = S * kpad / 64;
+        g.a_row0 = (int)ra;
+        g.b_row0 = (int)rb;
+        g.m = q.m;
+        g.n = q.n;
+        g.ldc = q.n;
+        g.vec_ok = ((reinterpret_cast<uintptr_t>(q.c) & 15) == 0 && q.n % 4 == 0) ? 1 : 0;
+        g.c = q.c;
+        tiles += (long long)((q.m + BM - 1) / BM) * g.tiles_n;
+        rj[i] = RowJob{ra, q.a, q.m, q.k, kpad, 0};
+        const int tn64 = (q.n + 63) / 64;
+        cj[i] = ColJob{coltiles, rb, q.b, tn64 * (kpad / 64), tn64, q.k, kpad, q.n, 0};
+        coltiles += (long long)tn64 * (kpad / 64);
+        ra += q.m;
+        rb += q.n;
+    }
+    if (ra >= (1ll << 31) || rb >= (1ll << 31) || tiles >= (1ll << 30))
+        return set_error(ctx, CHAI_ERR_UNSUPPORTED, "grouped gemm: too large");
+    const long long pitch = S * kmax;   // bf16 elements per stacked row
+    const size_t a_bytes = (size_t)ra * pitch * 2, b_bytes = (size_t)rb * pitch * 2;
+    const size_t g_bytes = groups.size() * sizeof(GroupEntry), r_bytes = rj.size() * sizeof(RowJob),
+                 c_bytes = cj.size() * sizeof(ColJob);
+    auto up = [](size_t x) { return (x + 1023) & ~size_t(1023); };
+    int st = ensure_scratch(ctx, up(a_bytes) + up(b_bytes) + up(g_bytes) + up(r_bytes) + up(c_bytes));
+    if (st) return st;
+    char* base = static_cast<char*>(ctx->scratch);
+    __nv_bfloat16* Ap = reinterpret_cast<__nv_bfloat16*>(base);
+    __nv_bfloat16* Bp = reinterpret_cast<__nv_bfloat16*>(base + up(a_bytes));
+    GroupEntry* dg = reinterpret_cast<GroupEntry*>(base + up(a_bytes) + up(b_bytes));
+    RowJob* drj = reinterpret_cast<RowJob*>(reinterpret_cast<char*>(dg) + up(g_bytes));
+    ColJob* dcj = reinterpret_cast<ColJob*>(reinterpret_cast<char*>(drj) + up(r_bytes));
+    cudaStream_t s = ctx->stream;
+    CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(dg, groups.data(), g_bytes, cudaMemcpyHostToDevice, s));
+    CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(drj, rj.data(), r_bytes, cudaMemcpyHostToDevice, s));
+    CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(dcj, cj.data(), c_bytes, cudaMemcpyHostToDevice, s));
+#define GSPLIT(SS)                                                                                      \
+    grouped_split_rows<SS><<<(unsigned)((ra + 3) / 4), 256, 0, s>>>(drj, count, ra, Ap, pitch);         \
+    grouped_split_cols<SS><<<(unsigned)coltiles, 256, 0, s>>>(dcj, count, Bp, pitch)
+    if (S == 1) { GSPLIT(1); } else if (S == 3) { GSPLIT(3); } else { GSPLIT(6); }
+#undef GSPLIT
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    CUtensorMap ma, mb;
+    st = make_map(ctx, &ma, Ap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, pitch, ra, 1, ra * pitch, 64, BM);
+    if (st) return st;
+    st = make_map(ctx, &mb, Bp, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, pitch, rb, 1, rb * pitch, 64, BN);
+    if (st) return st;
+    TileGrid tg;
+    tg.tiles_m = (int)tiles;
+    tg.tiles_n = 1;
+    tg.batch = 1;
+    EpiArgs ep;
+    memset(&ep, 0, sizeof ep);
+    ep.alpha = 1.0f;
+    ep.beta = 0.0f;
+    const unsigned grid = (unsigned)std::min<long long>(tiles, ctx->sm_count);
+    cudaEvent_t ev[2];
+    ktime_begin(ctx, "gemm_grouped", ev);
+    // Grouped problems have K <= a few hundred: for bf16 and bf16x3 the
+    // interleaved planes' accumulation error stays far inside the split's own
+    // truncation error, so they use one accumulator per tile and double-buffer
+    // TMEM (a tile's epilogue overlaps the next tile's MMAs); bf16x6, whose
+    // products reach FP32 level, keeps the separate correction accumulator.
+    if (S == 6 || kmax > 2048) {
+        cudaFuncSetAttribute(chai_gemm_tc_kernel<KIND_BF16, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SMEM_BYTES);
+        chai_gemm_tc_kernel<KIND_BF16, true, true><<<grid, THREADS, SMEM_BYTES, s>>>(ma, mb, 0, S, tg, ep,
+                                                                                     ctx->status_word, dg, count);
+    } else {
+        cudaFuncSetAttribute(chai_gemm_tc_kernel<KIND_BF16, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SMEM_BYTES);
+        chai_gemm_tc_kernel<KIND_BF16, false, true><<<grid, THREADS, SMEM_BYTES, s>>>(ma, mb, 0, S, tg, ep,
+                                                                                      ctx->status_word, dg, count);
+    }
+    ktime_end(ctx, "gemm_grouped", ev);
     CHAI_CUDA_TRY(ctx, cudaGetLastError());
     return CHAI_OK;
 }

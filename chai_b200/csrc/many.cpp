@@ -7,7 +7,7 @@
 // (api/chai.h:551-600).  Here traces that share one program -- the same cells
 // except for scalar values (W, H, seeds, literals) -- are compiled once, with
 // the per-trace scalars read from a device table, and run as ONE kernel over a
-// global list of 1024-element tiles:
+// global list of 8192-element tiles:
 //   tab[0] = number of tiles, tab[1] = number of traces, then per trace:
 //   { n, W, H, first tile, seed of each RNG node, bits of each varying scalar }.
 // Every CTA walks tiles blockIdx.x, +gridDim.x, ...; a tile finds its trace
@@ -177,9 +177,10 @@ static bool build_program(const std::vector<std::vector<Node>>& all, int root, d
        << " + 3] <= tile) lo = mid; else hi = mid - 1; }\n"
        << "    const long long* tp = rows + (long long)lo * " << p.stride << ";\n"
        << "    const long long n = tp[0], W = tp[1];\n"
-       << "    const long long c = (tile - tp[3]) * 256 + threadIdx.x;\n"
        << "    double red[1] = {0};\n"
-       << "    if (c * 4 < n) {\n"
+       << "    for (int sub = 0; sub < 8; sub++) {\n"
+       << "    const long long c = ((tile - tp[3]) * 8 + sub) * 256 + threadIdx.x;\n"
+       << "    if (c * 4 >= n) break;\n"
        << "    const long long e0 = c * 4;\n"
        << "    long long xx[4], yy[4]; { const long long y0 = e0 / W, x0 = e0 - y0 * W; "
           "for (int j = 0; j < 4; j++) { xx[j] = x0 + j; yy[j] = y0; } }\n";
@@ -347,7 +348,7 @@ extern "C" int chai_cuda_evaluate_many(chai_cuda_ctx* ctx, const chai_trace_desc
         row[1] = (long long)r.W;
         row[2] = (long long)r.H;
         row[3] = tiles;
-        tiles += (row[0] + 1023) / 1024;
+        tiles += (row[0] + 8191) / 8192;      // 8192-element tiles: 256 threads x 8 chunks of 4
         for (size_t k = 0; k < prog.rng_nodes.size(); k++) {
             const Node& rn = all[t][prog.rng_nodes[k]];
             row[4 + k] = (long long)(rn.prec == CHAI_F64 ? rn.seed : (uint32_t)rn.seed);

@@ -4,12 +4,6 @@
 
 namespace chai {
 
-int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_problem* p, int32_t count)
-{
-    (void)precision; (void)p; (void)count;
-    return set_error(ctx, CHAI_ERR_UNSUPPORTED, "grouped gemm not built");
-}
-
 int Tuner::tune(const chai_gemm_key* key, int mode, chai_gemm_cfg* out)
 {
     (void)key; (void)mode; (void)out;

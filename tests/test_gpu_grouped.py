@@ -1,0 +1,58 @@
+"""Grouped GEMM: many independent f32 problems of different shapes in one
+persistent tcgen05 launch (chai_cuda_gemm_grouped), each checked against the
+FP64 oracle with the componentwise-normalised error of test_gpu_gemm.py
+(bf16x3: 2^-14, bf16: 2^-7, bf16x6: 2^-20)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from chai_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+BOUND = {L.GEMM_BF16: 2.0 ** -7, L.GEMM_BF16X3: 2.0 ** -14, L.GEMM_BF16X6: 2.0 ** -20}
+
+
+def problems(count, seed=11, lo=32, hi=512):
+    rng = np.random.default_rng(seed)
+    return [tuple(int(v) for v in rng.integers(lo // 8, hi // 8 + 1, 3) * 8) for _ in range(count)]
+
+
+def run_grouped(dev, shapes, prec, seed=1):
+    import torch
+    rng = np.random.default_rng(seed)
+    As = [rng.uniform(-1, 1, (m, k)).astype(np.float32) for m, n, k in shapes]
+    Bs = [rng.uniform(-1, 1, (k, n)).astype(np.float32) for m, n, k in shapes]
+    ta = [torch.from_numpy(a).cuda() for a in As]
+    tb = [torch.from_numpy(b).cuda() for b in Bs]
+    tc = [torch.full((m, n), float("nan"), device="cuda") for m, n, k in shapes]
+    arr = (L.chai_gemm_problem * len(shapes))()
+    for i, (m, n, k) in enumerate(shapes):
+        arr[i] = L.chai_gemm_problem(m, n, k, 0, ta[i].data_ptr(), tb[i].data_ptr(), tc[i].data_ptr())
+    L.check(L.lib().chai_cuda_gemm_grouped(dev.ctx, prec, arr, len(shapes)), dev.ctx)
+    L.check(L.lib().chai_cuda_synchronize(dev.ctx), dev.ctx)
+    return As, Bs, [c.cpu().numpy() for c in tc]
+
+
+@pytest.mark.parametrize("prec", [L.GEMM_BF16, L.GEMM_BF16X3, L.GEMM_BF16X6])
+def test_grouped_gemm_vs_fp64(chai_dev, prec):
+    shapes = problems(48) + [(8, 8, 8), (513 // 8 * 8, 8, 504), (40, 512, 32)]
+    As, Bs, Cs = run_grouped(chai_dev, shapes, prec)
+    worst = 0.0
+    for a, b, c in zip(As, Bs, Cs):
+        c64 = oracle.gemm_f64(a, b)
+        bound = np.abs(a).astype(np.float64) @ np.abs(b).astype(np.float64)
+        worst = max(worst, float(np.max(np.abs(c - c64) / bound)))
+    assert worst <= BOUND[prec], worst
+
+
+def test_grouped_gemm_4096_problems_sample(chai_dev):
+    """The full 4096-problem group (M, N, K multiples of 8 in [32, 512],
+    seed 11); every 97th problem is checked against the FP64 oracle."""
+    shapes = problems(4096)
+    As, Bs, Cs = run_grouped(chai_dev, shapes, L.GEMM_BF16X3)
+    for i in range(0, 4096, 97):
+        c64 = oracle.gemm_f64(As[i], Bs[i])
+        bound = np.abs(As[i]).astype(np.float64) @ np.abs(Bs[i]).astype(np.float64)
+        assert np.max(np.abs(Cs[i] - c64) / bound) <= BOUND[L.GEMM_BF16X3], i
