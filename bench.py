@@ -554,8 +554,56 @@ def run_grouped(args, L, ctx, stream):
     }
 
 
+def run_tuner(args, L, ctx, stream):
+    """Learned tuner: exhaustive sweeps over 2000 training keys and 200 held-out
+    keys (M, N, K log-uniform in [64, 16384], seed 13, fp32 via bf16x3 and bf16
+    GEMM plus f32 GEMV), MLP trained on the GPU, then each held-out key tuned
+    twice from cold: learned (rank all configurations, time the top k) and
+    exhaustive (time all).  Quality is judged on the held-out key's own sweep."""
+    import torch
+    from chai_b200 import tuner as T
+    n_train = args.size or 2000
+    keys = T.shapes(n_train + 200, seed=13)
+    train_keys, held_keys = keys[:n_train], keys[n_train:]
+    data, sweep_s = T.collect(ctx, train_keys, log=lambda m: print(m, file=sys.stderr))
+    held, _ = T.collect(ctx, held_keys)
+    samples = [(k, c) for k, cs in data for c in cs if c.measured_us < 1e29]
+    t0 = time.perf_counter()
+    loss = T.train(ctx, samples, epochs=args.steps if args.steps > 100 else 4000, lr=1e-3, seed=1)
+    train_s = time.perf_counter() - t0
+    with Clocks(torch.cuda.current_device()) as clk:
+        rows = T.evaluate(ctx, held)
+    gm = lambda v: float(np.exp(np.mean(np.log(v)))) if len(v) else None
+    q = np.array([r["best_us"] / r["pick_us"] for r in rows])
+    qd = np.array([r["best_us"] / r["default_us"] for r in rows])
+    ls = sum(r["learned_s"] for r in rows)
+    es = sum(r["exhaustive_s"] for r in rows)
+    part = {}
+    for name, sel in (("gemm_fp32", lambda r: not r["gemv"] and r["precision"] == L.GEMM_FP32),
+                      ("gemm_bf16", lambda r: not r["gemv"] and r["precision"] == L.GEMM_BF16),
+                      ("gemv_f32", lambda r: r["gemv"])):
+        idx = [i for i, r in enumerate(rows) if sel(r)]
+        part[name] = {"keys": len(idx), "pick_vs_best_geomean": gm(q[idx]),
+                      "default_vs_best_geomean": gm(qd[idx]),
+                      "within_5pct": float(np.mean(q[idx] >= 1 / 1.05)) if idx else None,
+                      "cold_start_speedup": (sum(rows[i]["exhaustive_s"] for i in idx) /
+                                             max(1e-9, sum(rows[i]["learned_s"] for i in idx))) if idx else None}
+    return {
+        "metric": "tune time learned vs exhaustive", "unit": "x (cold-start speedup)", "value": es / ls,
+        "ms_per_step": 1e3 * ls / len(rows), "dtype": "f32/bf16", "higher_is_better": True,
+        "config": {"workload": "learned GEMM/GEMV tuner: %d train + %d held-out keys, M,N,K log-uniform "
+                               "[64,16384], seed 13" % (n_train, len(rows)), "top_k": 2,
+                   "search_space": {"gemm": T.GEMM_SPACE, "gemv": T.GEMV_SPACE}},
+        "tuner": {"pick_vs_best_geomean": gm(q), "within_5pct": float(np.mean(q >= 1 / 1.05)),
+                  "default_vs_best_geomean": gm(qd), "learned_s_total": ls, "exhaustive_s_total": es,
+                  "train_samples": len(samples), "train_loss": loss, "train_s": train_s, "sweep_s": sweep_s,
+                  "by_kind": part},
+        "e2e": None, "roofline": None, "clocks": clk.summary(), "gpu_launches": None,
+    }
+
+
 WORKLOADS = {"gemm": run_gemm, "mc": run_mc, "kirsch": run_kirsch, "gemv": run_gemv, "mc-many": run_mc_many,
-             "grouped": run_grouped}
+             "grouped": run_grouped, "tuner": run_tuner}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -571,6 +619,9 @@ def run_reference(args, steps=None):
         return {"impl": "reference", "unavailable": "oracle/_ref/ref_driver not built (reference sources absent)"}
     steps = steps or max(1, args.steps)
     wl = args.workload
+    if wl == "tuner":
+        return {"impl": "reference", "unavailable": "the reference tuner (StandardEM over generated OpenCL "
+                                                   "kernels) needs an OpenCL GPU device; none on this host"}
     times = []
     with tempfile.TemporaryDirectory() as td:
         rng = np.random.default_rng(1)
@@ -715,6 +766,8 @@ def main():
                 "config": dict(res["config"], parallelism="independent traces per GPU (dp%d)" % world)}
         for k in ("e2e", "roofline", "clocks", "gpu_launches"):
             line[k] = res.get(k)
+        if "tuner" in res:
+            line["tuner"] = res["tuner"]
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args)
         print(json.dumps(line))

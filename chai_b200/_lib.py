@@ -69,7 +69,7 @@ class chai_gemm_key(C.Structure):
 class chai_gemm_cfg(C.Structure):
     _fields_ = [("block_m", C.c_int32), ("block_n", C.c_int32), ("block_k", C.c_int32), ("stages", C.c_int32),
                 ("vec_width", C.c_int32), ("cluster_m", C.c_int32), ("cluster_n", C.c_int32),
-                ("reserved", C.c_int32), ("measured_us", C.c_double)]
+                ("group_m", C.c_int32), ("measured_us", C.c_double)]
 
 
 P = C.c_void_p
@@ -104,6 +104,17 @@ SIGNATURES = {
     "chai_cuda_tune": (C.c_int, [P, C.POINTER(chai_gemm_key), C.c_int, C.POINTER(chai_gemm_cfg)]),
     "chai_cuda_tune_db_load": (C.c_int, [P, C.c_char_p]),
     "chai_cuda_tune_db_save": (C.c_int, [P, C.c_char_p]),
+    "chai_cuda_tune_sweep": (C.c_int, [P, C.POINTER(chai_gemm_key), C.POINTER(chai_gemm_cfg), C.c_int,
+                                       C.POINTER(C.c_int)]),
+    "chai_cuda_tune_features": (C.c_int, [C.POINTER(chai_gemm_key), C.POINTER(chai_gemm_cfg),
+                                          C.POINTER(C.c_float)]),
+    "chai_cuda_mlp_train": (C.c_int, [P, C.POINTER(chai_gemm_key), C.POINTER(chai_gemm_cfg), C.c_size_t, C.c_int,
+                                      C.c_double, C.c_uint64, C.POINTER(C.c_double)]),
+    "chai_cuda_mlp_predict": (C.c_int, [P, C.POINTER(chai_gemm_key), C.POINTER(chai_gemm_cfg), C.c_size_t,
+                                        C.POINTER(C.c_double)]),
+    "chai_cuda_mlp_gradients": (C.c_int, [P, C.POINTER(chai_gemm_key), C.POINTER(chai_gemm_cfg), C.c_size_t,
+                                          C.POINTER(C.c_float), C.c_size_t, C.POINTER(C.c_double)]),
+    "chai_cuda_mlp_weights": (C.c_int, [P, C.POINTER(C.c_float), C.c_size_t, C.POINTER(C.c_size_t), C.c_int]),
 }
 
 _lib = None

@@ -152,6 +152,10 @@ static void parse_config(chai::Config& c, const char* text)
             c.rng_layout = (v == "counter") ? 1 : 0;
         } else if (k == "TunerMode") {
             c.tuner_mode = (v == "exhaustive") ? CHAI_TUNE_EXHAUSTIVE : CHAI_TUNE_LEARNED;
+        } else if (k == "TopK") {
+            c.top_k = std::max(1, atoi(v.c_str()));
+        } else if (k == "TuneJournal") {
+            c.tune_journal = v;
         } else if (k == "TuneDB") {
             c.tune_db = v;
         } else if (k == "JitCache") {
@@ -215,7 +219,7 @@ int chai_cuda_init(int device, const char* config, chai_cuda_ctx** out)
     ctx->kernel_timing = getenv("CHAI_KERNEL_TIMING") && atoi(getenv("CHAI_KERNEL_TIMING")) != 0;
     ctx->jit.reset(new Jit(ctx));
     ctx->tuner.reset(new Tuner(ctx));
-    if (!ctx->cfg.tune_db.empty()) ctx->tuner->load(ctx->cfg.tune_db);
+    if (!ctx->cfg.tune_db.empty() || !ctx->cfg.tune_journal.empty()) ctx->tuner->load(ctx->cfg.tune_db);
     *out = ctx;
     return CHAI_OK;
 }

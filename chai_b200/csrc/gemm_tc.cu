@@ -39,6 +39,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "tuner.h"
 
 namespace chai {
 
@@ -48,16 +49,22 @@ int launch_transpose(chai_cuda_ctx* ctx, uint32_t prec, const void* in, void* ou
 namespace tc {
 
 constexpr int BM = 128;
-constexpr int BN = 256;
 constexpr int KB_BYTES = 128;            // one swizzle row: 64 bf16 / 32 tf32 / 128 fp8
-constexpr int STAGES = 4;
 constexpr int A_STAGE = BM * KB_BYTES;   // 16 KiB
-constexpr int B_STAGE = BN * KB_BYTES;   // 32 KiB
-constexpr int SMEM_BYTES = STAGES * (A_STAGE + B_STAGE) + 1024 /*align*/ + 256 /*barriers*/;
 constexpr int THREADS = 192;
-constexpr unsigned TMEM_COLS = 512;                       // two 128 x 256 FP32 accumulators
 constexpr unsigned long long WAIT_NS = 2000000000ull;      // a wait gives up after 2 s
-constexpr int GROUP_M = 16;                                // tile raster: 16 M-tiles per group
+
+// Tunable tile configuration: N-tile width (128 or 256 columns), pipeline
+// depth (stages of {A, B} tiles in shared memory) and tile-raster group
+// height (M-tiles per column strip).  The instantiated (BN, stages) pairs are
+// (256, 3), (256, 4), (128, 4), (128, 6); group_m is a runtime value.
+template <int BNT, int ST>
+struct TcShape {
+    static constexpr int BN = BNT;
+    static constexpr int STAGES = ST;
+    static constexpr int B_STAGE = BN * KB_BYTES;
+    static constexpr int SMEM_BYTES = STAGES * (A_STAGE + B_STAGE) + 1024 /*align*/ + 256 /*barriers*/;
+};
 
 enum Kind { KIND_BF16 = 0, KIND_TF32 = 1 };
 
@@ -135,8 +142,8 @@ __device__ __forceinline__ unsigned long long smem_desc(unsigned addr)
     return d;
 }
 
-// Instruction descriptor: FP32 accumulate, K-major A and B, M = 128, N = 256.
-template <int KIND>
+// Instruction descriptor: FP32 accumulate, K-major A and B, M = 128, N = BN.
+template <int KIND, int BN>
 __device__ __forceinline__ unsigned instr_desc()
 {
     unsigned d = 0;
@@ -208,7 +215,7 @@ struct EpiArgs {
 };
 
 struct TileGrid {
-    int tiles_m, tiles_n, batch;
+    int tiles_m, tiles_n, batch, group_m;
 };
 
 // tile t -> (m, n, batch) in GROUP_M-high column strips, so the CTAs running
@@ -218,10 +225,11 @@ __device__ __forceinline__ void tile_coords(const TileGrid& g, int t, int& tm, i
     const int per_batch = g.tiles_m * g.tiles_n;
     tb = t / per_batch;
     t -= tb * per_batch;
-    const int group = t / (GROUP_M * g.tiles_n);
-    const int first_m = group * GROUP_M;
-    const int rows = min(GROUP_M, g.tiles_m - first_m);
-    const int r = t - group * GROUP_M * g.tiles_n;
+    const int gm = g.group_m;
+    const int group = t / (gm * g.tiles_n);
+    const int first_m = group * gm;
+    const int rows = min(gm, g.tiles_m - first_m);
+    const int r = t - group * gm * g.tiles_n;
     tm = first_m + r % rows;
     tn = r / rows;
 }
@@ -246,7 +254,7 @@ struct TileInfo {
 
 // Everything a role needs about tile t: single GEMM (tile raster over M, N,
 // batch) or grouped (problem found by binary search on tile_start).
-template <bool GROUPED>
+template <bool GROUPED, int BN>
 __device__ __forceinline__ TileInfo tile_info(int t, const TileGrid& tg, const EpiArgs& ep, int kblocks,
                                               const GroupEntry* groups, int ngroups)
 {
@@ -290,19 +298,21 @@ __device__ __forceinline__ TileInfo tile_info(int t, const TileGrid& tg, const E
 //   full[s] / empty[s]      TMA ring (count 1 / committed by tcgen05)
 //   tfull[a] / tempty[a]    accumulator a in TMEM columns 256*a (MMA commit /
 //                           4 epilogue warps)
-template <int KIND, bool SPLIT, bool GROUPED>
+template <int KIND, bool SPLIT, bool GROUPED, int BNT, int ST>
 __global__ void __launch_bounds__(THREADS, 1)
 chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                     int kblocks, int split_s, TileGrid tg, EpiArgs ep, int* status, const GroupEntry* groups,
                     int ngroups)
 {
+    constexpr int BN = BNT, STAGES = ST, B_STAGE = TcShape<BNT, ST>::B_STAGE;
     // Split precisions keep two accumulators per tile -- the a0*b0 blocks in
     // one, every correction block in the other -- so the large running sum
     // sees only the a0*b0 accumulation steps; they are added in FP32 in the
     // epilogue.  That uses all 512 TMEM columns, so split tiles are single
     // buffered (NB = 1); plain bf16 / tf32 tiles double-buffer (NB = 2).
-    constexpr int NB = SPLIT ? 1 : 2;
     constexpr unsigned BUF_COLS = SPLIT ? 2 * BN : BN;
+    constexpr int NB = BUF_COLS <= 256 ? 2 : 1;
+    constexpr unsigned TMEM_COLS = NB * BUF_COLS;              // 256 or 512 (power of two)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char* sa = smem;
@@ -346,7 +356,7 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
             long long it = 0, issued = 0;
             const int kx_mul = KB_BYTES / (KIND == KIND_TF32 ? 4 : 2);
             for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
-                const TileInfo ti = tile_info<GROUPED>(t, tg, ep, kblocks, groups, ngroups);
+                const TileInfo ti = tile_info<GROUPED, BN>(t, tg, ep, kblocks, groups, ngroups);
                 for (int kb = 0; kb < ti.kblocks; kb++, it++) {
                     const int s = (int)(it % STAGES);
                     const long long r = it / STAGES;
@@ -368,7 +378,7 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
     } else if (warp == 1) {
         // ---------------------------------------------------------------- MMA
         if (lane == 0) {
-            const unsigned idesc = instr_desc<KIND>();
+            const unsigned idesc = instr_desc<KIND, BN>();
             long long it = 0;
             int lt = 0;
             for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, lt++) {
@@ -381,7 +391,7 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const unsigned acc_main = tmem + (unsigned)ab * BUF_COLS;
                 const unsigned acc_corr = acc_main + BN;
-                const int tk = GROUPED ? tile_info<GROUPED>(t, tg, ep, kblocks, groups, ngroups).kblocks : kblocks;
+                const int tk = GROUPED ? tile_info<GROUPED, BN>(t, tg, ep, kblocks, groups, ngroups).kblocks : kblocks;
                 for (int kb = 0; kb < tk; kb++, it++) {
                     const int s = (int)(it % STAGES);
                     if (!mbar_wait(smem_u32(&full[s]), (unsigned)((it / STAGES) & 1), status, 103)) {
@@ -409,7 +419,7 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
             const int ab = lt % NB;
             const bool ok = mbar_wait(smem_u32(&tfull[ab]), (unsigned)((lt / NB) & 1), status, 104);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const TileInfo ti = tile_info<GROUPED>(t, tg, ep, kblocks, groups, ngroups);
+            const TileInfo ti = tile_info<GROUPED, BN>(t, tg, ep, kblocks, groups, ngroups);
             const int tn = ti.tn;
             const int row = ti.tm * BM + quarter * 32 + lane;
             float* crow = ti.c + ti.coff + (long long)row * ti.ldc;
@@ -736,6 +746,30 @@ static PFN_encodeTiled encode_fn(chai_cuda_ctx* ctx)
     return fn;
 }
 
+// Launch the (BN, stages) instantiation a configuration names.
+template <int KIND, bool SPLIT, bool GROUPED>
+static int launch_variant(chai_cuda_ctx* ctx, const TcCfg& c, unsigned grid, const CUtensorMap& ma,
+                          const CUtensorMap& mb, int kblocks, int S, const tc::TileGrid& tg,
+                          const tc::EpiArgs& ep, const tc::GroupEntry* g, int ng)
+{
+    using namespace tc;
+#define CHAI_TC_V(BNV, STV)                                                                                 \
+    do {                                                                                                    \
+        auto k = chai_gemm_tc_kernel<KIND, SPLIT, GROUPED, BNV, STV>;                                       \
+        const int sm = TcShape<BNV, STV>::SMEM_BYTES;                                                       \
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                          \
+        k<<<grid, THREADS, sm, ctx->stream>>>(ma, mb, kblocks, S, tg, ep, ctx->status_word, g, ng);         \
+    } while (0)
+    if (c.bn == 128) {
+        if (c.stages >= 6) CHAI_TC_V(128, 6); else CHAI_TC_V(128, 4);
+    } else {
+        if (c.stages <= 3) CHAI_TC_V(256, 3); else CHAI_TC_V(256, 4);
+    }
+#undef CHAI_TC_V
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    return CHAI_OK;
+}
+
 // rows x kelems (row-major, per batch `batch_stride` elements), box kbox x rbox
 static int make_map(chai_cuda_ctx* ctx, CUtensorMap* map, const void* base, CUtensorMapDataType dt, int esize,
                     long long kelems, long long rows, long long batch, long long batch_stride, int kbox, int rbox)
@@ -753,6 +787,11 @@ static int make_map(chai_cuda_ctx* ctx, CUtensorMap* map, const void* base, CUte
 }
 
 int launch_gemm_tc(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision)
+{
+    return launch_gemm_tc_cfg(ctx, d, precision, nullptr);
+}
+
+int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision, const TcCfg* cfg_in)
 {
     using namespace tc;
     if (d->trans_a || d->trans_b) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: transposed operands");
@@ -801,7 +840,13 @@ int launch_gemm_tc(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision)
     const CUtensorMapDataType dt = tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     st = make_map(ctx, &ma, Ap, dt, (int)esz, kp, M, batch, M * kp, kblk, BM);
     if (st) return st;
-    st = make_map(ctx, &mb, Bp, dt, (int)esz, kp, N, batch, N * kp, kblk, BN);
+    TcCfg cfg = default_tc_cfg();
+    if (cfg_in) cfg = *cfg_in;
+    else tuned_tc_cfg(ctx, M, N, K, precision, &cfg);
+    // only the instantiated tile widths exist; the raster group needs >= 1 row
+    if (cfg.bn != 128) cfg.bn = 256;
+    cfg.group_m = std::max(1, std::min(cfg.group_m, 1 << 16));
+    st = make_map(ctx, &mb, Bp, dt, (int)esz, kp, N, batch, N * kp, kblk, cfg.bn);
     if (st) return st;
     EpiArgs ep;
     ep.c = static_cast<float*>(d->c);
@@ -815,24 +860,18 @@ int launch_gemm_tc(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision)
     const int kblocks = (int)(kp / kblk);
     TileGrid tg;
     tg.tiles_m = (int)((M + BM - 1) / BM);
-    tg.tiles_n = (int)((N + BN - 1) / BN);
+    tg.tiles_n = (int)((N + cfg.bn - 1) / cfg.bn);
     tg.batch = (int)batch;
+    tg.group_m = cfg.group_m;
     const long long ntiles = (long long)tg.tiles_m * tg.tiles_n * tg.batch;
     if (ntiles > (1ll << 30)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: too many tiles");
     const unsigned grid = (unsigned)std::min<long long>(ntiles, ctx->sm_count);
-#define LAUNCH_TC(KD, SP)                                                                                      \
-    do {                                                                                                       \
-        cudaFuncSetAttribute(chai_gemm_tc_kernel<KD, SP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                             SMEM_BYTES);                                                                      \
-        chai_gemm_tc_kernel<KD, SP, false><<<grid, THREADS, SMEM_BYTES, s>>>(ma, mb, kblocks, S, tg, ep,       \
-                                                                              ctx->status_word, nullptr, 0);   \
-    } while (0)
     cudaEvent_t ev[2];
     ktime_begin(ctx, "gemm_tc", ev);
-    if (tf32) LAUNCH_TC(KIND_TF32, false);
-    else if (S == 1) LAUNCH_TC(KIND_BF16, false);
-    else LAUNCH_TC(KIND_BF16, true);
-#undef LAUNCH_TC
+    if (tf32) st = launch_variant<KIND_TF32, false, false>(ctx, cfg, grid, ma, mb, kblocks, S, tg, ep, nullptr, 0);
+    else if (S == 1) st = launch_variant<KIND_BF16, false, false>(ctx, cfg, grid, ma, mb, kblocks, S, tg, ep, nullptr, 0);
+    else st = launch_variant<KIND_BF16, true, false>(ctx, cfg, grid, ma, mb, kblocks, S, tg, ep, nullptr, 0);
+    if (st) return st;
     ktime_end(ctx, "gemm_tc", ev);
     CHAI_CUDA_TRY(ctx, cudaGetLastError());
     return CHAI_OK;
@@ -852,6 +891,8 @@ namespace chai {
 int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_problem* p, int32_t count)
 {
     using namespace tc;
+    const TcCfg cfg = default_tc_cfg();
+    const int BN = cfg.bn;
     if (count <= 0) return CHAI_OK;
     int prec = precision == CHAI_GEMM_AUTO ? ctx->cfg.gemm_precision : precision;
     if (prec == CHAI_GEMM_FP32) prec = CHAI_GEMM_BF16X3;   // f32 accuracy on the tensor cores
@@ -921,6 +962,7 @@ int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_p
     tg.tiles_m = (int)tiles;
     tg.tiles_n = 1;
     tg.batch = 1;
+    tg.group_m = 1;
     EpiArgs ep;
     memset(&ep, 0, sizeof ep);
     ep.alpha = 1.0f;
@@ -933,17 +975,11 @@ int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_p
     // truncation error, so they use one accumulator per tile and double-buffer
     // TMEM (a tile's epilogue overlaps the next tile's MMAs); bf16x6, whose
     // products reach FP32 level, keeps the separate correction accumulator.
-    if (S == 6 || kmax > 2048) {
-        cudaFuncSetAttribute(chai_gemm_tc_kernel<KIND_BF16, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SMEM_BYTES);
-        chai_gemm_tc_kernel<KIND_BF16, true, true><<<grid, THREADS, SMEM_BYTES, s>>>(ma, mb, 0, S, tg, ep,
-                                                                                     ctx->status_word, dg, count);
-    } else {
-        cudaFuncSetAttribute(chai_gemm_tc_kernel<KIND_BF16, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SMEM_BYTES);
-        chai_gemm_tc_kernel<KIND_BF16, false, true><<<grid, THREADS, SMEM_BYTES, s>>>(ma, mb, 0, S, tg, ep,
-                                                                                      ctx->status_word, dg, count);
-    }
+    if (S == 6 || kmax > 2048)
+        st = launch_variant<KIND_BF16, true, true>(ctx, cfg, grid, ma, mb, 0, S, tg, ep, dg, count);
+    else
+        st = launch_variant<KIND_BF16, false, true>(ctx, cfg, grid, ma, mb, 0, S, tg, ep, dg, count);
+    if (st) return st;
     ktime_end(ctx, "gemm_grouped", ev);
     CHAI_CUDA_TRY(ctx, cudaGetLastError());
     return CHAI_OK;

@@ -13,17 +13,19 @@
 #include <cuda_runtime.h>
 
 #include "internal.h"
+#include "tuner.h"
 
 namespace chai {
 
-template <class T>
-__global__ void __launch_bounds__(256) chai_gemv_n(const T* __restrict__ A, long long lda, const T* __restrict__ x,
-                                                   T* __restrict__ y, long long m, long long n, T alpha, T beta)
+template <class T, int WARPS, int UNROLL>
+__global__ void __launch_bounds__(WARPS * 32) chai_gemv_n(const T* __restrict__ A, long long lda,
+                                                          const T* __restrict__ x, T* __restrict__ y, long long m,
+                                                          long long n, T alpha, T beta)
 {
     typedef typename std::conditional<sizeof(T) == 4, float4, double2>::type V;
     constexpr int VE = 16 / sizeof(T);
     const int lane = threadIdx.x & 31;
-    const long long row = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const long long row = (long long)blockIdx.x * WARPS + (threadIdx.x >> 5);
     if (row >= m) return;
     const T* a = A + row * lda;
     T acc = 0;
@@ -34,17 +36,21 @@ __global__ void __launch_bounds__(256) chai_gemv_n(const T* __restrict__ A, long
         const V* av = reinterpret_cast<const V*>(a);
         const V* xv = reinterpret_cast<const V*>(x);
         long long v = lane;
-        for (; v + 96 < nv; v += 128) {
-            V a0 = __ldg(av + v), a1 = __ldg(av + v + 32), a2 = __ldg(av + v + 64), a3 = __ldg(av + v + 96);
-            V x0 = __ldg(xv + v), x1 = __ldg(xv + v + 32), x2 = __ldg(xv + v + 64), x3 = __ldg(xv + v + 96);
-            const T* pa[4] = {reinterpret_cast<const T*>(&a0), reinterpret_cast<const T*>(&a1),
-                              reinterpret_cast<const T*>(&a2), reinterpret_cast<const T*>(&a3)};
-            const T* px[4] = {reinterpret_cast<const T*>(&x0), reinterpret_cast<const T*>(&x1),
-                              reinterpret_cast<const T*>(&x2), reinterpret_cast<const T*>(&x3)};
+        // UNROLL independent 16-byte loads of A in flight per lane
+        for (; v + 32 * (UNROLL - 1) < nv; v += 32 * UNROLL) {
+            V ar[UNROLL], xr[UNROLL];
 #pragma unroll
-            for (int u = 0; u < 4; u++)
+            for (int u = 0; u < UNROLL; u++) {
+                ar[u] = __ldg(av + v + 32 * u);
+                xr[u] = __ldg(xv + v + 32 * u);
+            }
 #pragma unroll
-                for (int j = 0; j < VE; j++) acc = fma(pa[u][j], px[u][j], acc);
+            for (int u = 0; u < UNROLL; u++) {
+                const T* pa = reinterpret_cast<const T*>(&ar[u]);
+                const T* px = reinterpret_cast<const T*>(&xr[u]);
+#pragma unroll
+                for (int j = 0; j < VE; j++) acc = fma(pa[j], px[j], acc);
+            }
         }
         for (; v < nv; v += 32) {
             V a0 = __ldg(av + v), x0 = __ldg(xv + v);
@@ -106,14 +112,23 @@ __global__ void chai_gemv_t_finish(const T* __restrict__ partial, int splits, T*
 
 template <class T>
 static int gemv_t(chai_cuda_ctx* ctx, int trans, int64_t m, int64_t n, double alpha, const void* a, int64_t lda,
-                  const void* x, double beta, void* y)
+                  const void* x, double beta, void* y, const GemvCfg* cfg_in)
 {
     if (!trans) {
-        const unsigned blocks = (unsigned)((m + 7) / 8);
+        GemvCfg cfg;
+        if (cfg_in) cfg = *cfg_in;
+        else tuned_gemv_cfg(ctx, m, n, sizeof(T) == 8 ? CHAI_F64 : CHAI_F32, &cfg);
         cudaEvent_t ev[2];
         ktime_begin(ctx, "gemv", ev);
-        if (blocks) chai_gemv_n<T><<<blocks, 256, 0, ctx->stream>>>((const T*)a, lda, (const T*)x, (T*)y, m, n,
-                                                                    (T)alpha, (T)beta);
+#define CHAI_GV(W, U)                                                                                       \
+    chai_gemv_n<T, W, U><<<(unsigned)((m + W - 1) / W), W * 32, 0, ctx->stream>>>((const T*)a, lda, (const T*)x, \
+                                                                                 (T*)y, m, n, (T)alpha, (T)beta)
+        if (m > 0) {
+            if (cfg.warps <= 4) { if (cfg.unroll >= 4) CHAI_GV(4, 4); else CHAI_GV(4, 1); }
+            else if (cfg.warps <= 8) { if (cfg.unroll >= 4) CHAI_GV(8, 4); else CHAI_GV(8, 1); }
+            else { if (cfg.unroll >= 4) CHAI_GV(16, 4); else CHAI_GV(16, 1); }
+        }
+#undef CHAI_GV
         ktime_end(ctx, "gemv", ev);
         CHAI_CUDA_TRY(ctx, cudaGetLastError());
         return CHAI_OK;
@@ -138,12 +153,18 @@ static int gemv_t(chai_cuda_ctx* ctx, int trans, int64_t m, int64_t n, double al
     return CHAI_OK;
 }
 
+int launch_gemv_cfg(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha, const void* a,
+                    int64_t lda, const void* x, double beta, void* y, const GemvCfg* cfg)
+{
+    if (prec == CHAI_F32) return gemv_t<float>(ctx, trans, m, n, alpha, a, lda, x, beta, y, cfg);
+    if (prec == CHAI_F64) return gemv_t<double>(ctx, trans, m, n, alpha, a, lda, x, beta, y, cfg);
+    return set_error(ctx, CHAI_ERR_UNSUPPORTED, "gemv precision");
+}
+
 int launch_gemv(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha, const void* a,
                 int64_t lda, const void* x, double beta, void* y)
 {
-    if (prec == CHAI_F32) return gemv_t<float>(ctx, trans, m, n, alpha, a, lda, x, beta, y);
-    if (prec == CHAI_F64) return gemv_t<double>(ctx, trans, m, n, alpha, a, lda, x, beta, y);
-    return set_error(ctx, CHAI_ERR_UNSUPPORTED, "gemv precision");
+    return launch_gemv_cfg(ctx, prec, trans, m, n, alpha, a, lda, x, beta, y, nullptr);
 }
 
 // 32x32 tiled transpose through shared memory, per slot.

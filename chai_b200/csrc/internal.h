@@ -26,7 +26,9 @@ struct Config {
     double rng_pi = 3.14159;                 // M_PI as the reference JIT prints it
     int rng_layout = 0;                      // 0 chai, 1 counter
     int tuner_mode = CHAI_TUNE_LEARNED;
+    int top_k = 2;                           // learned tuner: configurations timed
     std::string tune_db;
+    std::string tune_journal;                // crash-safe TRY / OK markers of every timing
     std::string jit_cache;
 };
 

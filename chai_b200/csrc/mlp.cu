@@ -1,0 +1,312 @@
+// The tuner's cost model: a 12 -> 128 -> 128 -> 128 -> 1 ReLU MLP mapping
+// GEMM/GEMV shape and tile-configuration features to log(runtime).  Trained
+// and served on the GPU by the kernels in this file: a shared-memory tiled
+// FP32 matmul with optional transposes (forward and the three backward
+// products), bias / ReLU, mean-squared-error gradient, column sums for the
+// bias gradients and Adam.  The reference's counterpart is the EM search of
+// autotune/StandardEM.cpp:69-147, which has no model: it times every
+// candidate.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "internal.h"
+#include "mlp.h"
+
+namespace chai {
+
+// C[M x N] = op(A) op(B) (+ C when acc), op = transpose when t* != 0;
+// A is M x K (or K x M transposed), B is K x N (or N x K).  16 x 16 tiles.
+__global__ void mlp_matmul(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ C, int M,
+                           int N, int K, int ta, int tb, int acc)
+{
+    __shared__ float as[16][17], bs[16][17];
+    const int r = blockIdx.y * 16 + threadIdx.y, c = blockIdx.x * 16 + threadIdx.x;
+    float sum = 0.0f;
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        const int ka = k0 + threadIdx.x, kb = k0 + threadIdx.y;
+        as[threadIdx.y][threadIdx.x] = (r < M && ka < K) ? (ta ? A[(long long)ka * M + r] : A[(long long)r * K + ka]) : 0.0f;
+        bs[threadIdx.y][threadIdx.x] = (kb < K && c < N) ? (tb ? B[(long long)c * K + kb] : B[(long long)kb * N + c]) : 0.0f;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 16; k++) sum = fmaf(as[threadIdx.y][k], bs[k][threadIdx.x], sum);
+        __syncthreads();
+    }
+    if (r < M && c < N) C[(long long)r * N + c] = acc ? C[(long long)r * N + c] + sum : sum;
+}
+
+__global__ void mlp_bias_act(float* __restrict__ Y, const float* __restrict__ b, long long M, int N, int relu)
+{
+    const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (i >= M * N) return;
+    float v = Y[i] + b[i % N];
+    Y[i] = relu ? fmaxf(v, 0.0f) : v;
+}
+
+__global__ void mlp_relu_back(float* __restrict__ dY, const float* __restrict__ Y, long long n)
+{
+    const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (i < n && Y[i] <= 0.0f) dY[i] = 0.0f;
+}
+
+// d = 2 (p - y) / n; per-block partial of the squared error (deterministic)
+__global__ void mlp_mse(const float* __restrict__ p, const float* __restrict__ y, float* __restrict__ d,
+                        double* __restrict__ part, long long n)
+{
+    __shared__ double sm[256];
+    const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+    double e = 0.0;
+    if (i < n) {
+        const float diff = p[i] - y[i];
+        d[i] = 2.0f * diff / (float)n;
+        e = (double)diff * diff;
+    }
+    sm[threadIdx.x] = e;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sm[0];
+}
+
+// db[j] = sum_i dY[i][j], one block per column, fixed order
+__global__ void mlp_colsum(const float* __restrict__ dY, float* __restrict__ db, long long M, int N)
+{
+    __shared__ float sm[256];
+    const int j = blockIdx.x;
+    float s = 0.0f;
+    for (long long i = threadIdx.x; i < M; i += 256) s += dY[i * N + j];
+    sm[threadIdx.x] = s;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if (threadIdx.x < k) sm[threadIdx.x] += sm[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) db[j] = sm[0];
+}
+
+__global__ void mlp_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                         float* __restrict__ v, long long n, float lr, float b1, float b2, float eps, float c1, float c2)
+{
+    const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+static unsigned blocks_for(long long n) { return (unsigned)((n + 255) / 256); }
+
+Mlp::Mlp(chai_cuda_ctx* ctx) : ctx_(ctx)
+{
+    const int dims[5] = {MLP_IN, MLP_H, MLP_H, MLP_H, 1};
+    size_t off = 0;
+    for (int l = 0; l < 4; l++) {
+        in_[l] = dims[l];
+        out_[l] = dims[l + 1];
+        w_off_[l] = off;
+        off += (size_t)dims[l] * dims[l + 1];
+        b_off_[l] = off;
+        off += dims[l + 1];
+    }
+    count_ = off;
+}
+
+Mlp::~Mlp()
+{
+    for (float* p : {params_, grads_, m_, v_}) if (p) cudaFree(p);
+    for (float* p : acts_) if (p) cudaFree(p);
+    for (float* p : dacts_) if (p) cudaFree(p);
+    if (x_) cudaFree(x_);
+    if (y_) cudaFree(y_);
+    if (part_) cudaFree(part_);
+}
+
+int Mlp::ensure(size_t n)
+{
+    if (!params_) {
+        CHAI_CUDA_TRY(ctx_, cudaMalloc(&params_, count_ * sizeof(float)));
+        CHAI_CUDA_TRY(ctx_, cudaMalloc(&grads_, count_ * sizeof(float)));
+        CHAI_CUDA_TRY(ctx_, cudaMalloc(&m_, count_ * sizeof(float)));
+        CHAI_CUDA_TRY(ctx_, cudaMalloc(&v_, count_ * sizeof(float)));
+        init(1);
+    }
+    if (n <= cap_) return CHAI_OK;
+    for (float*& p : acts_) { if (p) cudaFree(p); p = nullptr; }
+    for (float*& p : dacts_) { if (p) cudaFree(p); p = nullptr; }
+    if (x_) cudaFree(x_);
+    if (y_) cudaFree(y_);
+    if (part_) cudaFree(part_);
+    for (int l = 0; l < 4; l++) {
+        CHAI_CUDA_TRY(ctx_, cudaMalloc(&acts_[l], n * out_[l] * sizeof(float)));
+        CHAI_CUDA_TRY(ctx_, cudaMalloc(&dacts_[l], n * out_[l] * sizeof(float)));
+    }
+    CHAI_CUDA_TRY(ctx_, cudaMalloc(&x_, n * MLP_IN * sizeof(float)));
+    CHAI_CUDA_TRY(ctx_, cudaMalloc(&y_, n * sizeof(float)));
+    CHAI_CUDA_TRY(ctx_, cudaMalloc(&part_, blocks_for((long long)n) * sizeof(double)));
+    cap_ = n;
+    return CHAI_OK;
+}
+
+// He-uniform weights, zero biases (host RNG, seeded)
+void Mlp::init(uint64_t seed)
+{
+    std::vector<float> h(count_, 0.0f);
+    std::mt19937_64 g(seed);
+    for (int l = 0; l < 4; l++) {
+        const float lim = std::sqrt(6.0f / (float)in_[l]);
+        std::uniform_real_distribution<float> u(-lim, lim);
+        for (size_t i = 0; i < (size_t)in_[l] * out_[l]; i++) h[w_off_[l] + i] = u(g);
+    }
+    cudaMemcpy(params_, h.data(), count_ * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemset(m_, 0, count_ * sizeof(float));
+    cudaMemset(v_, 0, count_ * sizeof(float));
+    step_ = 0;
+}
+
+int Mlp::upload(const float* x, const float* y, size_t n)
+{
+    int st = ensure(n);
+    if (st) return st;
+    CHAI_CUDA_TRY(ctx_, cudaMemcpyAsync(x_, x, n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice, ctx_->stream));
+    if (y) CHAI_CUDA_TRY(ctx_, cudaMemcpyAsync(y_, y, n * sizeof(float), cudaMemcpyHostToDevice, ctx_->stream));
+    return CHAI_OK;
+}
+
+void Mlp::forward(size_t n)
+{
+    cudaStream_t s = ctx_->stream;
+    const float* in = x_;
+    for (int l = 0; l < 4; l++) {
+        dim3 grid((out_[l] + 15) / 16, (unsigned)((n + 15) / 16));
+        mlp_matmul<<<grid, dim3(16, 16), 0, s>>>(in, params_ + w_off_[l], acts_[l], (int)n, out_[l], in_[l], 0, 0, 0);
+        mlp_bias_act<<<blocks_for((long long)n * out_[l]), 256, 0, s>>>(acts_[l], params_ + b_off_[l], (long long)n,
+                                                                         out_[l], l < 3);
+        in = acts_[l];
+    }
+}
+
+double Mlp::backward(size_t n)
+{
+    cudaStream_t s = ctx_->stream;
+    const unsigned nb = blocks_for((long long)n);
+    mlp_mse<<<nb, 256, 0, s>>>(acts_[3], y_, dacts_[3], part_, (long long)n);
+    for (int l = 3; l >= 0; l--) {
+        if (l < 3) mlp_relu_back<<<blocks_for((long long)n * out_[l]), 256, 0, s>>>(dacts_[l], acts_[l], (long long)n * out_[l]);
+        const float* in = l == 0 ? x_ : acts_[l - 1];
+        // dW = in^T dY  (in_[l] x out_[l])
+        dim3 gw((out_[l] + 15) / 16, (in_[l] + 15) / 16);
+        mlp_matmul<<<gw, dim3(16, 16), 0, s>>>(in, dacts_[l], grads_ + w_off_[l], in_[l], out_[l], (int)n, 1, 0, 0);
+        mlp_colsum<<<out_[l], 256, 0, s>>>(dacts_[l], grads_ + b_off_[l], (long long)n, out_[l]);
+        if (l > 0) {
+            // dX = dY W^T  (n x in_[l])
+            dim3 gx((in_[l] + 15) / 16, (unsigned)((n + 15) / 16));
+            mlp_matmul<<<gx, dim3(16, 16), 0, s>>>(dacts_[l], params_ + w_off_[l], dacts_[l - 1], (int)n, in_[l],
+                                                   out_[l], 0, 1, 0);
+        }
+    }
+    std::vector<double> part(nb);
+    cudaMemcpyAsync(part.data(), part_, nb * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    double e = 0.0;
+    for (double v : part) e += v;
+    return e / (double)n;
+}
+
+void Mlp::adam(double lr)
+{
+    step_++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, (float)step_), c2 = 1.0f - std::pow(b2, (float)step_);
+    mlp_adam<<<blocks_for((long long)count_), 256, 0, ctx_->stream>>>(params_, grads_, m_, v_, (long long)count_,
+                                                                       (float)lr, b1, b2, 1e-8f, c1, c2);
+}
+
+// Targets are standardised (y - mean) / scale; predictions are mapped back.
+int Mlp::train(const std::vector<float>& x, const std::vector<float>& y_raw, int epochs, double lr, uint64_t seed,
+               double* loss)
+{
+    const size_t n = y_raw.size();
+    if (n == 0) return set_error(ctx_, CHAI_ERR_INVALID, "mlp: no samples");
+    double mu = 0, var = 0;
+    for (float v : y_raw) mu += v;
+    mu /= (double)n;
+    for (float v : y_raw) var += (v - mu) * (v - mu);
+    mean_ = (float)mu;
+    scale_ = (float)std::sqrt(var / (double)n + 1e-12);
+    std::vector<float> y(n);
+    for (size_t i = 0; i < n; i++) y[i] = (y_raw[i] - mean_) / scale_;
+    int st = ensure(n);
+    if (st) return st;
+    init(seed);
+    st = upload(x.data(), y.data(), n);
+    if (st) return st;
+    double l = 0;
+    for (int e = 0; e < epochs; e++) {
+        forward(n);
+        l = backward(n);
+        adam(lr);
+    }
+    trained_ = true;
+    if (loss) *loss = l;
+    CHAI_CUDA_TRY(ctx_, cudaStreamSynchronize(ctx_->stream));
+    return CHAI_OK;
+}
+
+int Mlp::predict(const std::vector<float>& x, std::vector<double>& out)
+{
+    const size_t n = x.size() / MLP_IN;
+    int st = upload(x.data(), nullptr, n);
+    if (st) return st;
+    forward(n);
+    std::vector<float> p(n);
+    CHAI_CUDA_TRY(ctx_, cudaMemcpyAsync(p.data(), acts_[3], n * sizeof(float), cudaMemcpyDeviceToHost, ctx_->stream));
+    CHAI_CUDA_TRY(ctx_, cudaStreamSynchronize(ctx_->stream));
+    out.resize(n);
+    for (size_t i = 0; i < n; i++) out[i] = (double)p[i] * scale_ + mean_;
+    return CHAI_OK;
+}
+
+int Mlp::gradients(const std::vector<float>& x, const std::vector<float>& y_raw, std::vector<float>& g, double* loss)
+{
+    const size_t n = y_raw.size();
+    std::vector<float> y(n);
+    for (size_t i = 0; i < n; i++) y[i] = (y_raw[i] - mean_) / scale_;
+    int st = upload(x.data(), y.data(), n);
+    if (st) return st;
+    forward(n);
+    const double l = backward(n);
+    g.resize(count_);
+    CHAI_CUDA_TRY(ctx_, cudaMemcpy(g.data(), grads_, count_ * sizeof(float), cudaMemcpyDeviceToHost));
+    if (loss) *loss = l;
+    return CHAI_OK;
+}
+
+int Mlp::weights(float* buf, size_t cap, size_t* count, int set)
+{
+    int st = ensure(1);
+    if (st) return st;
+    if (count) *count = count_ + 2;
+    if (!buf) return CHAI_OK;
+    if (cap < count_ + 2) return set_error(ctx_, CHAI_ERR_INVALID, "mlp weights: buffer too small");
+    if (set) {
+        CHAI_CUDA_TRY(ctx_, cudaMemcpy(params_, buf, count_ * sizeof(float), cudaMemcpyHostToDevice));
+        mean_ = buf[count_];
+        scale_ = buf[count_ + 1];
+        trained_ = true;
+    } else {
+        CHAI_CUDA_TRY(ctx_, cudaMemcpy(buf, params_, count_ * sizeof(float), cudaMemcpyDeviceToHost));
+        buf[count_] = mean_;
+        buf[count_ + 1] = scale_;
+    }
+    return CHAI_OK;
+}
+
+}  // namespace chai

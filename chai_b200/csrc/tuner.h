@@ -6,6 +6,7 @@
 #include <map>
 #include <string>
 #include <tuple>
+#include <vector>
 
 #include "chai_b200.h"
 
@@ -13,18 +14,53 @@ struct chai_cuda_ctx;
 
 namespace chai {
 
+// tcgen05 GEMM tile configuration (gemm_tc.cu): N-tile width, pipeline
+// stages, tile-raster group height.
+struct TcCfg {
+    int bn = 256, stages = 4, group_m = 16;
+};
+inline TcCfg default_tc_cfg() { return TcCfg(); }
+bool tuned_tc_cfg(chai_cuda_ctx* ctx, long long m, long long n, long long k, int precision, TcCfg* out);
+
+// GEMV configuration (gemv.cu): warps (rows) per block, 16-byte loads in
+// flight per lane.
+struct GemvCfg {
+    int warps = 8, unroll = 4;
+};
+bool tuned_gemv_cfg(chai_cuda_ctx* ctx, long long m, long long n, int prec, GemvCfg* out);
+
+int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision, const TcCfg* cfg);
+int launch_gemv_cfg(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha, const void* a,
+                    int64_t lda, const void* x, double beta, void* y, const GemvCfg* cfg);
+
+// The cost model: features (tuner.cpp) -> 3 x 128 ReLU -> log runtime (mlp.cu).
+constexpr int MLP_IN = 12, MLP_H = 128;
+class Mlp;
+
 class Tuner {
 public:
-    explicit Tuner(chai_cuda_ctx* ctx) : ctx_(ctx) {}
+    explicit Tuner(chai_cuda_ctx* ctx);
+    ~Tuner();
     int tune(const chai_gemm_key* key, int mode, chai_gemm_cfg* out);
+    int sweep(const chai_gemm_key* key, chai_gemm_cfg* out, int cap, int* n);
     int load(const std::string& path);
     int save(const std::string& path) const;
-    // configuration to use for a GEMM without tuning (tuned entry if any)
     bool lookup(const chai_gemm_key* key, chai_gemm_cfg* out) const;
+    Mlp* mlp() { return mlp_; }
+    static std::vector<chai_gemm_cfg> space(const chai_gemm_key& key);
+    static void features(const chai_gemm_key& key, const chai_gemm_cfg& cfg, float* f);
+    int top_k = 2;
 
 private:
     chai_cuda_ctx* ctx_;
+    Mlp* mlp_;
     std::map<std::tuple<long long, long long, long long, int, int>, chai_gemm_cfg> db_;
+    std::map<std::string, int> bad_;     // configurations that crashed (journal)
+    std::string journal_;
+    void* bufs_[3] = {nullptr, nullptr, nullptr};
+    size_t buf_bytes_[3] = {0, 0, 0};
+    int time_cfg(const chai_gemm_key& key, chai_gemm_cfg& cfg, int reps);
+    int ensure_operands(const chai_gemm_key& key);
 };
 
 }  // namespace chai

@@ -253,15 +253,44 @@ typedef struct chai_gemm_key {
     int32_t precision;          /* CHAI_GEMM_* */
     int32_t is_gemv;
 } chai_gemm_key;
+/* GEMM: block_m 128, block_n 128|256 (tcgen05 N tile), block_k 128 bytes,
+ * stages 3..6 (shared-memory pipeline), group_m (tile-raster strip height),
+ * cluster 1x1.  GEMV: block_m = warps (rows) per block, vec_width = 16-byte
+ * loads in flight per lane. */
 typedef struct chai_gemm_cfg {
     int32_t block_m, block_n, block_k, stages;
-    int32_t vec_width, cluster_m, cluster_n, reserved;
-    double  measured_us;        /* timing of the chosen config (0 if not timed) */
+    int32_t vec_width, cluster_m, cluster_n, group_m;
+    double  measured_us;        /* timing of the configuration (0 if not timed) */
 } chai_gemm_cfg;
 enum { CHAI_TUNE_LEARNED = 0, CHAI_TUNE_EXHAUSTIVE = 1 };
+/* Choose a configuration for `key` and remember it (used by later GEMM/GEMV
+ * calls of that shape).  EXHAUSTIVE times every configuration of the search
+ * space (AutoTuneBench); LEARNED ranks them with the MLP cost model and times
+ * only the top k (TopK in the init config, default 2). */
 int chai_cuda_tune(chai_cuda_ctx* ctx, const chai_gemm_key* key, int mode, chai_gemm_cfg* out);
+/* Time every configuration of the search space for `key` (the exhaustive
+ * sweep that generates the cost model's training data). */
+int chai_cuda_tune_sweep(chai_cuda_ctx* ctx, const chai_gemm_key* key, chai_gemm_cfg* out, int cap, int* n);
+/* The 12 cost-model input features of (key, cfg). */
+int chai_cuda_tune_features(const chai_gemm_key* key, const chai_gemm_cfg* cfg, float* out12);
+/* Tuning DB / journal: best configuration per key, plus the MLP weights. */
 int chai_cuda_tune_db_load(chai_cuda_ctx* ctx, const char* path);
 int chai_cuda_tune_db_save(chai_cuda_ctx* ctx, const char* path);
+
+/* MLP cost model (MLP_IN=12 -> 128 -> 128 -> 128 -> 1, ReLU), trained on the
+ * GPU by this library's forward / backward / Adam kernels on measured
+ * (key, cfg, measured_us) samples; the target is log(measured_us). */
+int chai_cuda_mlp_train(chai_cuda_ctx* ctx, const chai_gemm_key* keys, const chai_gemm_cfg* cfgs, size_t n,
+                        int epochs, double lr, uint64_t seed, double* final_loss);
+int chai_cuda_mlp_predict(chai_cuda_ctx* ctx, const chai_gemm_key* keys, const chai_gemm_cfg* cfgs, size_t n,
+                          double* log_us);
+/* Loss and gradient of every weight for the current weights (no update). */
+int chai_cuda_mlp_gradients(chai_cuda_ctx* ctx, const chai_gemm_key* keys, const chai_gemm_cfg* cfgs, size_t n,
+                            float* grads, size_t cap, double* loss);
+/* Get (set = 0) or set (set = 1) all weights, in the order W1 b1 W2 b2 W3 b3
+ * W4 b4 (W row-major in x out), plus the target's mean and scale last;
+ * *count receives the number of floats. */
+int chai_cuda_mlp_weights(chai_cuda_ctx* ctx, float* buf, size_t cap, size_t* count, int set);
 
 #ifdef __cplusplus
 }
