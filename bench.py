@@ -571,9 +571,24 @@ def run_tuner(args, L, ctx, stream):
     t0 = time.perf_counter()
     loss = T.train(ctx, samples, epochs=args.steps if args.steps > 100 else 4000, lr=1e-3, seed=1)
     train_s = time.perf_counter() - t0
-    with Clocks(torch.cuda.current_device()) as clk:
-        rows = T.evaluate(ctx, held)
+    import chai_b200.api as ch
     gm = lambda v: float(np.exp(np.mean(np.log(v)))) if len(v) else None
+    by_k = {}
+    with tempfile.TemporaryDirectory() as td, Clocks(torch.cuda.current_device()) as clk:
+        db = os.path.join(td, "tune.db")
+        L.check(L.lib().chai_cuda_tune_db_save(ctx, db.encode()), ctx)
+        for k in (1, 2, 3):     # a fresh context per k: cold DB, the trained weights
+            dev = ch.Device(config="TuneDB=%s TopK=%d" % (db, k))
+            try:
+                r = T.evaluate(dev.ctx, held)
+            finally:
+                dev.close()
+            by_k[k] = r
+    rows = by_k[2]
+    topk = {k: {"pick_vs_best_geomean": gm(np.array([x["best_us"] / x["pick_us"] for x in r])),
+                "within_5pct": float(np.mean([x["best_us"] / x["pick_us"] >= 1 / 1.05 for x in r])),
+                "cold_start_speedup": sum(x["exhaustive_s"] for x in r) / sum(x["learned_s"] for x in r)}
+            for k, r in by_k.items()}
     q = np.array([r["best_us"] / r["pick_us"] for r in rows])
     qd = np.array([r["best_us"] / r["default_us"] for r in rows])
     ls = sum(r["learned_s"] for r in rows)
@@ -597,7 +612,7 @@ def run_tuner(args, L, ctx, stream):
         "tuner": {"pick_vs_best_geomean": gm(q), "within_5pct": float(np.mean(q >= 1 / 1.05)),
                   "default_vs_best_geomean": gm(qd), "learned_s_total": ls, "exhaustive_s_total": es,
                   "train_samples": len(samples), "train_loss": loss, "train_s": train_s, "sweep_s": sweep_s,
-                  "by_kind": part},
+                  "by_kind": part, "top_k": topk},
         "e2e": None, "roofline": None, "clocks": clk.summary(), "gpu_launches": None,
     }
 

@@ -161,6 +161,25 @@ int launch_gemv_cfg(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int
     return set_error(ctx, CHAI_ERR_UNSUPPORTED, "gemv precision");
 }
 
+template <class T>
+static void preload_gemv_t()
+{
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, chai_gemv_n<T, 4, 1>);
+    cudaFuncGetAttributes(&a, chai_gemv_n<T, 4, 4>);
+    cudaFuncGetAttributes(&a, chai_gemv_n<T, 8, 1>);
+    cudaFuncGetAttributes(&a, chai_gemv_n<T, 8, 4>);
+    cudaFuncGetAttributes(&a, chai_gemv_n<T, 16, 1>);
+    cudaFuncGetAttributes(&a, chai_gemv_n<T, 16, 4>);
+}
+
+// Load every GEMV variant now (see preload_gemm_kernels).
+void preload_gemv_kernels()
+{
+    preload_gemv_t<float>();
+    preload_gemv_t<double>();
+}
+
 int launch_gemv(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha, const void* a,
                 int64_t lda, const void* x, double beta, void* y)
 {

@@ -102,6 +102,42 @@ __global__ void mlp_adam(float* __restrict__ w, const float* __restrict__ g, flo
     w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
+// Inference: the whole network for one sample per CTA in one launch (thread j
+// owns hidden unit j; activations stay in shared memory).  Each dot product
+// runs from zero over the inputs in order and adds the bias last, the same
+// order as the layered training forward pass, so both give identical results.
+__global__ void __launch_bounds__(MLP_H) mlp_infer(const float* __restrict__ params, const float* __restrict__ x,
+                                                   float* __restrict__ out, int n, int w1, int b1, int w2, int b2,
+                                                   int w3, int b3, int w4, int b4)
+{
+    __shared__ float h0[MLP_H], h1[MLP_H], xin[MLP_IN];
+    const int s = blockIdx.x, j = threadIdx.x;
+    if (s >= n) return;
+    if (j < MLP_IN) xin[j] = x[(long long)s * MLP_IN + j];
+    __syncthreads();
+    float acc = 0.0f;
+#pragma unroll
+    for (int i = 0; i < MLP_IN; i++) acc = fmaf(xin[i], __ldg(params + w1 + i * MLP_H + j), acc);
+    h0[j] = fmaxf(acc + __ldg(params + b1 + j), 0.0f);
+    __syncthreads();
+    acc = 0.0f;
+#pragma unroll 8
+    for (int i = 0; i < MLP_H; i++) acc = fmaf(h0[i], __ldg(params + w2 + i * MLP_H + j), acc);
+    h1[j] = fmaxf(acc + __ldg(params + b2 + j), 0.0f);
+    __syncthreads();
+    acc = 0.0f;
+#pragma unroll 8
+    for (int i = 0; i < MLP_H; i++) acc = fmaf(h1[i], __ldg(params + w3 + i * MLP_H + j), acc);
+    __syncthreads();
+    h0[j] = fmaxf(acc + __ldg(params + b3 + j), 0.0f);
+    __syncthreads();
+    if (j == 0) {
+        acc = 0.0f;
+        for (int i = 0; i < MLP_H; i++) acc = fmaf(h0[i], __ldg(params + w4 + i), acc);
+        out[s] = acc + __ldg(params + b4);
+    }
+}
+
 static unsigned blocks_for(long long n) { return (unsigned)((n + 255) / 256); }
 
 Mlp::Mlp(chai_cuda_ctx* ctx) : ctx_(ctx)
@@ -127,6 +163,7 @@ Mlp::~Mlp()
     if (x_) cudaFree(x_);
     if (y_) cudaFree(y_);
     if (part_) cudaFree(part_);
+    if (host_) cudaFreeHost(host_);
 }
 
 int Mlp::ensure(size_t n)
@@ -263,14 +300,29 @@ int Mlp::train(const std::vector<float>& x, const std::vector<float>& y_raw, int
 int Mlp::predict(const std::vector<float>& x, std::vector<double>& out)
 {
     const size_t n = x.size() / MLP_IN;
-    int st = upload(x.data(), nullptr, n);
-    if (st) return st;
-    forward(n);
-    std::vector<float> p(n);
-    CHAI_CUDA_TRY(ctx_, cudaMemcpyAsync(p.data(), acts_[3], n * sizeof(float), cudaMemcpyDeviceToHost, ctx_->stream));
-    CHAI_CUDA_TRY(ctx_, cudaStreamSynchronize(ctx_->stream));
     out.resize(n);
-    for (size_t i = 0; i < n; i++) out[i] = (double)p[i] * scale_ + mean_;
+    if (n == 0) return CHAI_OK;
+    int st = ensure(n);
+    if (st) return st;
+    if (n > host_cap_) {
+        if (host_) cudaFreeHost(host_);
+        host_ = nullptr;
+        host_cap_ = 0;
+        CHAI_CUDA_TRY(ctx_, cudaMallocHost(&host_, n * (MLP_IN + 1) * sizeof(float)));
+        host_cap_ = n;
+    }
+    float* hx = host_;
+    float* hp = host_ + n * MLP_IN;
+    std::copy(x.begin(), x.end(), hx);
+    cudaStream_t s = ctx_->stream;
+    CHAI_CUDA_TRY(ctx_, cudaMemcpyAsync(x_, hx, n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice, s));
+    mlp_infer<<<(unsigned)n, MLP_H, 0, s>>>(params_, x_, acts_[3], (int)n, (int)w_off_[0], (int)b_off_[0],
+                                             (int)w_off_[1], (int)b_off_[1], (int)w_off_[2], (int)b_off_[2],
+                                             (int)w_off_[3], (int)b_off_[3]);
+    CHAI_CUDA_TRY(ctx_, cudaGetLastError());
+    CHAI_CUDA_TRY(ctx_, cudaMemcpyAsync(hp, acts_[3], n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    CHAI_CUDA_TRY(ctx_, cudaStreamSynchronize(s));
+    for (size_t i = 0; i < n; i++) out[i] = (double)hp[i] * scale_ + mean_;
     return CHAI_OK;
 }
 

@@ -36,6 +36,8 @@ private:
     float* x_ = nullptr;
     float* y_ = nullptr;
     double* part_ = nullptr;
+    float* host_ = nullptr;              // pinned staging of inference inputs / outputs
+    size_t host_cap_ = 0;
     size_t cap_ = 0;
     long long step_ = 0;
     float mean_ = 0.0f, scale_ = 1.0f;

@@ -33,6 +33,9 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
 int launch_gemv_cfg(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha, const void* a,
                     int64_t lda, const void* x, double beta, void* y, const GemvCfg* cfg);
 
+void preload_gemm_kernels();
+void preload_gemv_kernels();
+
 // The cost model: features (tuner.cpp) -> 3 x 128 ReLU -> log runtime (mlp.cu).
 constexpr int MLP_IN = 12, MLP_H = 128;
 class Mlp;
@@ -59,7 +62,8 @@ private:
     std::string journal_;
     void* bufs_[3] = {nullptr, nullptr, nullptr};
     size_t buf_bytes_[3] = {0, 0, 0};
-    int time_cfg(const chai_gemm_key& key, chai_gemm_cfg& cfg, int reps);
+    bool preloaded_ = false;
+    int time_cfg(const chai_gemm_key& key, chai_gemm_cfg& cfg, int reps, bool warm);
     int ensure_operands(const chai_gemm_key& key);
 };
 

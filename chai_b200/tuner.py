@@ -139,6 +139,13 @@ def evaluate(ctx, held_out, default_ids=None):
     learned pick and for the default configuration, and the wall time of each
     method (learned: ranking + timing the top k; exhaustive: the sweep)."""
     rows = []
+    # size every operand / scratch buffer for the largest key first, so that
+    # neither method's timing includes a first-touch allocation
+    for gemv in (0, 1):
+        ks = [k for k, _ in held_out if k.is_gemv == gemv]
+        for prec in sorted({k.precision for k in ks}):
+            sub = [k for k in ks if k.precision == prec]
+            sweep(ctx, key(max(k.m for k in sub), max(k.n for k in sub), max(k.k for k in sub), prec, bool(gemv)))
     for k, cfgs in held_out:
         by_id = {cfg_id(c): c.measured_us for c in cfgs}
         best = min(by_id.values())

@@ -13,14 +13,18 @@ Contents
   ops.c             restatement of the interpreter's matmul / GEMV / reduction /
                     gather semantics (interp/InterpMatmulBase.hpp:25-61,
                     interp/InterpAccum.cpp:13-70, interp/InterpGather.hpp:19-44)
+  mlp.py            restatement of the tuner's cost model (features, MLP
+                    forward / backward) for the GPU gradient check
   build_ref.py      recipe compiling the reference's own interpreter and its
-                    Random123 text from the reference sources into oracle/_ref/
+                    Random123 text (bijections and chai's uniform / normal
+                    wrappers) from the reference sources into oracle/_ref/
   ref_driver.cpp    runs named traces through the reference interpreter
-  ref.py            Python access to oracle/_ref (reference interpreter, pins)
 
-Parity pins: the Random123 restatement is checked against the reference's
-generated generator text and the vendored upstream Random123 text
-(tests/test_oracle.py); the array-op restatement is checked against the reference
-interpreter itself and against fixtures it produced (tests/golden/).
+Parity pins (tests/test_oracle.py): the Random123 restatement is checked
+against the reference JIT's generated text -- bijections and every uniform /
+normal wrapper -- and the vendored upstream Random123 text; the array-op
+restatement against the reference interpreter itself (oracle/_ref, when built)
+and against fixtures it produced (tests/golden/, made by
+tests/golden/make_golden.py).
 """
 from .cpu import *  # noqa: F401,F403

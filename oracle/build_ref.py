@@ -174,6 +174,99 @@ def build_r123_pins(force: bool = False) -> None:
     _run(["g++", "-O2", "-fPIC", "-shared", "-w", str(up), "-o", str(up_so)])
 
 
+# C spellings (GCC vector extensions) of the OpenCL vector types and built-ins
+# the generated wrappers use.
+_VEC_TYPES = {"uint": ("uint32_t", (2, 4)), "int": ("int32_t", (2, 4)), "float": ("float", (2, 4)),
+              "ulong": ("uint64_t", (2, 4)), "long": ("int64_t", (2, 4)), "double": ("double", (2, 4))}
+
+
+def _wrap_prelude() -> str:
+    lines = ["#include <stdint.h>", "#include <string.h>", "#include <tgmath.h>",
+             "typedef uint32_t uint; typedef uint64_t ulong; typedef unsigned char uchar;",
+             "static inline uint64_t mul_hi(uint64_t a, uint64_t b)",
+             "{ return (uint64_t)(((unsigned __int128)a * (unsigned __int128)b) >> 64); }"]
+    for name, (ct, widths) in _VEC_TYPES.items():
+        for n in widths:
+            t = "%s%d" % (name, n)
+            lines.append("typedef %s %s __attribute__((vector_size(%d * sizeof(%s))));" % (ct, t, n, ct))
+            lines.append("#define VEC_%s_1(x) ((%s){%s})" % (t, t, ", ".join(["(x)"] * n)))
+            args = ", ".join("a%d" % i for i in range(n))
+            lines.append("#define VEC_%s_%d(%s) ((%s){%s})" % (t, n, args, t, ", ".join("(a%d)" % i for i in range(n))))
+    return "\n".join(lines) + "\n"
+
+
+def _split_args(text: str, start: int):
+    """Top-level argument count of the parenthesised list opening at start."""
+    depth, count, i = 0, 1, start
+    while True:
+        c = text[i]
+        if c == "(":
+            depth += 1
+        elif c == ")":
+            depth -= 1
+            if depth == 0:
+                return count, i
+        elif c == "," and depth == 1:
+            count += 1
+        i += 1
+
+
+def _opencl_to_c(text: str) -> str:
+    """Rewrite the generated OpenCL generator text as C: vector casts and
+    literals, .sN components, convert_* built-ins, static inline functions."""
+    text = "\n".join(l for l in text.splitlines()
+                     if not re.match(r"typedef (ulong|uint|uchar) uint(64|32|8)_t;", l))
+    text = re.sub(r"^inline ", "static inline ", text, flags=re.M)
+    text = re.sub(r"\.s([0-3])\b", r"[\1]", text)
+    text = re.sub(r"convert_(float|double)\(", r"(\1)(", text)
+    text = re.sub(r"convert_((?:float|double)[24])\(([^()]*(?:\([^()]*\))?[^()]*)\)",
+                  r"__builtin_convertvector((\2), \1)", text)
+    pat = re.compile(r"\(((?:u?int|float|u?long|double)[24])\)\(")
+    out, pos = [], 0
+    for m in pat.finditer(text):
+        if m.start() < pos:
+            continue
+        n, _ = _split_args(text, m.end() - 1)
+        out.append(text[pos:m.start()])
+        out.append("VEC_%s_%d(" % (m.group(1), n))
+        pos = m.end()
+    out.append(text[pos:])
+    return "".join(out)
+
+
+def build_r123_wrapper_pins(force: bool = False) -> Path:
+    """Compile the reference JIT's complete generated Random123 text -- the
+    bijections and chai's per-variant uniform / normal wrappers with their
+    key / counter layout (Random123/R123Philox.cpp:288-523,
+    Random123/R123Threefry.cpp:289-535) -- as C with GCC vector types, and
+    export every wrapper as w_<name>(tid, idx, out)."""
+    so = OUT / "libr123_wrappers.so"
+    src_cl = OUT / "r123_jit.cl"
+    if not force and so.exists() and so.stat().st_mtime >= src_cl.stat().st_mtime:
+        return so
+    text = src_cl.read_text()
+    exports = []
+    for m in re.finditer(r"^inline (\w+) ((?:philox|threefry)_(?:uniform|normal)_\d+_\d+)\((uint(?:32|64)_t) tid, "
+                         r"\w+ idx\) \{", text, flags=re.M):
+        rt, name, at = m.groups()
+        exports.append("void w_%s(uint64_t tid, uint64_t idx, void* out) { %s r = %s((%s)tid, (%s)idx); "
+                       "memcpy(out, &r, sizeof r); }" % (name, rt, name, at, at))
+    c_src = OUT / "r123_wrappers.c"
+    c_src.write_text(_wrap_prelude() + _opencl_to_c(text) + "\n" + "\n".join(exports) + "\n")
+    _run(["gcc", "-O1", "-fPIC", "-shared", "-w", "-std=gnu11", "-ffp-contract=off", str(c_src), "-o", str(so),
+          "-lm"])
+    return so
+
+
+def build_all() -> None:
+    """Everything the oracle pins need that this host can build."""
+    build_oracle()
+    if available():
+        build()
+        build_r123_pins()
+        build_r123_wrapper_pins()
+
+
 def build_oracle() -> Path:
     """Compile the oracle's own C restatement (always possible; no reference
     sources needed) into oracle/_build/liboracle.so."""
@@ -191,4 +284,5 @@ if __name__ == "__main__":
     build_oracle()
     build(force="--force" in sys.argv)
     build_r123_pins(force="--force" in sys.argv)
+    build_r123_wrapper_pins(force="--force" in sys.argv)
     print(OUT)

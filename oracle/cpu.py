@@ -16,7 +16,7 @@ U32, I32, F32, F64 = 0, 1, 4, 8
 LAYOUT_CHAI, LAYOUT_COUNTER = 0, 1
 JIT_PI = 3.14159  # M_PI as the reference JIT prints it (6 significant digits)
 
-__all__ = ["lib", "rng_fill", "gemm_f64", "gemm_entries_f64", "gemv_f64", "sum_f32", "dot_f32",
+__all__ = ["lib", "rng_fill", "gemm_f64", "matmul_ref", "matvec_ref", "gemm_entries_f64", "gemv_f64", "sum_f32", "dot_f32",
            "gather2_floor", "kirsch", "philox4x32", "philox2x32", "philox2x64", "threefry4x32",
            "threefry4x32_chai", "threefry2x32", "threefry2x64", "PHILOX", "THREEFRY", "U32", "I32",
            "F32", "F64", "LAYOUT_CHAI", "LAYOUT_COUNTER", "JIT_PI"]
@@ -38,6 +38,8 @@ def lib():
         L.oracle_gemm_entries_f64.argtypes = [C.c_int64, C.c_int64, p, p, C.c_int64, p, p, p]
         L.oracle_gemv_f64.argtypes = [C.c_int64, C.c_int64, p, p, p]
         L.oracle_gemv_f32.argtypes = [C.c_int64, C.c_int64, p, p, p]
+        L.oracle_matmul_ref_f32.argtypes = [C.c_int64] * 4 + [p] * 3
+        L.oracle_matvec_ref_f32.argtypes = [C.c_int64] * 3 + [p] * 3
         L.oracle_sum_f32.argtypes = [C.c_int64, p]
         L.oracle_sum_f32.restype = C.c_double
         L.oracle_dot_f32.argtypes = [C.c_int64, p, p]
@@ -76,6 +78,27 @@ def gemm_f64(A: np.ndarray, B: np.ndarray) -> np.ndarray:
     Cm = np.empty((M, N), dtype=np.float64)
     lib().oracle_gemm_f32_to_f64(M, N, K, _ptr(A), _ptr(B), _ptr(Cm))
     return Cm
+
+
+def matmul_ref(A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    """The reference interpreter's f32 matmul: f32 products accumulated in
+    double, k ascending (interp/InterpMatmulBase.hpp:50-61)."""
+    A = np.ascontiguousarray(A, dtype=np.float32)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    M, Ka = A.shape
+    Kb, N = B.shape
+    out = np.empty((M, N), dtype=np.float32)
+    lib().oracle_matmul_ref_f32(M, N, Ka, Kb, _ptr(A), _ptr(B), _ptr(out))
+    return out
+
+
+def matvec_ref(A: np.ndarray, x: np.ndarray) -> np.ndarray:
+    """The interpreter's f32 matrix-vector product (InterpMatmulBase.hpp:37-47)."""
+    A = np.ascontiguousarray(A, dtype=np.float32)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty(A.shape[0], dtype=np.float32)
+    lib().oracle_matvec_ref_f32(A.shape[0], A.shape[1], x.shape[0], _ptr(A), _ptr(x), _ptr(out))
+    return out
 
 
 def gemm_entries_f64(A, B, rows, cols) -> np.ndarray:

@@ -14,7 +14,7 @@ candidates of that search before timing the top k:
   features (12): log2 M/14, log2 N/14, log2 K/14 (K = 1 for GEMV), split
     precision (fp32 via bf16x3) flag, single-pass tensor-core flag, GEMV flag,
     block_n/256, stages/6, log2(group_m)/6, GEMV warps/16, GEMV unroll/4,
-    log2(M N K)/42
+    wave efficiency (fraction of the last wave of CTAs with work)
   network: 12 -> 128 -> 128 -> 128 -> 1, ReLU on the hidden layers,
     y = x W + b with W stored row-major (in x out)
   target: (log(measured_us) - mean) / scale, loss = mean squared error
@@ -59,8 +59,21 @@ def features(m, n, k, precision, is_gemv, cfg) -> np.ndarray:
     f[8] = np.log2(g) / 6.0 if g > 0 else 0.0
     f[9] = cfg.get("block_m", 0) / 16.0 if is_gemv else 0.0
     f[10] = cfg.get("vec_width", 0) / 4.0 if is_gemv else 0.0
-    f[11] = np.log2(float(m) * n * k) / 42.0
+    f[11] = wave_efficiency(m, n, is_gemv, cfg)
     return f.astype(np.float32)
+
+
+def wave_efficiency(m, n, is_gemv, cfg) -> float:
+    """Fraction of the last wave with work: GEMM tiles of 128 x block_n over 148
+    persistent CTAs; GEMV blocks of `warps` rows, 64 / warps blocks per SM."""
+    if is_gemv:
+        w = max(1, cfg.get("block_m", 0))
+        units = np.ceil(max(1, m) / w)
+        per_wave = 148.0 * max(1, min(32, 64 // w))
+    else:
+        units = np.ceil(max(1, m) / 128.0) * np.ceil(max(1, n) / max(1, cfg.get("block_n", 0)))
+        per_wave = 148.0
+    return units / (np.ceil(units / per_wave) * per_wave)
 
 
 def count() -> int:

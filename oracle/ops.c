@@ -5,8 +5,9 @@
  *
  * Semantics followed:
  *   matmul / GEMM   interp/InterpMatmulBase.hpp:25-61 (row-major, result
- *                   width = B's width, height = A's height; double accumulator;
- *                   GEMM C = alpha*AB + beta*C)
+ *                   width = B's width, height = A's height; f32 products
+ *                   accumulated in double: oracle_matmul_ref_f32; GEMM
+ *                   C = alpha*AB + beta*C)
  *   matvec          interp/InterpMatmulBase.hpp:37-47
  *   sum / mean / dot_product   interp/InterpAccum.cpp:13-70,
  *                   interp/InterpDotprod.cpp:14-60 (double accumulator)
@@ -39,6 +40,41 @@ void oracle_gemm_f32_to_f64(int64_t M, int64_t N, int64_t K, const float* A, con
                 }
             }
         }
+    }
+}
+
+/* The interpreter's matmul arithmetic (interp/InterpMatmulBase.hpp:50-61):
+ * each product of two f32 operands is rounded to f32, then accumulated in
+ * double with k ascending; the f32 result is the double sum rounded.  When the
+ * inner dimensions differ the interpreter wraps both (z % K_a, z % K_b) up to
+ * the larger one. */
+void oracle_matmul_ref_f32(int64_t M, int64_t N, int64_t Ka, int64_t Kb, const float* A, const float* B, float* C)
+{
+    const int64_t K = Ka > Kb ? Ka : Kb;
+    #pragma omp parallel for
+    for (int64_t i = 0; i < M; i++)
+        for (int64_t j = 0; j < N; j++) {
+            double acc = 0.0;
+            for (int64_t z = 0; z < K; z++) {
+                const float p = A[i * Ka + z % Ka] * B[(z % Kb) * N + j];
+                acc += (double)p;
+            }
+            C[i * N + j] = (float)acc;
+        }
+}
+
+/* matrix-vector with the same arithmetic (InterpMatmulBase.hpp:37-47) */
+void oracle_matvec_ref_f32(int64_t M, int64_t Na, int64_t Nx, const float* A, const float* x, float* y)
+{
+    const int64_t N = Na > Nx ? Na : Nx;
+    #pragma omp parallel for
+    for (int64_t i = 0; i < M; i++) {
+        double acc = 0.0;
+        for (int64_t z = 0; z < N; z++) {
+            const float p = A[i * Na + z % Na] * x[z % Nx];
+            acc += (double)p;
+        }
+        y[i] = (float)acc;
     }
 }
 
