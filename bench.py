@@ -724,6 +724,18 @@ def cpu_baseline(args):
 
 # ---------------------------------------------------------------- main
 
+def aggregate_ranks(res, world, reduce_max):
+    """Whole-job figures from one rank's result under weak scaling: every rank
+    processes the same per-GPU workload, the job's step time is the maximum
+    over ranks (reduce_max: the collective), and `value` becomes the units all
+    ranks processed divided by that time."""
+    local_ms = res["ms_per_step"]
+    ms = reduce_max(local_ms)
+    res["value"] = res["value"] * world * local_ms / ms
+    res["ms_per_step"] = ms
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -766,13 +778,12 @@ def main():
     torch.cuda.synchronize()
     res = WORKLOADS[args.workload](args, L, dev.ctx, stream)
     torch.cuda.synchronize()
-    ms = res["ms_per_step"]
     if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-        res["value"] = res["value"] * world * res["ms_per_step"] / ms
-        res["ms_per_step"] = ms
+        def reduce_max(x):
+            t = torch.tensor([x], device="cuda", dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            return float(t.item())
+        aggregate_ranks(res, world, reduce_max)
     if rank == 0:
         line = {"metric": res["metric"], "value": res["value"], "unit": res["unit"], "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],

@@ -142,6 +142,30 @@ template <int OP, class T> __device__ __forceinline__ T f2(T a, T b);
     template <> __device__ __forceinline__ u32 f2<OP, u32>(u32 a, u32 b) { return EXPR; } \
     template <> __device__ __forceinline__ i32 f2<OP, i32>(i32 a, i32 b) { return EXPR; }
 
+// Packed f32 pairs: the element kernels hold 4 consecutive elements per
+// thread; add / sub / mul of f32 operands run as two sm_100 f32x2
+// instructions (round to nearest even per lane, the same IEEE results as the
+// scalar ops, half the instruction issue).
+template <int OP> struct pk2;
+template <> struct pk2<11> { static __device__ __forceinline__ unsigned long long op(unsigned long long a, unsigned long long b)
+    { unsigned long long d; asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; } };
+template <> struct pk2<13> { static __device__ __forceinline__ unsigned long long op(unsigned long long a, unsigned long long b)
+    { unsigned long long d; asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; } };
+template <> struct pk2<14> { static __device__ __forceinline__ unsigned long long op(unsigned long long a, unsigned long long b)
+    { unsigned long long d; asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; } };
+
+template <int OP> __device__ __forceinline__ void f2x4(const float* a, const float* b, float* o)
+{
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        unsigned long long pa, pb, d;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(pa) : "f"(a[2 * h]), "f"(a[2 * h + 1]));
+        asm("mov.b64 %0, {%1, %2};" : "=l"(pb) : "f"(b[2 * h]), "f"(b[2 * h + 1]));
+        d = pk2<OP>::op(pa, pb);
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(o[2 * h]), "=f"(o[2 * h + 1]) : "l"(d));
+    }
+}
+
 CHAI_F2ALL(11, a + b)
 CHAI_F2ALL(13, a * b)
 CHAI_F2ALL(14, a - b)

@@ -51,6 +51,19 @@ template <class T> __device__ __forceinline__ void st4(T* __restrict__ p, const 
     }
 }
 
+// 16 bytes of shared memory at p (16-byte aligned) into o[0 .. 16/sizeof(T)).
+template <class T> __device__ __forceinline__ void lds_vec(const T* p, T* o)
+{
+    if constexpr (sizeof(T) == 4) {
+        const uint4 r = *reinterpret_cast<const uint4*>(p);
+        o[0] = __builtin_bit_cast(T, r.x); o[1] = __builtin_bit_cast(T, r.y);
+        o[2] = __builtin_bit_cast(T, r.z); o[3] = __builtin_bit_cast(T, r.w);
+    } else {
+        const double2 r = *reinterpret_cast<const double2*>(p);
+        o[0] = (T)r.x; o[1] = (T)r.y;
+    }
+}
+
 // Block-wide sum of NRED doubles; thread 0 receives the totals.
 template <int NRED, int NT>
 __device__ __forceinline__ void block_sum(double (&v)[NRED])

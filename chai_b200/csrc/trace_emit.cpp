@@ -83,7 +83,7 @@ static PFN_encodeTiledT tensor_map_encoder()
 }
 
 // stencil tile geometry (outputs per CTA: TX x TY; halo: PX columns, R rows)
-constexpr int ST_TX = 128, ST_TY = 16, ST_PX = 4;
+constexpr int ST_TX = 128, ST_TY = 32, ST_PX = 4;
 
 int Translator::emit_group(const std::vector<int>& roots)
 {
@@ -177,9 +177,18 @@ int Translator::emit_group(const std::vector<int>& roots)
         R = std::max(R, (int)std::llabs(cy));
     }
     for (int src : srcs) tile_bytes += (size_t)(ST_TY + 2 * R) * (ST_TX + 2 * ST_PX) * prec_bytes(nodes_[src].prec);
-    mode2d = mode2d && any_gather && srcs.size() <= 2 && tile_bytes <= 40 * 1024;
+    mode2d = mode2d && any_gather && srcs.size() <= 2 && tile_bytes <= 46 * 1024;
     if (!mode2d) sten.clear();
     const int SH = ST_TY + 2 * R, SW = ST_TX + 2 * ST_PX;
+    std::map<std::pair<int, int>, int> win_lo, win_hi;   // (source tile, row offset) -> column range
+    std::set<std::pair<int, int>> win_done;
+    for (auto& kv : sten) {
+        const int k = (int)(std::find(srcs.begin(), srcs.end(), kv.second.src) - srcs.begin());
+        const std::pair<int, int> wk(k, kv.second.cy);
+        if (!win_lo.count(wk)) { win_lo[wk] = kv.second.cx; win_hi[wk] = kv.second.cx; }
+        win_lo[wk] = std::min(win_lo[wk], kv.second.cx);
+        win_hi[wk] = std::max(win_hi[wk], kv.second.cx);
+    }
     const bool use_tma = mode2d && (W % 4) == 0;
     std::vector<CUtensorMap> maps(srcs.size());
 
@@ -326,6 +335,11 @@ int Translator::emit_group(const std::vector<int>& roots)
                        << T << ")v" << nd.kids[1] << "[j] : (" << T << ")v" << nd.kids[2] << "[j];\n";
                     break;
                 }
+                if (ar == 2 && nd.prec == CHAI_F32 && (nd.op == 11 || nd.op == 13 || nd.op == 14) &&
+                    nodes_[nd.kids[0]].prec == CHAI_F32 && nodes_[nd.kids[1]].prec == CHAI_F32) {
+                    os << "    f2x4<" << nd.op << ">(v" << nd.kids[0] << ", v" << nd.kids[1] << ", v" << i << ");\n";
+                    break;
+                }
                 // operand precision: widest operand (fp-only ops at least f32);
                 // predicates return 1/0 in that precision
                 os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = f" << ar << "<" << nd.op << ", " << T
@@ -337,10 +351,34 @@ int Translator::emit_group(const std::vector<int>& roots)
             }
             case Node::GATHER: {
                 if (sten.count(i)) {
+                    // all gathers of one (source, row offset) share one window of the
+                    // staged row: columns lx + PX + cmin .. lx + PX + 3 + cmax, read with
+                    // 16-byte shared loads where aligned (lx and the tile pitch are
+                    // multiples of 4 elements)
                     const Sten& g = sten[i];
                     const int k = (int)(std::find(srcs.begin(), srcs.end(), g.src) - srcs.begin());
-                    os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = tile" << k << "[(ly + " << R + g.cy << ") * "
-                       << SW << " + lx + j + " << ST_PX + g.cx << "];\n";
+                    const std::pair<int, int> wkey(k, g.cy);
+                    const int cmin = win_lo[wkey], cmax = win_hi[wkey];
+                    const int b0 = ST_PX + cmin, w = 4 + cmax - cmin;
+                    const std::string wn = "w" + std::to_string(k) + "_" + std::to_string(g.cy + 8);
+                    const char* ST = ctype_of(nodes_[g.src].prec);
+                    const int ve = 16 / (int)prec_bytes(nodes_[g.src].prec);
+                    if (!win_done.count(wkey)) {
+                        win_done.insert(wkey);
+                        os << "    " << ST << " " << wn << "[" << w << "]; { const " << ST << "* rowp = tile" << k
+                           << " + (ly + " << R + g.cy << ") * " << SW << " + lx;\n";
+                        for (int t = 0; t < w;) {
+                            if ((b0 + t) % ve == 0 && t + ve <= w) {
+                                os << "      chai_k::lds_vec(rowp + " << b0 + t << ", " << wn << " + " << t << ");\n";
+                                t += ve;
+                            } else {
+                                os << "      " << wn << "[" << t << "] = rowp[" << b0 + t << "];\n";
+                                t++;
+                            }
+                        }
+                        os << "    }\n";
+                    }
+                    os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = " << wn << "[j + " << g.cx - cmin << "];\n";
                     break;
                 }
                 const Node& a = nodes_[nd.kids[0]];

@@ -72,7 +72,12 @@ def test_kirsch_trace_is_one_kernel_with_gathers():
     # every gather is a constant-offset stencil: one 2-D tiled kernel, the
     # source tile staged in shared memory by TMA (wrapped loads at borders)
     assert src.count("__global__") == 1 and src.count("gather_index") == 0
-    assert "tma_load_3d(tile0" in src and src.count("tile0[(ly") == 8
+    assert "tma_load_3d(tile0" in src
+    # the 8 gathers read 3 row windows (row offsets -1, 0, +1), each one
+    # 16-byte shared load plus two edge elements
+    assert src.count("const float* rowp = tile0") == 3 and src.count("chai_k::lds_vec(rowp") == 3
+    # f32 add / sub / mul run as packed f32x2 pairs
+    assert src.count("f2x4<11>") >= 20 and src.count("f2x4<14>") >= 8 and src.count("f2x4<13>") >= 8
 
 
 def test_data_dependent_gather_stays_generic():
