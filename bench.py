@@ -157,17 +157,58 @@ GEMM_PREC = {"fp32": 0, "tf32": 1, "bf16": 2, "bf16x3": 3, "bf16x6": 4}
 TENSOR_MULT = {0: 0, 1: 1, 2: 1, 3: 3, 4: 6}
 
 
+def gemm_operands(L, ctx, n, dist):
+    """f32 n x n operands from the library's own Philox fill (chai layout):
+    uniform[-1, 1) with seeds 1, 2, or N(0, 1) (Box-Muller) with seeds 3, 4."""
+    import torch
+    out = []
+    for seed in ((1, 2) if dist == "uniform" else (3, 4)):
+        t = torch.empty((n, n), device="cuda", dtype=torch.float32)
+        if dist == "uniform":
+            rd = L.chai_rng_desc(1230, 4, 0, 4, seed, n, n, 1, 1, -1.0, 1.0)
+        else:
+            rd = L.chai_rng_desc(1230, 4, 1, 4, seed, n, n, 1, 0, 0.0, 1.0)
+        L.check(L.lib().chai_cuda_rng_fill(ctx, C.byref(rd), C.c_void_p(t.data_ptr())), ctx)
+        if dist == "normal":
+            # chai's Box-Muller gives +-inf for the rare u = 0 draws (about one
+            # in 2^25); the precision sweep needs finite operands
+            t.nan_to_num_(nan=0.0, posinf=0.0, neginf=0.0)
+        out.append(t)
+    return out
+
+
+def gemm_error(A, B, Cm, samples=4096, seed=0):
+    """Error of C against the FP64 product on `samples` random entries (FP64
+    dot products on the GPU): max |C - C64| / (|A| |B|)_ij (componentwise-bound
+    normalised) and max |C - C64| / |C64|."""
+    import torch
+    n_m, n_n = Cm.shape
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    rows = torch.randint(0, n_m, (samples,), device="cuda", generator=g)
+    cols = torch.randint(0, n_n, (samples,), device="cuda", generator=g)
+    num, bnd = [], []
+    for c0 in range(0, samples, 512):
+        r, c = rows[c0:c0 + 512], cols[c0:c0 + 512]
+        a = A[r].double()
+        b = B[:, c].double().t()
+        num.append((a * b).sum(1))
+        bnd.append((a.abs() * b.abs()).sum(1))
+    c64 = torch.cat(num)
+    bound = torch.cat(bnd)
+    got = Cm[rows, cols].double()
+    err = (got - c64).abs()
+    ok = torch.isfinite(got)
+    return {"max_err_normalized": float((err / bound.clamp_min(1e-300)).max()),
+            "max_rel_err": float((err / c64.abs().clamp_min(1e-300)).max()),
+            "finite": bool(ok.all()), "error_samples": samples}
+
+
 def run_gemm(args, L, ctx, stream):
     import torch
     n = args.size or 16384
     prec = GEMM_PREC[args.precision]
-    # seeded uniform[-1, 1) operands from the library's own Philox fill (chai layout, seeds 1 and 2)
-    A = torch.empty((n, n), device="cuda", dtype=torch.float32)
-    B = torch.empty((n, n), device="cuda", dtype=torch.float32)
+    A, B = gemm_operands(L, ctx, n, "uniform")
     Cm = torch.empty((n, n), device="cuda", dtype=torch.float32)
-    for t, seed in ((A, 1), (B, 2)):
-        rd = L.chai_rng_desc(1230, 4, 0, 4, seed, n, n, 1, 1, -1.0, 1.0)
-        L.check(L.lib().chai_cuda_rng_fill(ctx, C.byref(rd), C.c_void_p(t.data_ptr())), ctx)
     d = L.chai_gemm_desc(prec, 0, 0, 0, n, n, n, A.data_ptr(), n, B.data_ptr(), n, Cm.data_ptr(), n, 1.0, 0.0, 1,
                          0, 0, 0)
 
@@ -184,6 +225,7 @@ def run_gemm(args, L, ctx, stream):
     ms = sum(ts) / len(ts)
     k_ms, k_n = kstats(L, ctx, "gemm_tc")
     kern_ms = k_ms / k_n if k_n else None
+    err = gemm_error(A, B, Cm)
     # e2e through the public entry points: pinned host A, B in, C out each step
     Ah = A.cpu().pin_memory()
     Bh = B.cpu().pin_memory()
@@ -230,11 +272,43 @@ def run_gemm(args, L, ctx, stream):
         "config": {"workload": "square GEMM M=N=K=%d, f32 operands uniform[-1,1) (chai Philox seeds 1,2), %s"
                    % (n, args.precision), "m": n, "n": n, "k": n,
                    "l2": "operands (%d MiB each) larger than L2" % (n * n * 4 >> 20),
-                   "includes": "operand split/transposition prepass + tcgen05 GEMM"},
+                   "includes": "operand split/transposition prepass + tcgen05 GEMM", "error_vs_fp64": err},
         "e2e": {"value": flops / (e_ms * 1e-3) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": 2 * n * n * 4,
                 "d2h_bytes_per_step": n * n * 4},
         "roofline": roof, "clocks": clk.summary(), "gpu_launches": args.steps * (1 if prec in (0, 2) else 3),
     }
+
+
+def gemm_sweep(args, L, ctx, stream, path):
+    """The GEMM precision sweep: M = N = K in {1024 .. 16384}, uniform[-1, 1)
+    and N(0, 1) operands, every arithmetic; time (CUDA events, median of 3
+    after a warm-up) and error against FP64 per shape.  Written to `path`."""
+    import torch
+    rows = []
+    for n in (1024, 2048, 4096, 8192, 16384):
+        for dist in ("uniform", "normal"):
+            A, B = gemm_operands(L, ctx, n, dist)
+            Cm = torch.empty((n, n), device="cuda", dtype=torch.float32)
+            for name in ("fp32", "tf32", "bf16", "bf16x3", "bf16x6"):
+                if name == "fp32" and n > 8192 and dist == "normal":
+                    continue
+                d = L.chai_gemm_desc(GEMM_PREC[name], 0, 0, 0, n, n, n, A.data_ptr(), n, B.data_ptr(), n,
+                                     Cm.data_ptr(), n, 1.0, 0.0, 1, 0, 0, 0)
+
+                def step():
+                    L.check(L.lib().chai_cuda_gemm(ctx, C.byref(d)), ctx)
+                step()
+                ts = time_events(step, 3, stream)
+                ms = statistics.median(ts)
+                row = {"n": n, "dist": dist, "precision": name, "ms": ms,
+                       "tflops": 2.0 * n ** 3 / (ms * 1e-3) / 1e12}
+                row.update(gemm_error(A, B, Cm, samples=2048))
+                rows.append(row)
+                print(json.dumps(row), file=sys.stderr)
+            del A, B, Cm
+            torch.cuda.empty_cache()
+    with open(path, "w") as f:
+        json.dump(rows, f, indent=1)
 
 
 def mc_expr(ch, g, W, H):
@@ -777,6 +851,8 @@ def main():
         pg.barrier()
     torch.cuda.synchronize()
     res = WORKLOADS[args.workload](args, L, dev.ctx, stream)
+    if args.sweep and args.workload == "gemm":
+        gemm_sweep(args, L, dev.ctx, stream, args.sweep)
     torch.cuda.synchronize()
     if pg:
         def reduce_max(x):

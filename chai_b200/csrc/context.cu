@@ -154,6 +154,8 @@ static void parse_config(chai::Config& c, const char* text)
             c.tuner_mode = (v == "exhaustive") ? CHAI_TUNE_EXHAUSTIVE : CHAI_TUNE_LEARNED;
         } else if (k == "TopK") {
             c.top_k = std::max(1, atoi(v.c_str()));
+        } else if (k == "PlanCache") {
+            c.plan_cache = v != "0" && v != "off";
         } else if (k == "TuneJournal") {
             c.tune_journal = v;
         } else if (k == "TuneDB") {
@@ -252,6 +254,12 @@ int chai_cuda_shutdown(chai_cuda_ctx* ctx)
 int chai_cuda_kernel_stats(chai_cuda_ctx* ctx, const char* name, double* total_ms, uint64_t* launches, int reset)
 {
     if (!ctx || !name) return CHAI_ERR_INVALID;
+    if (std::string(name) == "plan_replay") {      // evaluations replayed from the plan cache
+        if (total_ms) *total_ms = 0;
+        if (launches) *launches = ctx->plan_hits;
+        if (reset) ctx->plan_hits = 0;
+        return CHAI_OK;
+    }
     CHAI_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     auto& st = ctx->kstats[name];
     for (auto& p : st.pending) {

@@ -29,11 +29,13 @@ struct Config {
     int top_k = 2;                           // learned tuner: configurations timed
     std::string tune_db;
     std::string tune_journal;                // crash-safe TRY / OK markers of every timing
+    bool plan_cache = true;                  // replay recorded plans of repeated traces
     std::string jit_cache;
 };
 
 class Jit;      // runtime compilation cache (jit.cpp)
 class Tuner;    // learned / exhaustive GEMM tuner (tuner.cpp)
+struct Plan;    // recorded device operations of a trace (plan.h)
 
 }  // namespace chai
 
@@ -61,6 +63,8 @@ struct chai_cuda_ctx {
     struct KStat { double ms = 0; uint64_t launches = 0; std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending; };
     std::map<std::string, KStat> kstats;
     std::vector<cudaEvent_t> event_pool;
+    std::unordered_map<uint64_t, std::shared_ptr<chai::Plan>> plans;   // plan cache, by key hash
+    uint64_t plan_hits = 0;
 };
 
 namespace chai {

@@ -472,8 +472,14 @@ int Translator::run(const chai_trace_desc* t, const chai_buffer_binding* binds, 
         if (n.storage_buffer == b->second.buffer) continue;
         Buffer* dst = find_buffer(ctx_, b->second.buffer);
         if (!dst) return fail(CHAI_ERR_NOT_FOUND, "output buffer");
-        CHAI_CUDA_TRY(ctx_, cudaMemcpyAsync(dst->ptr, n.dev, node_bytes(n), cudaMemcpyDeviceToDevice,
-                                            ctx_->stream));
+        note_buffer(b->second.buffer, node_bytes(n), true);
+        Step cs;
+        cs.kind = Step::COPY;
+        cs.a = ref_of(dst->ptr);
+        cs.b = ref_of(n.dev);
+        cs.bytes = node_bytes(n);
+        int st = exec(cs);
+        if (st) return st;
     }
     return CHAI_OK;
 }
@@ -497,6 +503,7 @@ int Translator::assign_storage(int i)
         if (b->bytes < node_bytes(n)) return fail(CHAI_ERR_INVALID, "input buffer too small");
         n.dev = b->ptr;
         n.storage_buffer = n.buffer;
+        note_buffer(n.buffer, node_bytes(n), false);
         return CHAI_OK;
     }
     // the node is the final value of a bound variable -> its buffer
@@ -506,6 +513,7 @@ int Translator::assign_storage(int i)
         if (b == bindings_.end()) continue;
         int st = alloc_buffer(ctx_, b->second.buffer, node_bytes(n));
         if (st) return st;
+        note_buffer(b->second.buffer, node_bytes(n), true);
         Buffer* buf = find_buffer(ctx_, b->second.buffer);
         n.dev = buf->ptr;
         n.storage_buffer = b->second.buffer;
@@ -515,6 +523,7 @@ int Translator::assign_storage(int i)
     const size_t bytes = std::max<size_t>(256, (node_bytes(n) + 255) & ~size_t(255));
     CHAI_CUDA_TRY(ctx_, cudaMallocAsync(&p, bytes, ctx_->stream));
     temps_.push_back(p);
+    temp_sizes_.push_back(bytes);
     n.dev = p;
     return CHAI_OK;
 }

@@ -3,11 +3,13 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <string>
 #include <utility>
 #include <vector>
 
 #include "chai_b200.h"
+#include "plan.h"
 
 struct chai_cuda_ctx;
 
@@ -58,6 +60,13 @@ public:
     std::string all_sources;
     size_t kernels_launched = 0;
 
+    // plan cache (plan.h): record the device operations of this run with the
+    // provenance of their pointers, or replay a recorded plan
+    void begin_record(const std::vector<uint64_t>& buffer_ids);
+    std::unique_ptr<Plan> take_plan();          // null when the run is not replayable
+    // 0: replayed; > 0: the plan does not fit these buffers (translate instead); < 0: error
+    int replay(const Plan& p, const std::vector<uint64_t>& buffer_ids);
+
 private:
     chai_cuda_ctx* ctx_;
     bool dry_ = false;
@@ -73,6 +82,16 @@ private:
     std::vector<void*> temps_;
     uint32_t slots_ = 1;
     uint32_t unsupported_op_ = 0;
+    // plan recording / replay
+    bool recording_ = false, replaying_ = false, cacheable_ = true;
+    std::unique_ptr<Plan> plan_;
+    std::vector<uint64_t> buf_ids_;
+    std::vector<size_t> temp_sizes_;
+    Ref ref_of(const void* p);
+    void* ptr_of(const Ref& r) const;
+    void note_buffer(uint64_t id, size_t bytes, bool alloc);
+    int exec(Step& s);
+    int run_step(const Step& s);
 
     int fail(int st, const std::string& msg);
     int add(Node n);

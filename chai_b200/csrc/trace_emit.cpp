@@ -190,7 +190,7 @@ int Translator::emit_group(const std::vector<int>& roots)
         win_hi[wk] = std::max(win_hi[wk], kv.second.cx);
     }
     const bool use_tma = mode2d && (W % 4) == 0;
-    std::vector<CUtensorMap> maps(srcs.size());
+    std::vector<TmapRec> tmaps;
 
     std::ostringstream os;
     std::vector<KArg> args;
@@ -550,55 +550,65 @@ int Translator::emit_group(const std::vector<int>& roots)
     if (mode2d) {
         args.push_back({KArg::PTR, ctx_->status_word, 0});
         for (size_t k = 0; k < srcs.size(); k++) {
-            memset(&maps[k], 0, sizeof(CUtensorMap));
+            TmapRec m;
             if (use_tma) {
                 const Node& a = nodes_[srcs[k]];
-                PFN_encodeTiledT enc = tensor_map_encoder();
-                if (!enc) return fail(CHAI_ERR_NO_DEVICE, "cuTensorMapEncodeTiled unavailable");
-                const CUtensorMapDataType dt = a.prec == CHAI_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
-                                               : a.prec == CHAI_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
-                                               : a.prec == CHAI_I32 ? CU_TENSOR_MAP_DATA_TYPE_INT32
-                                                                    : CU_TENSOR_MAP_DATA_TYPE_UINT32;
                 const size_t eb = prec_bytes(a.prec);
-                cuuint64_t dims[3] = {(cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.slots};
-                cuuint64_t strides[2] = {(cuuint64_t)(a.W * eb), (cuuint64_t)(a.W * a.H * eb)};
-                cuuint32_t box[3] = {(cuuint32_t)SW, (cuuint32_t)SH, 1};
-                cuuint32_t estr[3] = {1, 1, 1};
-                if ((reinterpret_cast<uintptr_t>(a.dev) & 15) != 0)
-                    return fail(CHAI_ERR_INVALID, "stencil source not 16-byte aligned");
-                CUresult r = enc(&maps[k], dt, 3, a.dev, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-                if (r != CUDA_SUCCESS) return fail(CHAI_ERR_INVALID, "stencil tensor map encoding failed");
+                m.encode = true;
+                m.dt = a.prec == CHAI_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                       : a.prec == CHAI_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                       : a.prec == CHAI_I32 ? CU_TENSOR_MAP_DATA_TYPE_INT32
+                                            : CU_TENSOR_MAP_DATA_TYPE_UINT32;
+                m.dims[0] = a.W; m.dims[1] = a.H; m.dims[2] = a.slots;
+                m.strides[0] = a.W * eb; m.strides[1] = a.W * a.H * eb;
+                m.box[0] = (uint32_t)SW; m.box[1] = (uint32_t)SH; m.box[2] = 1;
+                m.base = ref_of(a.dev);
             }
-            args.push_back({KArg::REF, &maps[k], 0});
+            tmaps.push_back(m);
+            args.push_back({KArg::REF, nullptr, 0});
         }
     }
     for (size_t k = 0; k < n_checked; k++)
         if (args[k].kind == KArg::PTR && !args[k].ptr)
             return fail(CHAI_ERR_INVALID, "trace kernel operand without storage");
-    std::vector<void*> ptrs(args.size());
-    for (size_t k = 0; k < args.size(); k++)
-        ptrs[k] = args[k].kind == KArg::PTR ? (void*)&args[k].ptr
-                  : args[k].kind == KArg::REF ? args[k].ptr : (void*)&args[k].v;
-    cudaEvent_t kev[2];
-    ktime_begin(ctx_, "trace", kev);
-    const dim3 grid = mode2d ? dim3((unsigned)gx, (unsigned)gy, S) : dim3((unsigned)gx, S, 1);
-    st = ctx_->jit->launch(fn, grid, dim3(256, 1, 1), 0, ptrs.data());
+    Step ks;
+    ks.kind = Step::KERNEL;
+    ks.fn = fn;
+    ks.grid = mode2d ? dim3((unsigned)gx, (unsigned)gy, S) : dim3((unsigned)gx, S, 1);
+    ks.block = dim3(256, 1, 1);
+    ks.scratch_need = nred ? (size_t)nred * S * nblocks * sizeof(double) : 0;
+    for (size_t k = 0; k < args.size(); k++) {
+        Step::Arg a;
+        if (args[k].kind == KArg::I64) {
+            a.kind = Step::Arg::I64;
+            a.v = args[k].v;
+        } else if (args[k].kind == KArg::PTR) {
+            a.kind = Step::Arg::PTR;
+            a.r = ref_of(args[k].ptr);
+        } else {
+            a.kind = Step::Arg::TMAP;
+            a.map = (int)ks.maps.size();
+            ks.maps.push_back(tmaps[ks.maps.size()]);
+        }
+        ks.args.push_back(a);
+    }
+    st = exec(ks);
     if (st) return st;
-    ktime_end(ctx_, "trace", kev);
     kernels_launched++;
     if (nred) {
-        std::vector<void*> outs;
-        std::vector<int> precs;
-        std::vector<double> scales;
+        Step cs;
+        cs.kind = Step::COMBINE;
+        cs.partials = ref_of(partials);
+        cs.nblocks = (int)nblocks;
+        cs.nred = nred;
+        cs.slots = (int)S;
         for (int r : reds) {
             const Node& nd = nodes_[r];
-            outs.push_back(nd.dev);
-            precs.push_back(nd.prec);
-            scales.push_back(nd.op == 131 ? 1.0 / (double)n : 1.0);
+            cs.outs.push_back(ref_of(nd.dev));
+            cs.precs.push_back(nd.prec);
+            cs.scales.push_back(nd.op == 131 ? 1.0 / (double)n : 1.0);
         }
-        st = launch_combine(ctx_, partials, (int)nblocks, nred, (int)S, outs.data(), precs.data(), scales.data());
+        st = exec(cs);
         if (st) return st;
         kernels_launched++;
     }
@@ -612,7 +622,15 @@ int Translator::emit_linalg(int i)
     if (nd.kind == Node::TRANSPOSE) {
         const Node& a = nodes_[nd.kids[0]];
         kernels_launched++;
-        return launch_transpose(ctx_, a.prec, a.dev, nd.dev, (int64_t)a.W, (int64_t)a.H, a.slots);
+        Step ts;
+        ts.kind = Step::TRANSPOSE;
+        ts.prec = a.prec;
+        ts.a = ref_of(a.dev);
+        ts.b = ref_of(nd.dev);
+        ts.w = (int64_t)a.W;
+        ts.h = (int64_t)a.H;
+        ts.nslots = a.slots;
+        return exec(ts);
     }
     const Node& l = nodes_[nd.kids[0]];
     const Node& r = nodes_[nd.kids[1]];
@@ -628,7 +646,13 @@ int Translator::emit_linalg(int i)
     if (nd.kind == Node::MATMULG) {
         const Node& c = nodes_[nd.kids[2]];
         if (c.prec != prec) return fail(CHAI_ERR_UNSUPPORTED, "matmul C precision");
-        CHAI_CUDA_TRY(ctx_, cudaMemcpyAsync(nd.dev, c.dev, node_bytes(nd), cudaMemcpyDeviceToDevice, ctx_->stream));
+        Step cp;
+        cp.kind = Step::COPY;
+        cp.a = ref_of(nd.dev);
+        cp.b = ref_of(c.dev);
+        cp.bytes = node_bytes(nd);
+        int st = exec(cp);
+        if (st) return st;
         alpha = nd.alpha;
         beta = nd.beta;
     }
@@ -643,7 +667,13 @@ int Translator::emit_linalg(int i)
         d.c = nd.dev; d.ldc = (int64_t)nd.W;
         d.alpha = alpha; d.beta = beta;
         d.batch = batch; d.stride_a = sl; d.stride_b = sr; d.stride_c = so;
-        return launch_gemm(ctx_, &d);
+        Step gs;
+        gs.kind = Step::GEMM;
+        gs.desc = d;
+        gs.a = ref_of(d.a);
+        gs.b = ref_of(d.b);
+        gs.c = ref_of(d.c);
+        return exec(gs);
     }
     // matrix-vector / vector-matrix / outer product: per slot
     for (int64_t s = 0; s < batch; s++) {
@@ -657,13 +687,30 @@ int Translator::emit_linalg(int i)
             d.m = (int64_t)l.W; d.n = (int64_t)r.W; d.k = 1;
             d.a = A; d.lda = 1; d.b = B; d.ldb = (int64_t)r.W; d.c = C; d.ldc = (int64_t)r.W;
             d.alpha = alpha; d.beta = beta; d.batch = 1;
-            st = launch_gemm(ctx_, &d);
-        } else if (r.H == 1) {
-            if (l.W != r.W) return fail(CHAI_ERR_INVALID, "matvec length differs");
-            st = launch_gemv(ctx_, prec, 0, (int64_t)l.H, (int64_t)l.W, alpha, A, (int64_t)l.W, B, beta, C);
+            Step gs;
+            gs.kind = Step::GEMM;
+            gs.desc = d;
+            gs.a = ref_of(d.a);
+            gs.b = ref_of(d.b);
+            gs.c = ref_of(d.c);
+            st = exec(gs);
         } else {
-            if (l.W != r.H) return fail(CHAI_ERR_INVALID, "vecmat length differs");
-            st = launch_gemv(ctx_, prec, 1, (int64_t)r.H, (int64_t)r.W, alpha, B, (int64_t)r.W, A, beta, C);
+            Step vs;
+            vs.kind = Step::GEMV;
+            vs.prec = prec;
+            vs.alpha = alpha;
+            vs.beta = beta;
+            vs.c = ref_of(C);
+            if (r.H == 1) {
+                if (l.W != r.W) return fail(CHAI_ERR_INVALID, "matvec length differs");
+                vs.trans = 0; vs.m = (int64_t)l.H; vs.n = (int64_t)l.W; vs.lda = (int64_t)l.W;
+                vs.a = ref_of(A); vs.b = ref_of(B);
+            } else {
+                if (l.W != r.H) return fail(CHAI_ERR_INVALID, "vecmat length differs");
+                vs.trans = 1; vs.m = (int64_t)r.H; vs.n = (int64_t)r.W; vs.lda = (int64_t)r.W;
+                vs.a = ref_of(B); vs.b = ref_of(A);
+            }
+            st = exec(vs);
         }
         if (st) return st;
     }
@@ -679,18 +726,34 @@ int Translator::do_read(int i)
     size_t need = rd.read_kind == 0 ? vl * eb * v.slots : node_bytes(v);
     int st = alloc_buffer(ctx_, rd.buffer, need);
     if (st) return st;
+    note_buffer(rd.buffer, need, true);
     Buffer* dst = find_buffer(ctx_, rd.buffer);
     if (rd.read_kind == 0) {
         // read_scalar: the reference's FrontMem holds vecLength partials that
         // the client adds (api/ArrayFP.cpp:86-104); here the first is the
         // full value and the rest are zero.
-        CHAI_CUDA_TRY(ctx_, cudaMemsetAsync(dst->ptr, 0, need, ctx_->stream));
-        CHAI_CUDA_TRY(ctx_, cudaMemcpy2DAsync(dst->ptr, vl * eb, v.dev, (size_t)(v.W * v.H) * eb, eb, v.slots,
-                                              cudaMemcpyDeviceToDevice, ctx_->stream));
-    } else {
-        CHAI_CUDA_TRY(ctx_, cudaMemcpyAsync(dst->ptr, v.dev, need, cudaMemcpyDeviceToDevice, ctx_->stream));
+        Step ms;
+        ms.kind = Step::MEMSET;
+        ms.a = ref_of(dst->ptr);
+        ms.bytes = need;
+        st = exec(ms);
+        if (st) return st;
+        Step cs;
+        cs.kind = Step::COPY2D;
+        cs.a = ref_of(dst->ptr);
+        cs.dpitch = vl * eb;
+        cs.b = ref_of(v.dev);
+        cs.spitch = (size_t)(v.W * v.H) * eb;
+        cs.width = eb;
+        cs.height = v.slots;
+        return exec(cs);
     }
-    return CHAI_OK;
+    Step cs;
+    cs.kind = Step::COPY;
+    cs.a = ref_of(dst->ptr);
+    cs.b = ref_of(v.dev);
+    cs.bytes = need;
+    return exec(cs);
 }
 
 }  // namespace chai
@@ -703,11 +766,39 @@ extern "C" int chai_cuda_evaluate(chai_cuda_ctx* ctx, const chai_trace_desc* t, 
     if (!ctx || !t || (!t->stmts && t->n_stmts) || (!b && nb)) return CHAI_ERR_INVALID;
     if (fault_injected("evaluate")) return set_error(ctx, CHAI_ERR_INJECTED, "injected evaluate failure");
     cudaSetDevice(ctx->device);
+    std::vector<uint64_t> key, ids;
+    uint64_t h = 0;
+    if (ctx->cfg.plan_cache) {
+        plan_key(t, b, nb, key, ids);
+        h = 1469598103934665603ull;                       // FNV-1a over the key words
+        for (uint64_t w : key) { h ^= w; h *= 1099511628211ull; }
+        auto it = ctx->plans.find(h);
+        if (it != ctx->plans.end() && it->second->key == key) {
+            Translator tr(ctx);
+            int st = tr.replay(*it->second, ids);
+            if (st < 0) return st;
+            if (st == 0) {
+                cudaError_t e = cudaGetLastError();
+                if (e != cudaSuccess) return cuda_status(ctx, e, "evaluate");
+                ctx->plan_hits++;
+                return CHAI_OK;
+            }
+        }
+    }
     Translator tr(ctx);
+    if (ctx->cfg.plan_cache) tr.begin_record(ids);
     int st = tr.run(t, b, nb);
     if (st) return st;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(ctx, e, "evaluate");
+    if (ctx->cfg.plan_cache) {
+        std::unique_ptr<Plan> p = tr.take_plan();
+        if (p) {
+            if (ctx->plans.size() >= 1024) ctx->plans.clear();
+            p->key = std::move(key);
+            ctx->plans[h] = std::shared_ptr<Plan>(std::move(p));
+        }
+    }
     return CHAI_OK;
 }
 

@@ -83,7 +83,11 @@ const char* chai_cuda_last_error(chai_cuda_ctx* ctx);
 /* Device time of a hot kernel ("gemm_tc", "trace", "gemv") accumulated over
  * its launches, measured with CUDA events on the context stream when the
  * process runs with CHAI_KERNEL_TIMING=1 (the counterpart of the reference's
- * per-dispatch timing, runtime/Scheduler.cpp:198-220). */
+ * per-dispatch timing, runtime/Scheduler.cpp:198-220).  The name
+ * "plan_replay" reports in *launches the number of evaluations replayed from
+ * the plan cache (config PlanCache=1, the default: a trace whose cells,
+ * scalars, shapes and bindings repeat an earlier one re-issues its recorded
+ * device operations on its own buffers without translating again). */
 int chai_cuda_kernel_stats(chai_cuda_ctx* ctx, const char* name, double* total_ms, uint64_t* launches,
                            int reset);
 /* Run subsequent work on an external cudaStream_t (NULL = the context's own). */
