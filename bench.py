@@ -153,8 +153,8 @@ def traffic(name):
     return None
 
 
-GEMM_PREC = {"fp32": 0, "tf32": 1, "bf16": 2, "bf16x3": 3, "bf16x6": 4}
-TENSOR_MULT = {0: 0, 1: 1, 2: 1, 3: 3, 4: 6}
+GEMM_PREC = {"fp32": 0, "tf32": 1, "bf16": 2, "bf16x3": 3, "bf16x6": 4, "fp8": 5}
+TENSOR_MULT = {0: 0, 1: 1, 2: 1, 3: 3, 4: 6, 5: 1}
 
 
 def gemm_operands(L, ctx, n, dist):
@@ -262,9 +262,14 @@ def run_gemm(args, L, ctx, stream):
     roof = None
     if prec and kern_ms:
         achieved = tensor_flops / (kern_ms * 1e-3) / 1e12
-        roof = {"bound": "tensor", "achieved": achieved, "peak": P["bf16_tflops"], "unit": "TFLOP/s",
-                "frac": achieved / P["bf16_tflops"], "traffic": traffic("gemm_tc_%s_%d" % (args.precision, n)),
-                "peak_source": "%s (bf16 dense, burst)" % kind, "kernel": "chai_gemm_tc_kernel",
+        # the tensor pipe's dense rate: tf32 half of bf16, fp8 twice bf16
+        rate = {1: 0.5, 5: 2.0}.get(prec, 1.0)
+        peak = P["bf16_tflops"] * rate
+        src = "%s (bf16 dense, burst)" % kind if rate == 1.0 else \
+            "%s bf16 dense burst x %g (the %s rate)" % (kind, rate, args.precision)
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": traffic("gemm_tc_%s_%d" % (args.precision, n)),
+                "peak_source": src, "kernel": "chai_gemm_tc_kernel",
                 "kernel_ms": kern_ms, "algorithmic_flops": tensor_flops}
     return {
         "metric": "GEMM TFLOP/s at err vs FP32", "unit": "TFLOP/s", "value": flops / (ms * 1e-3) / 1e12,
@@ -275,7 +280,7 @@ def run_gemm(args, L, ctx, stream):
                    "includes": "operand split/transposition prepass + tcgen05 GEMM", "error_vs_fp64": err},
         "e2e": {"value": flops / (e_ms * 1e-3) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": 2 * n * n * 4,
                 "d2h_bytes_per_step": n * n * 4},
-        "roofline": roof, "clocks": clk.summary(), "gpu_launches": args.steps * (1 if prec in (0, 2) else 3),
+        "roofline": roof, "clocks": clk.summary(), "gpu_launches": args.steps * {0: 1, 5: 6}.get(prec, 3),
     }
 
 
@@ -289,7 +294,7 @@ def gemm_sweep(args, L, ctx, stream, path):
         for dist in ("uniform", "normal"):
             A, B = gemm_operands(L, ctx, n, dist)
             Cm = torch.empty((n, n), device="cuda", dtype=torch.float32)
-            for name in ("fp32", "tf32", "bf16", "bf16x3", "bf16x6"):
+            for name in ("fp32", "tf32", "bf16", "bf16x3", "bf16x6", "fp8"):
                 if name == "fp32" and n > 8192 and dist == "normal":
                     continue
                 d = L.chai_gemm_desc(GEMM_PREC[name], 0, 0, 0, n, n, n, A.data_ptr(), n, B.data_ptr(), n,

@@ -32,6 +32,7 @@
 // copies, releases TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -66,7 +67,7 @@ struct TcShape {
     static constexpr int SMEM_BYTES = STAGES * (A_STAGE + B_STAGE) + 1024 /*align*/ + 256 /*barriers*/;
 };
 
-enum Kind { KIND_BF16 = 0, KIND_TF32 = 1 };
+enum Kind { KIND_BF16 = 0, KIND_TF32 = 1, KIND_FP8 = 2 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p)
 {
@@ -148,7 +149,8 @@ __device__ __forceinline__ unsigned instr_desc()
 {
     unsigned d = 0;
     d |= 1u << 4;                                   // C format F32
-    const unsigned fmt = KIND == KIND_TF32 ? 2u : 1u;   // BF16 = 1, TF32 = 2
+    // kind::f16: BF16 = 1; kind::tf32: TF32 = 2; kind::f8f6f4: E4M3 = 0
+    const unsigned fmt = KIND == KIND_TF32 ? 2u : KIND == KIND_FP8 ? 0u : 1u;
     d |= fmt << 7;                                  // A format
     d |= fmt << 10;                                 // B format
     d |= (unsigned)(BN >> 3) << 17;                 // N / 8
@@ -163,6 +165,10 @@ __device__ __forceinline__ void mma(unsigned tmem, unsigned long long a, unsigne
     if (KIND == KIND_TF32)
         asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+                     ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    else if (KIND == KIND_FP8)
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}"
                      ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
     else
         asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -212,6 +218,11 @@ struct EpiArgs {
     int m, n;
     float alpha, beta;
     int vec_ok;        // 16-byte aligned rows of C
+    // FP8: dequantisation scales, one per 128-row tile of A and per
+    // 128-column block of B (per batch entry: tiles_m and nb128 of them)
+    const float* sa;
+    const float* sb;
+    int nb128;
 };
 
 struct TileGrid {
@@ -354,7 +365,7 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
         // ------------------------------------------------------------ producer
         if (lane == 0) {
             long long it = 0, issued = 0;
-            const int kx_mul = KB_BYTES / (KIND == KIND_TF32 ? 4 : 2);
+            const int kx_mul = KB_BYTES / (KIND == KIND_TF32 ? 4 : KIND == KIND_FP8 ? 1 : 2);
             for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
                 const TileInfo ti = tile_info<GROUPED, BN>(t, tg, ep, kblocks, groups, ngroups);
                 for (int kb = 0; kb < ti.kblocks; kb++, it++) {
@@ -453,8 +464,11 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
                 }
                 const int col = tn * BN + c0;
                 if (!do_store || row >= ti.m || col >= ti.n) continue;
+                float scale = ep.alpha;
+                if (KIND == KIND_FP8)
+                    scale *= ep.sa[(long long)ti.tb * tg.tiles_m + ti.tm] * ep.sb[(long long)ti.tb * ep.nb128 + col / 128];
 #pragma unroll
-                for (int i = 0; i < 64; i++) v[i] *= ep.alpha;
+                for (int i = 0; i < 64; i++) v[i] *= scale;
                 if (ti.vec_ok && col + 64 <= ti.n) {
                     float4* p = reinterpret_cast<float4*>(crow + col);
 #pragma unroll
@@ -625,6 +639,125 @@ __global__ void transpose_pad_f32(const float* __restrict__ x, long long ld, lon
         const int cc = c0 + i, kk = k0 + threadIdx.x;
         if (cc < cols && kk < kpad) out[(long long)cc * kpad + kk] = tile[threadIdx.x][i];
     }
+}
+
+// ------------------------------------------------- FP8 (e4m3) prepass
+// Per-tile scales: one per 128-row tile of A (over all of K) and one per
+// 128-column block of B; s = amax / 448 (the largest finite e4m3), operands
+// quantised as e4m3(x / s) with saturation, products dequantised by
+// s_A * s_B in the epilogue.  amax is kept as the bit pattern of a
+// non-negative float, so atomicMax on the integer orders it correctly.
+
+constexpr float kE4M3Max = 448.0f;
+
+__device__ __forceinline__ float block_max_256(float m)
+{
+    __shared__ float red[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    return m;
+}
+
+// grid (ceil(k / 2048), tiles, batch): |A| max over rows [128 t, 128 t + 128) x one K chunk
+__global__ void __launch_bounds__(256) amax_rows128(const float* __restrict__ x, long long ld, long long sx, int rows,
+                                                    int k, unsigned* __restrict__ amax, int tiles)
+{
+    const int t = blockIdx.y, batch = blockIdx.z;
+    const int k0 = blockIdx.x * 2048, k1 = min(k, k0 + 2048);
+    x += batch * sx;
+    float m = 0.0f;
+    for (int r = t * 128; r < min(rows, t * 128 + 128); r++)
+        for (int kk = k0 + threadIdx.x; kk < k1; kk += 256) m = fmaxf(m, fabsf(x[(long long)r * ld + kk]));
+    m = block_max_256(m);
+    if (threadIdx.x == 0) atomicMax(amax + (long long)batch * tiles + t, __float_as_uint(m));
+}
+
+// grid (ceil(cols / 128), ceil(k / 256), batch), 128 threads: |B| max per 128-column block
+__global__ void __launch_bounds__(128) amax_cols128(const float* __restrict__ x, long long ld, long long sx, int k,
+                                                    int cols, unsigned* __restrict__ amax, int nb)
+{
+    const int c = blockIdx.x * 128 + threadIdx.x, batch = blockIdx.z;
+    const int k0 = blockIdx.y * 256, k1 = min(k, k0 + 256);
+    x += batch * sx;
+    float m = 0.0f;
+    if (c < cols)
+        for (int kk = k0; kk < k1; kk++) m = fmaxf(m, fabsf(x[(long long)kk * ld + c]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float red[4];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        atomicMax(amax + (long long)batch * nb + blockIdx.x, __float_as_uint(fmaxf(fmaxf(red[0], red[1]), fmaxf(red[2], red[3]))));
+}
+
+__device__ __forceinline__ float inv_scale(unsigned amax_bits)
+{
+    const float a = __uint_as_float(amax_bits);
+    return a > 0.0f ? kE4M3Max / a : 1.0f;
+}
+
+__device__ __forceinline__ unsigned char to_e4m3(float v)
+{
+    return (unsigned char)__nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
+}
+
+// A (rows x k) -> A8 (rows x kpad e4m3); grid (ceil(kpad / 4096), rows, batch), 16 values per thread
+__global__ void __launch_bounds__(256) quant_rows_e4m3(const float* __restrict__ x, long long ld, long long sx, int rows,
+                                                       int k, int kpad, const unsigned* __restrict__ amax, int tiles,
+                                                       unsigned char* __restrict__ out, long long so)
+{
+    const int row = blockIdx.y, batch = blockIdx.z;
+    const float inv = inv_scale(amax[(long long)batch * tiles + row / 128]);
+    const float* xr = x + batch * sx + (long long)row * ld;
+    unsigned char* o = out + batch * so + (long long)row * kpad;
+    for (int k0 = (blockIdx.x * 256 + threadIdx.x) * 16; k0 < kpad; k0 += gridDim.x * 256 * 16) {
+        unsigned char q[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) q[i] = k0 + i < k ? to_e4m3(xr[k0 + i] * inv) : (unsigned char)0;
+        *reinterpret_cast<uint4*>(o + k0) = *reinterpret_cast<const uint4*>(q);
+    }
+}
+
+// B (k x cols) -> B8 (cols x kpad e4m3, K-major); 64 x 64 tiles, grid (ceil(cols/64), kpad/64, batch)
+__global__ void __launch_bounds__(256) quant_cols_e4m3(const float* __restrict__ x, long long ld, long long sx, int k,
+                                                       int cols, int kpad, const unsigned* __restrict__ amax, int nb,
+                                                       unsigned char* __restrict__ out, long long so)
+{
+    __shared__ float tile[64][65];
+    const int batch = blockIdx.z, c0 = blockIdx.x * 64, k0 = blockIdx.y * 64;
+    x += batch * sx;
+    out += batch * so;
+    for (int i = threadIdx.x >> 6; i < 64; i += 4) {
+        const int kk = k0 + i, cc = c0 + (threadIdx.x & 63);
+        tile[i][threadIdx.x & 63] = (kk < k && cc < cols) ? x[(long long)kk * ld + cc] : 0.0f;
+    }
+    __syncthreads();
+    // thread -> (column c0 + j, 16 consecutive k)
+    const int j = threadIdx.x >> 2, kq = (threadIdx.x & 3) * 16;
+    const int cc = c0 + j;
+    if (cc >= cols) return;
+    const float inv = inv_scale(amax[(long long)batch * nb + cc / 128]);
+    unsigned char q[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) q[i] = to_e4m3(tile[kq + i][j] * inv);
+    *reinterpret_cast<uint4*>(out + (long long)cc * kpad + k0 + kq) = *reinterpret_cast<const uint4*>(q);
+}
+
+// amax bits -> dequantisation scale (in place)
+__global__ void scales_from_amax(unsigned* __restrict__ a, int n)
+{
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    const float m = __uint_as_float(a[i]);
+    reinterpret_cast<float*>(a)[i] = m > 0.0f ? m / kE4M3Max : 1.0f;
 }
 
 // ----------------------------------------------------- grouped prepass
@@ -804,6 +937,7 @@ void preload_gemm_kernels()
     preload_variants<KIND_TF32, false>();
     preload_variants<KIND_BF16, false>();
     preload_variants<KIND_BF16, true>();
+    preload_variants<KIND_FP8, false>();
     cudaFuncAttributes a;
     cudaFuncGetAttributes(&a, split_rows_bf16<1, 0>);
     cudaFuncGetAttributes(&a, split_rows_bf16<3, 0>);
@@ -824,24 +958,30 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
 {
     using namespace tc;
     if (d->trans_a || d->trans_b) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: transposed operands");
-    if (precision == CHAI_GEMM_FP8) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "fp8 gemm not built");
     const long long M = d->m, N = d->n, K = d->k, batch = d->batch > 0 ? d->batch : 1;
     if (M == 0 || N == 0) return CHAI_OK;
     if (K == 0) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: K = 0");
     if (M > 65535 || batch > 65535) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: M or batch above 65535");
     if (M > (1ll << 31) || N > (1ll << 31)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: size");
     const bool tf32 = precision == CHAI_GEMM_TF32;
+    const bool fp8 = precision == CHAI_GEMM_FP8;
     const int S = precision == CHAI_GEMM_BF16X3 ? 3 : precision == CHAI_GEMM_BF16X6 ? 6 : 1;
-    const int kblk = tf32 ? 32 : 64;                       // elements per 128-byte K block
+    const int kblk = tf32 ? 32 : fp8 ? 128 : 64;           // elements per 128-byte K block
     const long long kpad = (K + kblk - 1) / kblk * kblk;
     const long long kp = S * kpad;                         // K' of the planes
-    const size_t esz = tf32 ? 4 : 2;
+    const size_t esz = tf32 ? 4 : fp8 ? 1 : 2;
     const size_t a_bytes = (size_t)batch * M * kp * esz, b_bytes = (size_t)batch * N * kp * esz;
-    int st = ensure_scratch(ctx, a_bytes + b_bytes + 1024);
+    const long long tiles_m128 = (M + 127) / 128, nb128 = (N + 127) / 128;
+    const size_t b_off = (a_bytes + 1023) & ~size_t(1023);
+    const size_t s_off = (b_off + b_bytes + 255) & ~size_t(255);
+    const size_t s_bytes = fp8 ? (size_t)batch * (tiles_m128 + nb128) * 4 : 0;
+    int st = ensure_scratch(ctx, s_off + s_bytes + 1024);
     if (st) return st;
     char* base = static_cast<char*>(ctx->scratch);
     void* Ap = base;
-    void* Bp = base + ((a_bytes + 1023) & ~size_t(1023));
+    void* Bp = base + b_off;
+    unsigned* amax_a = reinterpret_cast<unsigned*>(base + s_off);
+    unsigned* amax_b = amax_a + batch * tiles_m128;
     const float* A = static_cast<const float*>(d->a);
     const float* B = static_cast<const float*>(d->b);
     cudaStream_t s = ctx->stream;
@@ -850,7 +990,20 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
         dim3 rgrid((unsigned)std::min<long long>((kpad / 8 + 255) / 256, 64), (unsigned)M, (unsigned)batch);
         dim3 tgrid((unsigned)((N + 31) / 32), (unsigned)((kpad + 31) / 32), (unsigned)batch);
         dim3 sgrid((unsigned)((N + 63) / 64), (unsigned)(kpad / 64), (unsigned)batch);
-        if (tf32) {
+        if (fp8) {
+            CHAI_CUDA_TRY(ctx, cudaMemsetAsync(amax_a, 0, s_bytes, s));
+            amax_rows128<<<dim3((unsigned)((K + 2047) / 2048), (unsigned)tiles_m128, (unsigned)batch), 256, 0, s>>>(
+                A, d->lda, d->stride_a, (int)M, (int)K, amax_a, (int)tiles_m128);
+            amax_cols128<<<dim3((unsigned)nb128, (unsigned)((K + 255) / 256), (unsigned)batch), 128, 0, s>>>(
+                B, d->ldb, d->stride_b, (int)K, (int)N, amax_b, (int)nb128);
+            quant_rows_e4m3<<<dim3((unsigned)std::min<long long>((kpad + 4095) / 4096, 64), (unsigned)M,
+                                   (unsigned)batch), 256, 0, s>>>(A, d->lda, d->stride_a, (int)M, (int)K, (int)kpad,
+                                                                   amax_a, (int)tiles_m128, (unsigned char*)Ap, M * kp);
+            quant_cols_e4m3<<<dim3((unsigned)((N + 63) / 64), (unsigned)(kpad / 64), (unsigned)batch), 256, 0, s>>>(
+                B, d->ldb, d->stride_b, (int)K, (int)N, (int)kpad, amax_b, (int)nb128, (unsigned char*)Bp, N * kp);
+            const int ns = (int)(batch * (tiles_m128 + nb128));
+            scales_from_amax<<<(ns + 255) / 256, 256, 0, s>>>(amax_a, ns);
+        } else if (tf32) {
             pad_rows_f32<<<rgrid, 256, 0, s>>>(A, d->lda, d->stride_a, (int)M, (int)K, (int)kpad, (float*)Ap, M * kp);
             transpose_pad_f32<<<tgrid, dim3(32, 8), 0, s>>>(B, d->ldb, d->stride_b, (int)K, (int)N, (int)kpad,
                                                             (float*)Bp, N * kp);
@@ -866,7 +1019,8 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
         CHAI_CUDA_TRY(ctx, cudaGetLastError());
     }
     CUtensorMap ma, mb;
-    const CUtensorMapDataType dt = tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const CUtensorMapDataType dt = tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : fp8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     st = make_map(ctx, &ma, Ap, dt, (int)esz, kp, M, batch, M * kp, kblk, BM);
     if (st) return st;
     TcCfg cfg = default_tc_cfg();
@@ -886,6 +1040,9 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     ep.alpha = (float)d->alpha;
     ep.beta = (float)d->beta;
     ep.vec_ok = ((reinterpret_cast<uintptr_t>(d->c) & 15) == 0 && d->ldc % 4 == 0 && d->stride_c % 4 == 0) ? 1 : 0;
+    ep.sa = fp8 ? reinterpret_cast<const float*>(amax_a) : nullptr;
+    ep.sb = fp8 ? reinterpret_cast<const float*>(amax_b) : nullptr;
+    ep.nb128 = (int)nb128;
     const int kblocks = (int)(kp / kblk);
     TileGrid tg;
     tg.tiles_m = (int)((M + BM - 1) / BM);
@@ -898,6 +1055,7 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     cudaEvent_t ev[2];
     ktime_begin(ctx, "gemm_tc", ev);
     if (tf32) st = launch_variant<KIND_TF32, false, false>(ctx, cfg, grid, ma, mb, kblocks, S, tg, ep, nullptr, 0);
+    else if (fp8) st = launch_variant<KIND_FP8, false, false>(ctx, cfg, grid, ma, mb, kblocks, S, tg, ep, nullptr, 0);
     else if (S == 1) st = launch_variant<KIND_BF16, false, false>(ctx, cfg, grid, ma, mb, kblocks, S, tg, ep, nullptr, 0);
     else st = launch_variant<KIND_BF16, true, false>(ctx, cfg, grid, ma, mb, kblocks, S, tg, ep, nullptr, 0);
     if (st) return st;

@@ -8,7 +8,9 @@ gives C = K) and the "paranoid" L1 check against a CPU double reference.
 
 Bounds: bf16 2^-7, tf32 2^-9 (operands keep 10 mantissa bits), bf16x3 2^-14
 (dropped a1*b1 and residual terms ~2^-16), bf16x6 within 4x the FP32 SIMT
-GEMM's own error plus 2^-22 (FP32 accumulation dominates), fp32 SIMT 2^-18."""
+GEMM's own error plus 2^-22 (FP32 accumulation dominates), fp32 SIMT 2^-18,
+fp8 e4m3 with per-tile scales 2^-4 (3 mantissa bits: each operand is off by
+at most 2^-4 of its tile's scale-relative magnitude)."""
 import ctypes as C
 
 import numpy as np
@@ -19,7 +21,8 @@ from chai_b200 import _lib as L
 
 pytestmark = pytest.mark.gpu
 
-BOUND = {L.GEMM_BF16: 2.0 ** -7, L.GEMM_TF32: 2.0 ** -9, L.GEMM_BF16X3: 2.0 ** -14, L.GEMM_FP32: 2.0 ** -18}
+BOUND = {L.GEMM_BF16: 2.0 ** -7, L.GEMM_TF32: 2.0 ** -9, L.GEMM_BF16X3: 2.0 ** -14, L.GEMM_FP32: 2.0 ** -18,
+         L.GEMM_FP8: 2.0 ** -4}
 
 
 def run_gemm(dev, A, B, prec, alpha=1.0, beta=0.0, C0=None):
@@ -49,7 +52,7 @@ def norm_err(Cg, A, B):
 SHAPES = [(128, 256, 64), (200, 300, 100), (512, 512, 512), (256, 384, 2048), (1, 17, 9)]
 
 
-@pytest.mark.parametrize("prec", [L.GEMM_FP32, L.GEMM_BF16, L.GEMM_TF32, L.GEMM_BF16X3, L.GEMM_BF16X6])
+@pytest.mark.parametrize("prec", [L.GEMM_FP32, L.GEMM_BF16, L.GEMM_TF32, L.GEMM_BF16X3, L.GEMM_BF16X6, L.GEMM_FP8])
 @pytest.mark.parametrize("shape", SHAPES)
 def test_gemm_precision_vs_fp64(chai_dev, prec, shape):
     M, N, K = shape
@@ -72,7 +75,30 @@ def test_gemm_sentinel(chai_dev, prec):
     assert np.all(Cg == K)
 
 
-@pytest.mark.parametrize("prec", [L.GEMM_BF16X3, L.GEMM_TF32])
+def test_fp8_sentinel(chai_dev):
+    """A = B = 1: e4m3(448) * e4m3(448) * (1/448)^2 summed K times -> K to one
+    rounding of the dequantisation scale."""
+    M, N, K = 256, 512, 768
+    Cg = run_gemm(chai_dev, np.ones((M, K), np.float32), np.ones((K, N), np.float32), L.GEMM_FP8)
+    assert np.all(np.abs(Cg - K) <= 2.0 ** -20 * K)
+
+
+def test_fp8_per_tile_scales(chai_dev):
+    """Row tiles of A and column blocks of B with magnitudes 10^-3 .. 10^3: a
+    scale per 128-row tile of A and per 128-column block of B keeps the error
+    relative to each tile's own magnitude (a single scale would flush the
+    small tiles to zero)."""
+    rng = np.random.default_rng(21)
+    M, N, K = 384, 520, 200
+    A = rng.uniform(-1, 1, (M, K)).astype(np.float32)
+    B = rng.uniform(-1, 1, (K, N)).astype(np.float32)
+    A *= np.repeat(10.0 ** np.array([-3.0, 0.0, 3.0]), 128)[:, None].astype(np.float32)
+    B *= np.repeat(10.0 ** np.array([2.0, -2.0, 0.0, 1.0, -3.0]), 128)[None, :N].astype(np.float32)
+    Cg = run_gemm(chai_dev, A, B, L.GEMM_FP8)
+    assert norm_err(Cg, A, B) <= 2.0 ** -4
+
+
+@pytest.mark.parametrize("prec", [L.GEMM_BF16X3, L.GEMM_TF32, L.GEMM_FP8])
 def test_gemm_alpha_beta_batch(chai_dev, prec):
     """C = alpha A B + beta C over a strided batch (matmulG over vector slots)."""
     rng = np.random.default_rng(9)
