@@ -227,7 +227,18 @@ struct EpiArgs {
 
 struct TileGrid {
     int tiles_m, tiles_n, batch, group_m;
+    int plane_k;       // split precisions: K elements per stored plane (plane p starts at column p * plane_k)
 };
+
+// Split precisions store each distinct bf16 plane once per row, side by side
+// along K: [p0 | p1] (x3) or [p0 | p1 | p2] (x6), each plane_k wide.  The MMA
+// walks S product blocks per 64-element K chunk; block s multiplies A plane
+// kSelA[.][s] by B plane kSelB[.][s] (s = 0 is the a0 b0 product).
+__constant__ unsigned char kSelA[3][6] = {{0}, {0, 0, 1}, {0, 0, 1, 0, 1, 2}};
+__constant__ unsigned char kSelB[3][6] = {{0}, {0, 1, 0}, {0, 1, 0, 2, 1, 0}};
+
+template <int S> struct Planes { static constexpr int P = S == 1 ? 1 : (S == 3 ? 2 : 3); };
+__host__ __device__ constexpr int distinct_planes(int S) { return S == 1 ? 1 : (S == 3 ? 2 : 3); }
 
 // tile t -> (m, n, batch) in GROUP_M-high column strips, so the CTAs running
 // at one time share a small set of A and B panels in L2
@@ -377,8 +388,15 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
                     }
                     const unsigned fb = smem_u32(&full[s]);
                     mbar_expect_tx(fb, A_STAGE + B_STAGE);
-                    tma_load_3d(smem_u32(sa + s * A_STAGE), &map_a, fb, kb * kx_mul, ti.arow, ti.tb);
-                    tma_load_3d(smem_u32(sb + s * B_STAGE), &map_b, fb, kb * kx_mul, ti.brow, ti.tb);
+                    int xa = kb * kx_mul, xb = xa;
+                    if (SPLIT || split_s > 1) {
+                        const int blk = kb % split_s, chunk = kb / split_s;
+                        const int sel = split_s == 3 ? 1 : 2;
+                        xa = kSelA[sel][blk] * tg.plane_k + chunk * kx_mul;
+                        xb = kSelB[sel][blk] * tg.plane_k + chunk * kx_mul;
+                    }
+                    tma_load_3d(smem_u32(sa + s * A_STAGE), &map_a, fb, xa, ti.arow, ti.tb);
+                    tma_load_3d(smem_u32(sb + s * B_STAGE), &map_b, fb, xb, ti.brow, ti.tb);
                     issued = it + 1;
                 }
             }
@@ -513,9 +531,6 @@ __device__ __forceinline__ void split3(float a, __nv_bfloat16 (&p)[3])
     p[2] = __float2bfloat16_rn(r2);
 }
 
-// plane index of K-block s for the A and B sides of a split precision
-__constant__ unsigned char kSelA[3][6] = {{0}, {0, 0, 1}, {0, 0, 1, 0, 1, 2}};
-__constant__ unsigned char kSelB[3][6] = {{0}, {0, 1, 0}, {0, 1, 0, 2, 1, 0}};
 
 // 8 consecutive values -> 16-byte chunks of plane p0/p1/p2
 __device__ __forceinline__ void split8(const float (&a)[8], uint4 (&q)[3])
@@ -531,18 +546,19 @@ __device__ __forceinline__ void split8(const float (&a)[8], uint4 (&q)[3])
     for (int j = 0; j < 3; j++) q[j] = *reinterpret_cast<const uint4*>(h[j]);
 }
 
-// A (rows x k, row-major, leading dim ld) -> A' (rows x S*kpad bf16); each
-// thread splits 8 consecutive elements and writes one 16-byte chunk per block
-template <int S, int MODE>
+// A (rows x k, row-major, leading dim ld) -> A' (rows x P*kpad bf16, the P
+// distinct planes side by side); each thread splits 8 consecutive elements and
+// writes one 16-byte chunk per plane
+template <int S>
 __global__ void __launch_bounds__(256) split_rows_bf16(const float* __restrict__ x, long long ld, long long sx,
                                                        int rows, int k, int kpad, __nv_bfloat16* __restrict__ out,
                                                        long long so)
 {
     const int batch = blockIdx.z;
     const int row = blockIdx.y;
+    constexpr int P = Planes<S>::P;
     x += batch * sx + (long long)row * ld;
-    out += batch * so + (long long)row * S * kpad;
-    const int sel = S == 1 ? 0 : (S == 3 ? 1 : 2);
+    out += batch * so + (long long)row * P * kpad;
     const bool vec = ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
     for (int k8 = blockIdx.x * blockDim.x + threadIdx.x; k8 * 8 < kpad; k8 += gridDim.x * blockDim.x) {
         const int kk = k8 * 8;
@@ -557,11 +573,8 @@ __global__ void __launch_bounds__(256) split_rows_bf16(const float* __restrict__
         }
         uint4 q[3];
         split8(a, q);
-        const int kb = kk >> 6, j = kk & 63;
 #pragma unroll
-        for (int s = 0; s < S; s++)
-            *reinterpret_cast<uint4*>(out + (long long)(kb * S + s) * 64 + j) =
-                q[MODE == 0 ? kSelA[sel][s] : kSelB[sel][s]];
+        for (int p = 0; p < P; p++) *reinterpret_cast<uint4*>(out + (long long)p * kpad + kk) = q[p];
     }
 }
 
@@ -593,7 +606,7 @@ __global__ void __launch_bounds__(256) split_cols_bf16(const float* __restrict__
         for (int q = 0; q < 4; q++) tile[i][tx * 4 + q] = v[q];
     }
     __syncthreads();
-    const int sel = S == 1 ? 0 : (S == 3 ? 1 : 2);
+    constexpr int P = Planes<S>::P;
     // 64 columns x 8 runs of 8 k = 512 items, two per thread
     for (int item = threadIdx.x; item < 512; item += 256) {
         const int c = item >> 3, r = item & 7;
@@ -604,10 +617,9 @@ __global__ void __launch_bounds__(256) split_cols_bf16(const float* __restrict__
         for (int i = 0; i < 8; i++) a[i] = tile[r * 8 + i][c];
         uint4 q[3];
         split8(a, q);
-        const int kb = kk >> 6, j = kk & 63;
-        __nv_bfloat16* o = out + (long long)cc * S * kpad;
+        __nv_bfloat16* o = out + (long long)cc * P * kpad;
 #pragma unroll
-        for (int s = 0; s < S; s++) *reinterpret_cast<uint4*>(o + (long long)(kb * S + s) * 64 + j) = q[kSelB[sel][s]];
+        for (int p = 0; p < P; p++) *reinterpret_cast<uint4*>(o + (long long)p * kpad + kk) = q[p];
     }
 }
 
@@ -780,7 +792,8 @@ struct ColJob {
 // 4 rows per 256-thread block (64 threads x 8 elements per row pass)
 template <int S>
 __global__ void __launch_bounds__(256) grouped_split_rows(const RowJob* __restrict__ jobs, int njobs, long long nrows,
-                                                          __nv_bfloat16* __restrict__ out, long long pitch)
+                                                          __nv_bfloat16* __restrict__ out, long long pitch,
+                                                          int plane_k)
 {
     const long long row = (long long)blockIdx.x * 4 + (threadIdx.x >> 6);
     if (row >= nrows) return;
@@ -793,7 +806,7 @@ __global__ void __launch_bounds__(256) grouped_split_rows(const RowJob* __restri
     const RowJob j = jobs[lo];
     const float* x = j.src + (row - j.row0) * (long long)j.k;
     __nv_bfloat16* o = out + row * pitch;
-    const int sel = S == 1 ? 0 : (S == 3 ? 1 : 2);
+    constexpr int P = Planes<S>::P;
     const bool vec = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
     for (int k8 = lane; k8 * 8 < j.kpad; k8 += 64) {
         const int kk = k8 * 8;
@@ -808,15 +821,15 @@ __global__ void __launch_bounds__(256) grouped_split_rows(const RowJob* __restri
         }
         uint4 q[3];
         split8(a, q);
-        const int kb = kk >> 6, jj = kk & 63;
 #pragma unroll
-        for (int s = 0; s < S; s++) *reinterpret_cast<uint4*>(o + (long long)(kb * S + s) * 64 + jj) = q[kSelA[sel][s]];
+        for (int p = 0; p < P; p++) *reinterpret_cast<uint4*>(o + (long long)p * plane_k + kk) = q[p];
     }
 }
 
 template <int S>
 __global__ void __launch_bounds__(256) grouped_split_cols(const ColJob* __restrict__ jobs, int njobs,
-                                                          __nv_bfloat16* __restrict__ out, long long pitch)
+                                                          __nv_bfloat16* __restrict__ out, long long pitch,
+                                                          int plane_k)
 {
     __shared__ float tile[64][65];
     const long long t = blockIdx.x;
@@ -839,7 +852,7 @@ __global__ void __launch_bounds__(256) grouped_split_cols(const ColJob* __restri
         }
     }
     __syncthreads();
-    const int sel = S == 1 ? 0 : (S == 3 ? 1 : 2);
+    constexpr int P = Planes<S>::P;
     for (int item = threadIdx.x; item < 512; item += 256) {
         const int c = item >> 3, r = item & 7;
         const int cc = c0 + c, kk = k0 + r * 8;
@@ -849,10 +862,9 @@ __global__ void __launch_bounds__(256) grouped_split_cols(const ColJob* __restri
         for (int i = 0; i < 8; i++) a[i] = tile[r * 8 + i][c];
         uint4 q[3];
         split8(a, q);
-        const int kb = kk >> 6, jj = kk & 63;
         __nv_bfloat16* o = out + (j.row0 + cc) * pitch;
 #pragma unroll
-        for (int s = 0; s < S; s++) *reinterpret_cast<uint4*>(o + (long long)(kb * S + s) * 64 + jj) = q[kSelB[sel][s]];
+        for (int p = 0; p < P; p++) *reinterpret_cast<uint4*>(o + (long long)p * plane_k + kk) = q[p];
     }
 }
 
@@ -939,9 +951,9 @@ void preload_gemm_kernels()
     preload_variants<KIND_BF16, true>();
     preload_variants<KIND_FP8, false>();
     cudaFuncAttributes a;
-    cudaFuncGetAttributes(&a, split_rows_bf16<1, 0>);
-    cudaFuncGetAttributes(&a, split_rows_bf16<3, 0>);
-    cudaFuncGetAttributes(&a, split_rows_bf16<6, 0>);
+    cudaFuncGetAttributes(&a, split_rows_bf16<1>);
+    cudaFuncGetAttributes(&a, split_rows_bf16<3>);
+    cudaFuncGetAttributes(&a, split_rows_bf16<6>);
     cudaFuncGetAttributes(&a, split_cols_bf16<1>);
     cudaFuncGetAttributes(&a, split_cols_bf16<3>);
     cudaFuncGetAttributes(&a, split_cols_bf16<6>);
@@ -968,7 +980,7 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     const int S = precision == CHAI_GEMM_BF16X3 ? 3 : precision == CHAI_GEMM_BF16X6 ? 6 : 1;
     const int kblk = tf32 ? 32 : fp8 ? 128 : 64;           // elements per 128-byte K block
     const long long kpad = (K + kblk - 1) / kblk * kblk;
-    const long long kp = S * kpad;                         // K' of the planes
+    const long long kp = distinct_planes(S) * kpad;        // stored row: the distinct planes side by side
     const size_t esz = tf32 ? 4 : fp8 ? 1 : 2;
     const size_t a_bytes = (size_t)batch * M * kp * esz, b_bytes = (size_t)batch * N * kp * esz;
     const long long tiles_m128 = (M + 127) / 128, nb128 = (N + 127) / 128;
@@ -1011,7 +1023,7 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
             __nv_bfloat16* a2 = (__nv_bfloat16*)Ap;
             __nv_bfloat16* b2 = (__nv_bfloat16*)Bp;
 #define SPLIT(SS)                                                                                                   \
-    split_rows_bf16<SS, 0><<<rgrid, 256, 0, s>>>(A, d->lda, d->stride_a, (int)M, (int)K, (int)kpad, a2, M * kp);    \
+    split_rows_bf16<SS><<<rgrid, 256, 0, s>>>(A, d->lda, d->stride_a, (int)M, (int)K, (int)kpad, a2, M * kp);    \
     split_cols_bf16<SS><<<sgrid, 256, 0, s>>>(B, d->ldb, d->stride_b, (int)K, (int)N, (int)kpad, b2, N * kp)
             if (S == 1) { SPLIT(1); } else if (S == 3) { SPLIT(3); } else { SPLIT(6); }
 #undef SPLIT
@@ -1043,12 +1055,13 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     ep.sa = fp8 ? reinterpret_cast<const float*>(amax_a) : nullptr;
     ep.sb = fp8 ? reinterpret_cast<const float*>(amax_b) : nullptr;
     ep.nb128 = (int)nb128;
-    const int kblocks = (int)(kp / kblk);
+    const int kblocks = (int)(S * kpad / kblk);            // product blocks the MMA walks
     TileGrid tg;
     tg.tiles_m = (int)((M + BM - 1) / BM);
     tg.tiles_n = (int)((N + cfg.bn - 1) / cfg.bn);
     tg.batch = (int)batch;
     tg.group_m = cfg.group_m;
+    tg.plane_k = (int)kpad;
     const long long ntiles = (long long)tg.tiles_m * tg.tiles_n * tg.batch;
     if (ntiles > (1ll << 30)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: too many tiles");
     const unsigned grid = (unsigned)std::min<long long>(ntiles, ctx->sm_count);
@@ -1078,7 +1091,10 @@ namespace chai {
 int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_problem* p, int32_t count)
 {
     using namespace tc;
-    const TcCfg cfg = default_tc_cfg();
+    TcCfg cfg;
+    cfg.bn = 256;
+    cfg.stages = 4;
+    cfg.group_m = 1;
     const int BN = cfg.bn;
     if (count <= 0) return CHAI_OK;
     int prec = precision == CHAI_GEMM_AUTO ? ctx->cfg.gemm_precision : precision;
@@ -1117,7 +1133,7 @@ int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_p
     }
     if (ra >= (1ll << 31) || rb >= (1ll << 31) || tiles >= (1ll << 30))
         return set_error(ctx, CHAI_ERR_UNSUPPORTED, "grouped gemm: too large");
-    const long long pitch = S * kmax;   // bf16 elements per stacked row
+    const long long pitch = distinct_planes(S) * kmax;   // bf16 elements per stacked row
     const size_t a_bytes = (size_t)ra * pitch * 2, b_bytes = (size_t)rb * pitch * 2;
     const size_t g_bytes = groups.size() * sizeof(GroupEntry), r_bytes = rj.size() * sizeof(RowJob),
                  c_bytes = cj.size() * sizeof(ColJob);
@@ -1135,8 +1151,8 @@ int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_p
     CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(drj, rj.data(), r_bytes, cudaMemcpyHostToDevice, s));
     CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(dcj, cj.data(), c_bytes, cudaMemcpyHostToDevice, s));
 #define GSPLIT(SS)                                                                                      \
-    grouped_split_rows<SS><<<(unsigned)((ra + 3) / 4), 256, 0, s>>>(drj, count, ra, Ap, pitch);         \
-    grouped_split_cols<SS><<<(unsigned)coltiles, 256, 0, s>>>(dcj, count, Bp, pitch)
+    grouped_split_rows<SS><<<(unsigned)((ra + 3) / 4), 256, 0, s>>>(drj, count, ra, Ap, pitch, (int)kmax); \
+    grouped_split_cols<SS><<<(unsigned)coltiles, 256, 0, s>>>(dcj, count, Bp, pitch, (int)kmax)
     if (S == 1) { GSPLIT(1); } else if (S == 3) { GSPLIT(3); } else { GSPLIT(6); }
 #undef GSPLIT
     CHAI_CUDA_TRY(ctx, cudaGetLastError());
@@ -1150,6 +1166,7 @@ int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_p
     tg.tiles_n = 1;
     tg.batch = 1;
     tg.group_m = 1;
+    tg.plane_k = (int)kmax;
     EpiArgs ep;
     memset(&ep, 0, sizeof ep);
     ep.alpha = 1.0f;
