@@ -826,6 +826,7 @@ def main():
     ap.add_argument("--size", type=int, default=0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", default=None, help="back-end configuration string (chai_cuda_init)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -848,7 +849,7 @@ def main():
         pg = dist
     from chai_b200 import _lib as L
     import chai_b200.api as ch
-    dev = ch.init(device=local)
+    dev = ch.init(config=args.config, device=local)
     stream = torch.cuda.Stream()          # one stream shared by torch events and the library
     torch.cuda.set_stream(stream)
     L.lib().chai_cuda_set_stream(dev.ctx, C.c_void_p(stream.cuda_stream))

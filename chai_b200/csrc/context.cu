@@ -154,6 +154,10 @@ static void parse_config(chai::Config& c, const char* text)
             c.tuner_mode = (v == "exhaustive") ? CHAI_TUNE_EXHAUSTIVE : CHAI_TUNE_LEARNED;
         } else if (k == "TopK") {
             c.top_k = std::max(1, atoi(v.c_str()));
+        } else if (k == "StencilRows") {
+            c.stencil_rows = atoi(v.c_str());
+        } else if (k == "StencilMinBlocks") {
+            c.stencil_min_blocks = std::max(0, std::min(8, atoi(v.c_str())));
         } else if (k == "PlanCache") {
             c.plan_cache = v != "0" && v != "off";
         } else if (k == "TuneJournal") {

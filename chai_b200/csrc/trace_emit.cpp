@@ -83,10 +83,12 @@ static PFN_encodeTiledT tensor_map_encoder()
 }
 
 // stencil tile geometry (outputs per CTA: TX x TY; halo: PX columns, R rows)
-constexpr int ST_TX = 128, ST_TY = 32, ST_PX = 4;
+constexpr int ST_TX = 128, ST_PX = 4;
 
 int Translator::emit_group(const std::vector<int>& roots)
 {
+    // stencil tile height (rows of outputs per CTA; a multiple of 8)
+    const int ST_TY = std::max(8, std::min(64, ctx_->cfg.stencil_rows / 8 * 8));
     const Node& r0 = nodes_[roots[0]];
     uint64_t W = r0.W, H = r0.H;
     uint32_t S = r0.slots;
@@ -197,8 +199,9 @@ int Translator::emit_group(const std::vector<int>& roots)
     args.push_back({KArg::I64, nullptr, n});
     args.push_back({KArg::I64, nullptr, (long long)W});
     args.push_back({KArg::I64, nullptr, (long long)H});
-    os << "extern \"C\" __global__ void __launch_bounds__(256) chai_group(const long long n, const long long W, "
-          "const long long H";
+    os << "extern \"C\" __global__ void __launch_bounds__(256";
+    if (mode2d && ctx_->cfg.stencil_min_blocks > 0) os << ", " << ctx_->cfg.stencil_min_blocks;
+    os << ") chai_group(const long long n, const long long W, const long long H";
     bool need_xy = false;
     for (int i : body) {
         const Node& nd = nodes_[i];
