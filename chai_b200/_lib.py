@@ -17,7 +17,8 @@ ERR = {-1: "INVALID", -2: "UNSUPPORTED", -3: "OOM", -4: "LAUNCH", -5: "TIMEOUT",
        -7: "NO_DEVICE", -8: "JIT", -9: "INJECTED"}
 U32, I32, F32, F64 = 0, 1, 4, 8
 PHILOX, THREEFRY = 1230, 1231
-BC_OPCODE, BC_VARIABLE, BC_SCALAR, BC_MEMORY = 0, 1, 2, 3
+BC_OPCODE, BC_VARIABLE, BC_SCALAR, BC_MEMORY, BC_KERNEL = 0, 1, 2, 3, 4
+KARG_ARRAY, KARG_LOCAL, KARG_SCALAR = 0, 1, 2
 GEMM_FP32, GEMM_TF32, GEMM_BF16, GEMM_BF16X3, GEMM_BF16X6, GEMM_FP8, GEMM_FP64, GEMM_AUTO = range(8)
 TUNE_LEARNED, TUNE_EXHAUSTIVE = 0, 1
 
@@ -32,9 +33,21 @@ class chai_stmt(C.Structure):
                 ("reserved", C.c_uint32), ("cells", C.POINTER(chai_bc))]
 
 
+class chai_kernel_arg(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("prec", C.c_uint32), ("variable", C.c_uint32), ("version", C.c_uint32),
+                ("value", C.c_double)]
+
+
+class chai_inline_kernel(C.Structure):
+    _fields_ = [("source", C.c_char_p), ("name", C.c_char_p), ("n_args", C.c_uint32), ("reserved", C.c_uint32),
+                ("args", C.POINTER(chai_kernel_arg)), ("global_size", C.c_uint64 * 2),
+                ("local_size", C.c_uint64 * 2)]
+
+
 class chai_trace_desc(C.Structure):
     _fields_ = [("num_traces", C.c_uint32), ("n_stmts", C.c_uint32), ("stmts", C.POINTER(chai_stmt)),
-                ("hash", C.c_uint64)]
+                ("hash", C.c_uint64), ("kernels", C.POINTER(chai_inline_kernel)), ("n_kernels", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class chai_buffer_binding(C.Structure):

@@ -101,16 +101,18 @@ class Device:
         if self.ctx:
             L.lib().chai_cuda_release(self.ctx, bid)
 
-    def evaluate(self, stmts, bindings, num_traces: int = 1):
-        desc, keep = build_desc(stmts, num_traces)
+    def evaluate(self, stmts, bindings, num_traces: int = 1, kernels=None):
+        desc, keep = build_desc(stmts, num_traces, kernels)
         binds = (L.chai_buffer_binding * _max(1, len(bindings)))()
         for i, b in enumerate(bindings):
             binds[i] = L.chai_buffer_binding(*b)
         L.check(L.lib().chai_cuda_evaluate(self.ctx, C.byref(desc), binds, len(bindings)), self.ctx)
 
 
-def build_desc(stmts, num_traces=1):
-    """chai_trace_desc from [(lhs_var, lhs_ver, [cells...]), ...]."""
+def build_desc(stmts, num_traces=1, kernels=None):
+    """chai_trace_desc from [(lhs_var, lhs_ver, [cells...]), ...] and the
+    trace's inline kernels [(source, name, [(kind, prec, var, ver, value)],
+    (g0, g1), (l0, l1)), ...]."""
     arr = (L.chai_stmt * _max(1, len(stmts)))()
     keep = [arr]
     for i, (var, ver, cells) in enumerate(stmts):
@@ -120,6 +122,19 @@ def build_desc(stmts, num_traces=1):
         keep.append(ca)
         arr[i] = L.chai_stmt(var, ver, len(cells), 0, ca)
     desc = L.chai_trace_desc(num_traces, len(stmts), arr, 0)
+    if kernels:
+        ka = (L.chai_inline_kernel * len(kernels))()
+        for i, (src, name, args, gsize, lsize) in enumerate(kernels):
+            aa = (L.chai_kernel_arg * _max(1, len(args)))()
+            for j, (kind, prec, var, ver, value) in enumerate(args):
+                aa[j] = L.chai_kernel_arg(kind, prec, var, ver, float(value))
+            sb, nb = src.encode(), name.encode()
+            keep += [aa, sb, nb]
+            ka[i] = L.chai_inline_kernel(sb, nb, len(args), 0, aa, (C.c_uint64 * 2)(*gsize),
+                                         (C.c_uint64 * 2)(*lsize))
+        keep.append(ka)
+        desc.kernels = ka
+        desc.n_kernels = len(kernels)
     keep.append(desc)
     return desc, keep
 
@@ -158,6 +173,7 @@ class _Client:
     read-back, and the arrays that own device buffers."""
     pending: list = []            # (lhs_var, lhs_ver, cells, owner array or None)
     keep: list = []               # make1/make2 arrays whose host data the trace reads
+    kernels: list = []            # inline OpenCL kernels of the pending trace
     vars = itertools.count(1)
 
 
@@ -165,7 +181,9 @@ def _schedule():
     """Evaluate the pending trace (Scheduler::wait -> DeviceBase::evaluate)."""
     dev = vm()
     stmts = _Client.pending
+    kernels = _Client.kernels
     _Client.pending = []
+    _Client.kernels = []
     if not stmts:
         return
     assigned = {}
@@ -176,6 +194,10 @@ def _schedule():
                 referenced.add(c[1])
         if owner is not None:
             assigned[var] = owner
+    for _, _, args, _, _ in kernels:
+        for kind, _, var, _, _ in args:
+            if kind == L.KARG_ARRAY:
+                referenced.add(var)
     bindings = []
     # inputs: arrays from earlier traces referenced here
     for var in referenced:
@@ -196,7 +218,7 @@ def _schedule():
             weakref.finalize(a, _release, a._buffer)
         bindings.append((var, a.prec, a.W, a.H, a.slots, 0, a._buffer))
     try:
-        dev.evaluate([(v, ver, cells) for v, ver, cells, _ in stmts], bindings)
+        dev.evaluate([(v, ver, cells) for v, ver, cells, _ in stmts], bindings, kernels=kernels)
     finally:
         _Client.keep = []
 
@@ -596,6 +618,83 @@ def transpose(a):
 
 def matmul(a, b, c=None, alpha=1.0, beta=1.0):
     return _Matmul(a, b, c, alpha, beta)
+
+
+# ------------------------------------------------------------------ inline OpenCL
+
+_CL_SCALARS = {"unsigned": L.U32, "uint": L.U32, "int": L.I32, "float": L.F32, "double": L.F64}
+
+
+def _cl_signatures(text):
+    """Argument kinds and precisions of every `__kernel void NAME(...)` in the
+    program text, as api/ProgramCL.cpp:45-176 reads them: __global / global /
+    image2d_t parameters are arrays, __local / local ones local memory, the
+    rest scalars; the precision is the parameter's uint / unsigned / int /
+    float / double keyword."""
+    import re
+    sigs = {}
+    for m in re.finditer(r"\b(?:__kernel|kernel)\s+void\s+(\w+)\s*\(([^)]*)\)", text):
+        args = []
+        for p in m.group(2).split(","):
+            toks = p.replace("*", " ").split()
+            if not toks:
+                continue
+            if any(t in ("__global", "global", "image2d_t") for t in toks):
+                kind = L.KARG_ARRAY
+            elif any(t in ("__local", "local") for t in toks):
+                kind = L.KARG_LOCAL
+            else:
+                kind = L.KARG_SCALAR
+            prec = next((_CL_SCALARS[t] for t in toks if t in _CL_SCALARS), -1)
+            args.append((kind, prec))
+        sigs[m.group(1)] = args
+    return sigs
+
+
+class ProgramCL:
+    """Inline OpenCL kernels (api/chai.h ProgramCL).  The C++ form
+    `(prog, "name", A, 1.5f)(N, 1)` is written `prog("name", A, f32(1.5))(N, 1)`:
+    array arguments are updated in place, and later statements see the new
+    values; the kernel runs in statement order within the trace."""
+
+    def __init__(self, text):
+        self.text = text if isinstance(text, str) else "\n".join(text)
+        self._sigs = _cl_signatures(self.text)
+
+    def __call__(self, name, *args):
+        if name not in self._sigs:
+            raise ValueError("ProgramCL: no __kernel named %r" % name)
+        return _KernelCall(self, name, args)
+
+
+class _KernelCall:
+    def __init__(self, prog, name, args):
+        self.prog, self.name, self.args = prog, name, args
+
+    def __call__(self, *ws):
+        """(global0, local0) or (global0, global1, local0, local1)."""
+        if len(ws) == 2:
+            gsize, lsize = (ws[0], 0), (ws[1], 0)
+        elif len(ws) == 4:
+            gsize, lsize = (ws[0], ws[1]), (ws[2], ws[3])
+        else:
+            raise TypeError("work space: (global0, local0) or (global0, global1, local0, local1)")
+        sig = self.prog._sigs[self.name]
+        if len(sig) != len(self.args):
+            raise TypeError("ProgramCL: %s takes %d arguments" % (self.name, len(sig)))
+        args = []
+        for (kind, prec), a in zip(sig, self.args):
+            if kind == L.KARG_ARRAY:
+                if not isinstance(a, Array):
+                    raise TypeError("ProgramCL: array arguments must be array variables")
+                args.append((kind, a.prec, a.var, a.version - 1, 0.0))
+                _Client.keep.append(a)
+            else:
+                args.append((kind, prec if prec >= 0 else L.F32, 0, 0, float(a)))
+        idx = len(_Client.kernels)
+        _Client.kernels.append((self.prog.text, self.name, args, gsize, lsize))
+        var = next(_Client.vars)
+        _Client.pending.append((var, 1, [_bc(L.BC_KERNEL, buffer=idx), _op(50)], None))
 
 
 # ------------------------------------------------------------------ many traces

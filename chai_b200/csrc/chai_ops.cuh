@@ -143,9 +143,11 @@ template <int OP, class T> __device__ __forceinline__ T f2(T a, T b);
     template <> __device__ __forceinline__ i32 f2<OP, i32>(i32 a, i32 b) { return EXPR; }
 
 // Packed f32 pairs: the element kernels hold 4 consecutive elements per
-// thread; add / sub / mul of f32 operands run as two sm_100 f32x2
-// instructions (round to nearest even per lane, the same IEEE results as the
-// scalar ops, half the instruction issue).
+// thread; add / sub of f32 operands run as two sm_100 f32x2 instructions
+// (round to nearest even per lane, the same IEEE results as the scalar ops,
+// half the instruction issue).  The translator never emits the packed
+// multiply: ptxas contracts mul.rn.f32x2 followed by add / sub.rn.f32x2 into a
+// single-rounding packed FMA.
 template <int OP> struct pk2;
 template <> struct pk2<11> { static __device__ __forceinline__ unsigned long long op(unsigned long long a, unsigned long long b)
     { unsigned long long d; asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; } };

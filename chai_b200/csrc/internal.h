@@ -31,7 +31,7 @@ struct Config {
     std::string tune_journal;                // crash-safe TRY / OK markers of every timing
     bool plan_cache = true;                  // replay recorded plans of repeated traces
     int stencil_rows = 32;                   // output rows per stencil tile (multiple of 8, <= 64)
-    int stencil_min_blocks = 6;              // __launch_bounds__ minimum blocks per SM for stencil kernels
+    int stencil_min_blocks = 0;              // __launch_bounds__ minimum blocks per SM for stencil kernels (0: none)
     std::string jit_cache;
 };
 

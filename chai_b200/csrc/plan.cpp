@@ -47,6 +47,31 @@ void plan_key(const chai_trace_desc* t, const chai_buffer_binding* b, size_t nb,
         key.push_back(b[i].slots);
         key.push_back(ordinal(b[i].buffer));
     }
+    // inline kernels: program text, name, arguments, NDRange
+    auto text_hash = [](const char* p) -> uint64_t {
+        uint64_t h = 1469598103934665603ull;
+        for (; p && *p; p++) { h ^= (unsigned char)*p; h *= 1099511628211ull; }
+        return h;
+    };
+    const uint32_t nk = t->kernels ? t->n_kernels : 0;
+    key.push_back(nk);
+    for (uint32_t k = 0; k < nk; k++) {
+        const chai_inline_kernel& kd = t->kernels[k];
+        key.push_back(text_hash(kd.source));
+        key.push_back(text_hash(kd.name));
+        key.push_back(kd.n_args);
+        for (uint32_t a = 0; a < kd.n_args && kd.args; a++) {
+            const chai_kernel_arg& g = kd.args[a];
+            uint64_t bits;
+            memcpy(&bits, &g.value, 8);
+            key.push_back(((uint64_t)g.kind << 32) | g.prec);
+            key.push_back(g.kind == CHAI_KARG_ARRAY ? ((var_ordinal(g.variable) << 32) | g.version) : bits);
+        }
+        key.push_back(kd.global_size[0]);
+        key.push_back(kd.global_size[1]);
+        key.push_back(kd.local_size[0]);
+        key.push_back(kd.local_size[1]);
+    }
     for (uint32_t s = 0; s < t->n_stmts; s++) {
         const chai_stmt& st = t->stmts[s];
         key.push_back((var_ordinal(st.lhs_variable) << 32) | st.lhs_version);
@@ -224,7 +249,7 @@ int Translator::run_step(const Step& s)
             }
             cudaEvent_t kev[2];
             ktime_begin(ctx_, "trace", kev);
-            int st = ctx_->jit->launch(s.fn, s.grid, s.block, 0, ptrs.data());
+            int st = ctx_->jit->launch(s.fn, s.grid, s.block, s.smem, ptrs.data());
             if (st) return st;
             ktime_end(ctx_, "trace", kev);
             return CHAI_OK;

@@ -50,6 +50,7 @@ struct Step {
     };
     std::vector<Arg> args;
     std::vector<TmapRec> maps;
+    size_t smem = 0;                // dynamic shared memory bytes
     size_t scratch_need = 0;        // ensure_scratch before the step
     // COMBINE
     int nblocks = 0, nred = 0, slots = 0;

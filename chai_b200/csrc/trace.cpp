@@ -210,6 +210,27 @@ int Translator::parse(const chai_stmt& s, int& pos)
         n.W = nodes_[k].W; n.H = nodes_[k].H; n.slots = nodes_[k].slots;
         return add(n);
     }
+    if (op == 50) {
+        // kernel_from_opencl: [{KERNEL, index}, 50]
+        if (pos < 0 || s.cells[pos].kind != CHAI_BC_KERNEL) return -1;
+        const uint64_t kidx = s.cells[pos--].buffer;
+        if (!kernels_ || kidx >= n_kernels_) return -1;
+        const chai_inline_kernel& kd = kernels_[kidx];
+        if (!kd.source || !kd.name || (kd.n_args && !kd.args)) return -1;
+        n.kind = Node::INLINE;
+        n.buffer = kidx;
+        for (uint32_t a = 0; a < kd.n_args; a++) {
+            if (kd.args[a].kind != CHAI_KARG_ARRAY) continue;
+            Node v;
+            v.kind = Node::VAR;
+            v.var = kd.args[a].variable;
+            v.ver = kd.args[a].version;
+            const int k = resolve_var(v);
+            if (k < 0) return -1;
+            n.kids.push_back(k);
+        }
+        return add(n);
+    }
     if (op >= 110 && op <= 115) {
         n.kind = Node::RNG;
         n.variant = (uint32_t)scalar_cell(s, pos, ok);
@@ -390,6 +411,9 @@ int Translator::run(const chai_trace_desc* t, const chai_buffer_binding* binds, 
 {
     for (size_t i = 0; i < nb; i++) bindings_[binds[i].variable] = binds[i];
     slots_ = t->num_traces ? t->num_traces : 1;
+    kernels_ = t->kernels;
+    n_kernels_ = t->kernels ? t->n_kernels : 0;
+    int first_inline = -1;      // statement index of the first inline kernel
     // 1-2: parse all statements
     for (uint32_t i = 0; i < t->n_stmts; i++) {
         const chai_stmt& s = t->stmts[i];
@@ -404,6 +428,27 @@ int Translator::run(const chai_trace_desc* t, const chai_buffer_binding* binds, 
         if (pos != -1) return fail(CHAI_ERR_INVALID, "trailing cells in statement " + std::to_string(i));
         if (nodes_[root].kind == Node::READ) {
             reads_.push_back(root);
+        } else if (nodes_[root].kind == Node::INLINE) {
+            // the kernel updates its array arguments in place: later statements
+            // reading (variable, version) see the values after the kernel
+            if (first_inline < 0) first_inline = (int)stmt_roots_.size();
+            stmt_roots_.push_back(std::make_pair(s.lhs_variable, root));
+            const chai_inline_kernel& kd = kernels_[nodes_[root].buffer];
+            size_t m = 0;
+            for (uint32_t a = 0; a < kd.n_args; a++) {
+                if (kd.args[a].kind != CHAI_KARG_ARRAY) continue;
+                const int pre = nodes_[root].kids[m++];
+                Node after;
+                after.kind = Node::AFTER;
+                after.kids = {root, pre};
+                after.prec = nodes_[pre].prec;
+                after.W = nodes_[pre].W; after.H = nodes_[pre].H; after.slots = nodes_[pre].slots;
+                after.var = kd.args[a].variable;
+                after.ver = kd.args[a].version;
+                const int id = add(after);
+                assigned_[std::make_pair(kd.args[a].variable, kd.args[a].version)] = id;
+                latest_[kd.args[a].variable] = id;
+            }
         } else {
             assigned_[std::make_pair(s.lhs_variable, s.lhs_version)] = root;
             latest_[s.lhs_variable] = root;
@@ -432,12 +477,25 @@ int Translator::run(const chai_trace_desc* t, const chai_buffer_binding* binds, 
             case Node::MAKE:
                 materialize_[i] = true;   // values that already live in HBM
                 break;
+            case Node::INLINE:
+                materialize_[i] = true;
+                for (int k : n.kids) materialize_[k] = true;
+                break;
+            case Node::AFTER:
+                materialize_[i] = true;
+                break;
             default:
                 break;
         }
     }
     for (auto& kv : latest_)
         if (bindings_.count(kv.first)) materialize_[kv.second] = true;
+    // an inline kernel is a barrier: every value assigned before it is
+    // computed (into HBM) before it runs
+    for (int k = 0; k < first_inline; k++) {
+        const int r = stmt_roots_[k].second;
+        if (nodes_[r].kind != Node::INLINE) materialize_[r] = true;
+    }
     // storage for materialised nodes
     for (size_t i = 0; i < nodes_.size(); i++) {
         if (!materialize_[i]) continue;
@@ -470,6 +528,10 @@ int Translator::run(const chai_trace_desc* t, const chai_buffer_binding* binds, 
         const Node& n = nodes_[kv.second];
         if (n.kind == Node::INPUT && n.var == kv.first) continue;
         if (n.storage_buffer == b->second.buffer) continue;
+        // (a value updated in place by an inline kernel lives in its
+        // argument's storage; the bound buffer may not exist yet)
+        int ast = alloc_buffer(ctx_, b->second.buffer, node_bytes(n));
+        if (ast) return ast;
         Buffer* dst = find_buffer(ctx_, b->second.buffer);
         if (!dst) return fail(CHAI_ERR_NOT_FOUND, "output buffer");
         note_buffer(b->second.buffer, node_bytes(n), true);
@@ -493,6 +555,13 @@ int Translator::assign_storage(int i)
 {
     Node& n = nodes_[i];
     if (n.dev) return CHAI_OK;
+    if (n.kind == Node::INLINE) return CHAI_OK;       // no value of its own
+    if (n.kind == Node::AFTER) {                       // the argument's storage, updated in place
+        const Node& pre = nodes_[n.kids[1]];
+        n.dev = pre.dev;
+        n.storage_buffer = pre.storage_buffer;
+        return CHAI_OK;
+    }
     if (dry_) {
         n.dev = reinterpret_cast<void*>(uintptr_t(0x10000) * (i + 1));
         return CHAI_OK;
@@ -563,7 +632,14 @@ int Translator::schedule(const std::vector<int>& order)
     };
     for (int i : order) {
         Node& n = nodes_[i];
-        if (n.kind == Node::INPUT || n.kind == Node::MAKE) continue;
+        if (n.kind == Node::INPUT || n.kind == Node::MAKE || n.kind == Node::AFTER) continue;
+        if (n.kind == Node::INLINE) {
+            int st = flush();
+            if (st) return st;
+            st = emit_inline(i);
+            if (st) return st;
+            continue;
+        }
         if (n.kind == Node::MATMUL || n.kind == Node::MATMULG || n.kind == Node::TRANSPOSE) {
             int st = flush();
             if (st) return st;

@@ -16,8 +16,11 @@ struct chai_cuda_ctx;
 namespace chai {
 
 struct Node {
+    // INLINE: an inline OpenCL kernel (buffer = its index in the trace's kernel
+    // table, kids = its array arguments); AFTER: an array argument's value once
+    // the kernel has run (kids = {INLINE, value before}; same storage)
     enum Kind { VAR, INPUT, SCALAR, OP, CONVERT, RNG, INDEX, FILL, MAKE, READ, MATMUL, MATMULG, TRANSPOSE,
-                REDUCE, GATHER } kind = OP;
+                REDUCE, GATHER, INLINE, AFTER } kind = OP;
     uint32_t op = 0;
     int prec = CHAI_F32;
     uint64_t W = 1, H = 1;
@@ -104,6 +107,13 @@ private:
     int emit_group(const std::vector<int>& roots);
     int emit_linalg(int i);
     int do_read(int i);
+    int emit_inline(int i);
+    const chai_inline_kernel* kernels_ = nullptr;
+    uint32_t n_kernels_ = 0;
 };
+
+// OpenCL C program text -> CUDA source (inline_cl.cpp)
+int opencl_to_cuda(const std::string& src, const std::string& name, const std::vector<size_t>& local_bytes,
+                   int work_dim, std::string& out, std::string& err);
 
 }  // namespace chai

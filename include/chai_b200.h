@@ -110,7 +110,7 @@ int chai_cuda_release(chai_cuda_ctx* ctx, uint64_t id);
 /* ----------------------------------------------------------------- trace */
 
 /* One bytecode cell, mirroring chai_internal::BC (bytecode/BC.hpp:15-36). */
-enum { CHAI_BC_OPCODE = 0, CHAI_BC_VARIABLE = 1, CHAI_BC_SCALAR = 2, CHAI_BC_MEMORY = 3 };
+enum { CHAI_BC_OPCODE = 0, CHAI_BC_VARIABLE = 1, CHAI_BC_SCALAR = 2, CHAI_BC_MEMORY = 3, CHAI_BC_KERNEL = 4 };
 typedef struct chai_bc {
     uint32_t kind;      /* CHAI_BC_* */
     uint32_t code;      /* opcode (ByteCodes.hpp numbers) or variable number */
@@ -131,11 +131,42 @@ typedef struct chai_stmt {
 } chai_stmt;
 
 /* A vectorised trace (common/VectorTrace.hpp:28-119). */
+/* Inline OpenCL kernel of a trace: ProgramCL (api/ProgramCL.cpp; the
+ * reference records it as the statement [AstOpenCL box, kernel_from_opencl]
+ * and prints / enqueues it in jitast/AstOpenCL.cpp, enqueue/EnqueueOpenCL.cpp).
+ * Here the statement is [{CHAI_BC_KERNEL, .buffer = index into
+ * chai_trace_desc.kernels}, opcode 50]; the OpenCL C text is compiled for
+ * sm_100a by NVRTC through a prelude that maps the OpenCL work-item functions,
+ * address-space qualifiers and barrier onto CUDA.  Array arguments are the
+ * arrays' device storage, updated in place: statements after the kernel read
+ * the updated values under the same (variable, version), as in the
+ * reference.  Scalar OpenCL C only (no vector types, no image2d_t). */
+enum { CHAI_KARG_ARRAY = 0, CHAI_KARG_LOCAL = 1, CHAI_KARG_SCALAR = 2 };
+typedef struct chai_kernel_arg {
+    uint32_t kind;              /* CHAI_KARG_* */
+    uint32_t prec;              /* element / scalar precision: CHAI_U32, CHAI_I32, CHAI_F32, CHAI_F64 */
+    uint32_t variable;          /* ARRAY: the array variable and its current version */
+    uint32_t version;
+    double   value;             /* SCALAR: the value; LOCAL: number of elements */
+} chai_kernel_arg;
+typedef struct chai_inline_kernel {
+    const char* source;         /* the whole OpenCL C program text */
+    const char* name;           /* the __kernel function to run */
+    uint32_t n_args;
+    uint32_t reserved;
+    const chai_kernel_arg* args;
+    uint64_t global_size[2];    /* work items per dimension; global_size[1] = 0 for 1-D */
+    uint64_t local_size[2];     /* work-group size per dimension (divides global_size) */
+} chai_inline_kernel;
+
 typedef struct chai_trace_desc {
     uint32_t num_traces;        /* slots: identical traces batched together */
     uint32_t n_stmts;
     const chai_stmt* stmts;
     uint64_t hash;              /* front-end trace hash (0: computed here) */
+    const chai_inline_kernel* kernels;   /* inline kernels the statements refer to (may be NULL) */
+    uint32_t n_kernels;
+    uint32_t reserved;
 } chai_trace_desc;
 
 /* Variables that live outside the trace: inputs computed by earlier traces and

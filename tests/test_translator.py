@@ -76,8 +76,9 @@ def test_kirsch_trace_is_one_kernel_with_gathers():
     # the 8 gathers read 3 row windows (row offsets -1, 0, +1), each one
     # 16-byte shared load plus two edge elements
     assert src.count("const float* rowp = tile0") == 3 and src.count("chai_k::lds_vec(rowp") == 3
-    # f32 add / sub / mul run as packed f32x2 pairs
-    assert src.count("f2x4<11>") >= 20 and src.count("f2x4<14>") >= 8 and src.count("f2x4<13>") >= 8
+    # f32 add / sub run as packed f32x2 pairs; multiplies stay scalar (a packed
+    # multiply feeding a packed add would be contracted into one rounding)
+    assert src.count("f2x4<11>") >= 20 and src.count("f2x4<14>") >= 8 and src.count("f2x4<13>") == 0
 
 
 def test_data_dependent_gather_stays_generic():
