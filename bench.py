@@ -374,6 +374,82 @@ def run_mc(args, L, ctx, stream):
     }
 
 
+def run_mc_hbm(args, L, ctx, stream):
+    """The materialised Monte Carlo variant: Z (2^27 f32 normals, 512 MiB)
+    already in HBM, payoff = mean(max(100 exp(0.03 + 0.2 Z) - 100, 0)) as one
+    fused trace reading it once (4 bytes per element)."""
+    import torch
+    import chai_b200.api as ch
+    W, H = 8192, 16384
+    n = W * H
+    dev = ch.vm()
+    z = torch.empty(n, device="cuda", dtype=torch.float32)
+    rd = L.chai_rng_desc(1230, 4, 1, 4, 42, W, H, 1, 0, 0.0, 1.0)
+    L.check(L.lib().chai_cuda_rng_fill(ctx, C.byref(rd), C.c_void_p(z.data_ptr())), ctx)
+    z.nan_to_num_(nan=0.0, posinf=0.0, neginf=0.0)      # the rare u = 0 draws
+    zid, pid = 77101, 77102
+    L.check(L.lib().chai_cuda_buffer_wrap(ctx, zid, C.c_void_p(z.data_ptr()), n * 4), ctx)
+    ch._Client.pending = []
+    z_var = next(ch._Client.vars)
+    Z = ch._Raw([ch._bc(L.BC_VARIABLE, z_var, 0)], L.F32, W, H)
+    f = np.float32
+    P = ch.Arrayf32(ch.mean(ch.max(f(100) * ch.exp(f(0.05 - 0.5 * 0.2 * 0.2) + f(0.2) * Z) - f(100), f(0))))
+    stmts = [(v, ver, cells) for v, ver, cells, _ in ch._Client.pending]
+    ch._Client.pending = []
+    desc, keep = ch.build_desc(stmts)
+    barr = (L.chai_buffer_binding * 2)(L.chai_buffer_binding(z_var, 4, W, H, 1, 0, zid),
+                                       L.chai_buffer_binding(P.var, 4, 1, 1, 1, 0, pid))
+
+    def step():
+        L.check(L.lib().chai_cuda_evaluate(dev.ctx, C.byref(desc), barr, 2), dev.ctx)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    kstats(L, ctx, "trace")
+    flush = l2_flusher()
+    with Clocks(torch.cuda.current_device()) as clk:
+        ts = time_events(step, args.steps, stream, flush=flush)
+    ms = sum(ts) / len(ts)
+    k_ms, k_n = kstats(L, ctx, "trace")
+    kern_ms = k_ms / k_n if k_n else None
+    nbytes = 4 * n
+    P_, kind = peaks()
+    roof = None
+    if kern_ms:
+        ach = nbytes / (kern_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": ach, "peak": P_["hbm_gbs"], "unit": "GB/s", "frac": ach / P_["hbm_gbs"],
+                "traffic": traffic("trace_mc_hbm"), "peak_source": "%s (copy)" % kind,
+                "kernel": "chai_group (MC over Z in HBM)", "kernel_ms": kern_ms, "algorithmic_bytes": nbytes}
+    # e2e: Z from pinned host memory each step, payoff read back
+    zh = z.cpu().pin_memory()
+    ze = 77103
+    L.check(L.lib().chai_cuda_buffer_alloc(ctx, ze, n * 4), ctx)
+    barr2 = (L.chai_buffer_binding * 2)(L.chai_buffer_binding(z_var, 4, W, H, 1, 0, ze),
+                                        L.chai_buffer_binding(P.var, 4, 1, 1, 1, 0, pid))
+    out = (C.c_float * 1)()
+
+    def e2e():
+        L.check(L.lib().chai_cuda_upload(ctx, ze, C.c_void_p(zh.data_ptr()), n * 4), ctx)
+        L.check(L.lib().chai_cuda_evaluate(dev.ctx, C.byref(desc), barr2, 2), dev.ctx)
+        L.check(L.lib().chai_cuda_readback(ctx, pid, out, 4), ctx)
+
+    e2e()
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.steps, 5))):
+        e2e()
+    e_ms = (time.perf_counter() - t0) * 1e3 / max(1, min(args.steps, 5))
+    return {
+        "metric": "trace HBM GB/s", "unit": "GB/s", "value": nbytes / (ms * 1e-3) / 1e9, "ms_per_step": ms,
+        "dtype": "f32", "higher_is_better": True,
+        "config": {"workload": "Monte Carlo payoff over 2^27 f32 normals already in HBM (materialised Z), fused",
+                   "normals": n, "payoff": float(out[0]), "l2": "flushed between steps (Z 512 MiB > L2)"},
+        "e2e": {"value": nbytes / (e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": 4},
+        "roofline": roof, "clocks": clk.summary(), "gpu_launches": args.steps * 2,
+    }
+
+
 def kirsch_expr(ch, A, W, H):
     f = np.float32
     X, Y = ch.index_f32(0, W, H), ch.index_f32(1, W, H)
@@ -696,8 +772,8 @@ def run_tuner(args, L, ctx, stream):
     }
 
 
-WORKLOADS = {"gemm": run_gemm, "mc": run_mc, "kirsch": run_kirsch, "gemv": run_gemv, "mc-many": run_mc_many,
-             "grouped": run_grouped, "tuner": run_tuner}
+WORKLOADS = {"gemm": run_gemm, "mc": run_mc, "mc-hbm": run_mc_hbm, "kirsch": run_kirsch, "gemv": run_gemv,
+             "mc-many": run_mc_many, "grouped": run_grouped, "tuner": run_tuner}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -741,6 +817,13 @@ def run_reference(args, steps=None):
             cmd = None
             unit, metric = "Gnormals/s", "trace throughput (64 uneven MC traces, one persistent launch)"
             sample = "64 sequential interpreter MC traces, lengths 1/16 of the GPU workload's"
+        elif wl == "mc-hbm":
+            n = 1 << 19
+            rng.standard_normal(n).astype(np.float32).tofile(td + "/Z")
+            cmd = [str(drv), "mc", str(n), td + "/Z"]
+            unit, metric = "GB/s", "trace HBM GB/s"
+            conv = lambda ms: 4 * n / (ms * 1e-3) / 1e9
+            sample = "interpreter MC payoff over 2^19 given normals (make1)"
         elif wl == "mc":
             W, H = 1024, 512
             cmd = [str(drv), "mc_rng", str(W), str(H)]

@@ -155,7 +155,7 @@ def evaluate(ctx, held_out, default_ids=None):
         t0 = time.perf_counter()
         sweep(ctx, k)
         t_exh = time.perf_counter() - t0
-        dflt = (8, 0, 0, 0, 4, 0) if k.is_gemv else (128, 256, 128, 4, 4, 16)
+        dflt = (4, 0, 0, 0, 1, 0) if k.is_gemv else (128, 256, 128, 4, 4, 16)
         rows.append(dict(m=k.m, n=k.n, k=k.k, precision=k.precision, gemv=k.is_gemv, best_us=best,
                          pick_us=by_id.get(cfg_id(pick), float("nan")),
                          default_us=by_id.get(dflt, float("nan")), learned_s=t_learned, exhaustive_s=t_exh))
