@@ -91,6 +91,7 @@ SIGNATURES = {
     "chai_cuda_init": (C.c_int, [C.c_int, C.c_char_p, C.POINTER(P)]),
     "chai_cuda_shutdown": (C.c_int, [P]),
     "chai_cuda_synchronize": (C.c_int, [P]),
+    "chai_cuda_selftest_wait": (C.c_int, [P, C.c_double]),
     "chai_cuda_error_string": (C.c_char_p, [C.c_int]),
     "chai_cuda_last_error": (C.c_char_p, [P]),
     "chai_cuda_set_stream": (C.c_int, [P, P]),

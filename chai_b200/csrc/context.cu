@@ -281,6 +281,14 @@ int chai_cuda_kernel_stats(chai_cuda_ctx* ctx, const char* name, double* total_m
     return CHAI_OK;
 }
 
+int chai_cuda_selftest_wait(chai_cuda_ctx* ctx, double limit_ms)
+{
+    if (!ctx || !(limit_ms > 0) || limit_ms > 2000) return CHAI_ERR_INVALID;
+    int st = launch_wait_selftest(ctx, limit_ms);
+    if (st) return st;
+    return chai_cuda_synchronize(ctx);
+}
+
 int chai_cuda_synchronize(chai_cuda_ctx* ctx)
 {
     if (!ctx) return CHAI_ERR_INVALID;

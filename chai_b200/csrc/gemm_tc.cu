@@ -109,17 +109,30 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 
-// Bounded wait: false (and the status word set) once WAIT_NS has passed.
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int* status, int code)
+// Bounded wait: false (and the status word set) once `limit_ns` has passed.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int* status, int code,
+                                          unsigned long long limit_ns = WAIT_NS)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > WAIT_NS) {
+        if (global_ns() - t0 > limit_ns) {
             atomicExch(status, code);
             return false;
         }
+    }
+}
+
+// Self-test of the bounded wait: one thread waits on an mbarrier that nothing
+// ever arrives on; the wait must give up after limit_ns and report `code`.
+__global__ void chai_wait_selftest(int* status, unsigned long long limit_ns, int code)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&bar), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_wait(smem_u32(&bar), 0, status, code, limit_ns);
     }
 }
 
@@ -959,6 +972,13 @@ void preload_gemm_kernels()
     cudaFuncGetAttributes(&a, split_cols_bf16<6>);
     cudaFuncGetAttributes(&a, pad_rows_f32);
     cudaFuncGetAttributes(&a, transpose_pad_f32);
+}
+
+int launch_wait_selftest(chai_cuda_ctx* ctx, double limit_ms)
+{
+    tc::chai_wait_selftest<<<1, 32, 0, ctx->stream>>>(ctx->status_word, (unsigned long long)(limit_ms * 1e6), 199);
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    return CHAI_OK;
 }
 
 int launch_gemm_tc(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision)

@@ -73,6 +73,8 @@ namespace chai {
 
 int set_error(chai_cuda_ctx* ctx, int status, const std::string& msg);
 int cuda_status(chai_cuda_ctx* ctx, cudaError_t e, const char* what);
+int launch_wait_selftest(chai_cuda_ctx* ctx, double limit_ms);   // gemm_tc.cu
+
 // Grow the context scratch to at least `bytes` (stream-ordered).
 int ensure_scratch(chai_cuda_ctx* ctx, size_t bytes);
 Buffer* find_buffer(chai_cuda_ctx* ctx, uint64_t id);

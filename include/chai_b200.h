@@ -78,6 +78,14 @@ int chai_cuda_init(int device, const char* config, chai_cuda_ctx** out);
 int chai_cuda_shutdown(chai_cuda_ctx* ctx);
 int chai_cuda_synchronize(chai_cuda_ctx* ctx);
 const char* chai_cuda_error_string(int status);
+/* Failure-detection self-test: one kernel waits on a shared-memory mbarrier
+ * that nothing arrives on, with the bounded wait every persistent kernel of
+ * this library uses (try_wait in a loop limited by %globaltimer); after
+ * `limit_ms` (0 < limit_ms <= 2000) it gives up and writes the context status
+ * word, so the call returns CHAI_ERR_TIMEOUT and the context stays usable.
+ * No counterpart in the reference (its device code has no waits). */
+int chai_cuda_selftest_wait(chai_cuda_ctx* ctx, double limit_ms);
+
 /* Human-readable detail of the last failure on this context. */
 const char* chai_cuda_last_error(chai_cuda_ctx* ctx);
 /* Device time of a hot kernel ("gemm_tc", "trace", "gemv") accumulated over
