@@ -12,10 +12,158 @@
 // when beta != 0).
 #include <cuda_runtime.h>
 
+#include "chai_trace_prelude.cuh"
 #include "internal.h"
 #include "tuner.h"
 
 namespace chai {
+
+// ------------------------------------------------- bulk-copy GEMV (A x)
+// A streamed through shared memory by cp.async.bulk (the copy engine keeps
+// the bytes in flight, not registers): each block owns a contiguous run of
+// rows; a producer warp issues 16 KB row chunks into a 4-stage ring, 8
+// consumer warps each take 16 consecutive bytes per thread of a chunk (x from
+// L1), and the 256 partial sums of a row are reduced in a fixed tree.  Used
+// when A, x, the row pitch and the row length are 16-byte aligned.
+constexpr int GB_STAGES = 4, GB_CHUNK = 16384, GB_CONSUMERS = 8;
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(chai_k::smem_u32(dst)), "l"(src), "r"(bytes), "r"(chai_k::smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(chai_k::smem_u32(bar)) : "memory");
+}
+
+template <class T>
+__global__ void __launch_bounds__((GB_CONSUMERS + 1) * 32) chai_gemv_bulk(const T* __restrict__ A, long long lda,
+                                                                           const T* __restrict__ x, T* __restrict__ y,
+                                                                           long long m, long long n, T alpha, T beta,
+                                                                           long long rows_per_block, int* status)
+{
+    typedef typename std::conditional<sizeof(T) == 4, float4, double2>::type V;
+    constexpr int VE = 16 / sizeof(T);                      // elements per 16 bytes
+    constexpr int CE = GB_CHUNK / sizeof(T);                // elements per chunk
+    constexpr int PER = CE / (GB_CONSUMERS * 32 * VE);      // 16-byte vectors per thread per chunk
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long full[GB_STAGES], empty[GB_STAGES];
+    __shared__ T red[2][GB_CONSUMERS];
+    __shared__ int abort_flag;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long r0 = (long long)blockIdx.x * rows_per_block;
+    const long long r1 = r0 + rows_per_block < m ? r0 + rows_per_block : m;
+    const long long cpr = (n + CE - 1) / CE;                // chunks per row
+    const long long jobs = r0 < r1 ? (r1 - r0) * cpr : 0;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < GB_STAGES; s++) {
+            chai_k::mbar_init(&full[s], 1);
+            chai_k::mbar_init(&empty[s], GB_CONSUMERS);
+        }
+        abort_flag = 0;
+    }
+    __syncthreads();
+    if (warp == GB_CONSUMERS) {
+        // producer
+        if (lane == 0) {
+            long long issued = 0;
+            for (long long j = 0; j < jobs && !abort_flag; j++) {
+                const int s = (int)(j % GB_STAGES);
+                const long long round = j / GB_STAGES;
+                if (round > 0 && !chai_k::mbar_wait_bounded(&empty[s], (unsigned)((round - 1) & 1), status)) {
+                    abort_flag = 1;
+                    break;
+                }
+                const long long row = r0 + j / cpr, c = j % cpr;
+                const long long len = (n - c * CE) < CE ? (n - c * CE) : CE;
+                chai_k::mbar_expect_tx(&full[s], (unsigned)(len * sizeof(T)));
+                bulk_load(smem + (size_t)s * GB_CHUNK, A + row * lda + c * CE, (unsigned)(len * sizeof(T)), &full[s]);
+                issued = j + 1;
+            }
+            // every issued copy has landed before the block exits
+            for (long long j = issued - GB_STAGES < 0 ? 0 : issued - GB_STAGES; j < issued; j++)
+                chai_k::mbar_wait_bounded(&full[j % GB_STAGES], (unsigned)((j / GB_STAGES) & 1), status);
+        }
+        return;
+    }
+    // consumers
+    // A wait that runs out (or another warp's) marks the warp bad: it stops
+    // waiting and computing but still reaches every row's named barrier, so no
+    // consumer warp can block on one that left.
+    const int t = threadIdx.x;                              // 0 .. 255
+    T acc = 0;
+    bool bad = false;
+    for (long long j = 0; j < jobs; j++) {
+        const int s = (int)(j % GB_STAGES);
+        if (!bad) {
+            if (*reinterpret_cast<volatile int*>(&abort_flag)) bad = true;
+            else if (!chai_k::mbar_wait_bounded(&full[s], (unsigned)((j / GB_STAGES) & 1), status)) {
+                abort_flag = 1;
+                bad = true;
+            }
+        }
+        const long long row = r0 + j / cpr, c = j % cpr;
+        if (!bad) {
+            const long long len = (n - c * CE) < CE ? (n - c * CE) : CE;
+            const V* av = reinterpret_cast<const V*>(smem + (size_t)s * GB_CHUNK);
+            const V* xv = reinterpret_cast<const V*>(x + c * CE);
+#pragma unroll
+            for (int i = 0; i < PER; i++) {
+                const int v = i * (GB_CONSUMERS * 32) + t;      // vector index within the chunk
+                if ((long long)v * VE < len) {
+                    const V a = av[v];
+                    const V b = __ldg(xv + v);
+                    const T* pa = reinterpret_cast<const T*>(&a);
+                    const T* pb = reinterpret_cast<const T*>(&b);
+#pragma unroll
+                    for (int e = 0; e < VE; e++) acc = fma(pa[e], pb[e], acc);
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0 && !bad) mbar_arrive(&empty[s]);
+        if (c == cpr - 1) {
+            // row done: fixed-order tree over the 256 consumer threads
+            T w = acc;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+            const int par = (int)((row - r0) & 1);
+            if (lane == 0) red[par][warp] = w;
+            asm volatile("bar.sync 1, %0;" ::"n"(GB_CONSUMERS * 32));
+            if (t == 0) {
+                T sum = 0;
+#pragma unroll
+                for (int k = 0; k < GB_CONSUMERS; k++) sum += red[par][k];
+                y[row] = beta == (T)0 ? alpha * sum : alpha * sum + beta * y[row];
+            }
+            acc = 0;
+        }
+    }
+}
+
+static bool gemv_bulk_ok(const void* a, long long lda, const void* x, long long n, size_t esz)
+{
+    return ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(x)) & 15) == 0 &&
+           (lda * (long long)esz) % 16 == 0 && (n * (long long)esz) % 16 == 0 && n > 0;
+}
+
+template <class T>
+static int launch_gemv_bulk(chai_cuda_ctx* ctx, long long m, long long n, T alpha, const T* a, long long lda,
+                            const T* x, T beta, T* y)
+{
+    const int smem = GB_STAGES * GB_CHUNK;
+    cudaFuncSetAttribute(chai_gemv_bulk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const long long blocks = std::min<long long>(m, (long long)ctx->sm_count * 3);
+    const long long rpb = (m + blocks - 1) / blocks;
+    const long long grid = (m + rpb - 1) / rpb;
+    chai_gemv_bulk<T><<<(unsigned)grid, (GB_CONSUMERS + 1) * 32, smem, ctx->stream>>>(a, lda, x, y, m, n, alpha,
+                                                                                       beta, rpb, ctx->status_word);
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    return CHAI_OK;
+}
 
 template <class T, int WARPS, int UNROLL>
 __global__ void __launch_bounds__(WARPS * 32) chai_gemv_n(const T* __restrict__ A, long long lda,
@@ -120,6 +268,13 @@ static int gemv_t(chai_cuda_ctx* ctx, int trans, int64_t m, int64_t n, double al
         else tuned_gemv_cfg(ctx, m, n, sizeof(T) == 8 ? CHAI_F64 : CHAI_F32, &cfg);
         cudaEvent_t ev[2];
         ktime_begin(ctx, "gemv", ev);
+        if (cfg.warps == 0 && m > 0 && gemv_bulk_ok(a, lda, x, n, sizeof(T))) {
+            const int st = launch_gemv_bulk<T>(ctx, m, n, (T)alpha, (const T*)a, lda, (const T*)x, (T)beta, (T*)y);
+            if (st) return st;
+            ktime_end(ctx, "gemv", ev);
+            return CHAI_OK;
+        }
+        if (cfg.warps == 0) cfg = GemvCfg{4, 1};
 #define CHAI_GV(W, U)                                                                                       \
     chai_gemv_n<T, W, U><<<(unsigned)((m + W - 1) / W), W * 32, 0, ctx->stream>>>((const T*)a, lda, (const T*)x, \
                                                                                  (T*)y, m, n, (T)alpha, (T)beta)

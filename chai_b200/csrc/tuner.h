@@ -24,8 +24,10 @@ bool tuned_tc_cfg(chai_cuda_ctx* ctx, long long m, long long n, long long k, int
 
 // GEMV configuration (gemv.cu): warps (rows) per block, 16-byte loads in
 // flight per lane.
+// warps = 0 selects the bulk-copy kernel (A streamed through shared memory by
+// cp.async.bulk) when the operands are 16-byte aligned.
 struct GemvCfg {
-    int warps = 4, unroll = 1;   // the fastest at 8192^2 in f32 and f64 (exhaustive sweep on a B200)
+    int warps = 0, unroll = 1;
 };
 bool tuned_gemv_cfg(chai_cuda_ctx* ctx, long long m, long long n, int prec, GemvCfg* out);
 

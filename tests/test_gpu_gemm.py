@@ -126,3 +126,27 @@ def test_gemm_paranoid_l1(chai_dev, prec):
     Cg = run_gemm(chai_dev, A, B, prec)
     assert np.abs(Cg - oracle.gemm_f64(A, B)).sum() < 1.0
     assert abs(Cg.mean() - 0.25 * n) / (0.25 * n) < 0.1
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("shape", [(1, 4), (37, 4096), (300, 8192), (1000, 4100), (5, 20000)])
+def test_gemv_bulk_copy_path(chai_dev, dtype, shape):
+    """The cp.async.bulk GEMV (16-byte aligned A, x, pitch and row length):
+    rows shorter than one 16 KB chunk, exactly one, several, a ragged last
+    chunk; alpha and beta applied once.  Against the FP64 product,
+    componentwise-normalised: 2^-20 (f32), 2^-45 (f64)."""
+    import torch
+    m, n = shape
+    rng = np.random.default_rng(m + n)
+    A = rng.uniform(-1, 1, (m, n)).astype(dtype)
+    x = rng.uniform(-1, 1, n).astype(dtype)
+    y0 = rng.uniform(-1, 1, m).astype(dtype)
+    a, xv, y = torch.from_numpy(A).cuda(), torch.from_numpy(x).cuda(), torch.from_numpy(y0.copy()).cuda()
+    prec = L.F32 if dtype == np.float32 else L.F64
+    L.check(L.lib().chai_cuda_gemv(chai_dev.ctx, prec, 0, m, n, 0.5, a.data_ptr(), n, xv.data_ptr(), -2.0,
+                                   y.data_ptr()), chai_dev.ctx)
+    L.check(L.lib().chai_cuda_synchronize(chai_dev.ctx), chai_dev.ctx)
+    want = 0.5 * (A.astype(np.float64) @ x.astype(np.float64)) - 2.0 * y0.astype(np.float64)
+    bound = 0.5 * (np.abs(A).astype(np.float64) @ np.abs(x).astype(np.float64)) + 2.0 * np.abs(y0)
+    err = np.max(np.abs(y.cpu().numpy().astype(np.float64) - want) / bound)
+    assert err <= (2.0 ** -20 if dtype == np.float32 else 2.0 ** -45), err
