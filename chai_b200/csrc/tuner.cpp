@@ -58,6 +58,10 @@ std::vector<chai_gemm_cfg> Tuner::space(const chai_gemm_key& key)
 {
     std::vector<chai_gemm_cfg> v;
     if (key.is_gemv) {
+        chai_gemm_cfg bulk{};          // warps 0: the cp.async.bulk kernel
+        bulk.vec_width = 1;
+        bulk.cluster_m = bulk.cluster_n = 1;
+        v.push_back(bulk);
         for (int w : {4, 8, 16})
             for (int u : {1, 4}) {
                 chai_gemm_cfg c{};

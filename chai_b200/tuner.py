@@ -19,7 +19,7 @@ from . import _lib as L
 
 N_FEATURES = 12
 GEMM_SPACE = 12
-GEMV_SPACE = 6
+GEMV_SPACE = 7
 
 
 def key(m, n, k=1, precision=L.GEMM_BF16X3, is_gemv=False) -> L.chai_gemm_key:
@@ -155,7 +155,7 @@ def evaluate(ctx, held_out, default_ids=None):
         t0 = time.perf_counter()
         sweep(ctx, k)
         t_exh = time.perf_counter() - t0
-        dflt = (4, 0, 0, 0, 1, 0) if k.is_gemv else (128, 256, 128, 4, 4, 16)
+        dflt = (0, 0, 0, 0, 1, 0) if k.is_gemv else (128, 256, 128, 4, 4, 16)
         rows.append(dict(m=k.m, n=k.n, k=k.k, precision=k.precision, gemv=k.is_gemv, best_us=best,
                          pick_us=by_id.get(cfg_id(pick), float("nan")),
                          default_us=by_id.get(dflt, float("nan")), learned_s=t_learned, exhaustive_s=t_exh))

@@ -299,7 +299,8 @@ typedef struct chai_gemm_key {
 /* GEMM: block_m 128, block_n 128|256 (tcgen05 N tile), block_k 128 bytes,
  * stages 3..6 (shared-memory pipeline), group_m (tile-raster strip height),
  * cluster 1x1.  GEMV: block_m = warps (rows) per block, vec_width = 16-byte
- * loads in flight per lane. */
+ * loads in flight per lane; block_m = 0 is the bulk-copy kernel (A streamed
+ * through shared memory, 16-byte aligned operands). */
 typedef struct chai_gemm_cfg {
     int32_t block_m, block_n, block_k, stages;
     int32_t vec_width, cluster_m, cluster_n, group_m;

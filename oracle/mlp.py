@@ -32,7 +32,7 @@ GEMM_FP32, GEMM_TF32, GEMM_BF16, GEMM_BF16X3, GEMM_BF16X6, GEMM_FP8, GEMM_FP64 =
 def space(is_gemv: bool):
     """Search space as dicts of chai_gemm_cfg fields (tuner.cpp Tuner::space)."""
     if is_gemv:
-        return [dict(block_m=w, vec_width=u) for w in (4, 8, 16) for u in (1, 4)]
+        return [dict(block_m=0, vec_width=1)] + [dict(block_m=w, vec_width=u) for w in (4, 8, 16) for u in (1, 4)]
     out = []
     for bn in (128, 256):
         for s in ((3, 4) if bn == 256 else (4, 6)):
