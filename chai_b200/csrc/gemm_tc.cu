@@ -802,40 +802,36 @@ struct ColJob {
     int tiles, tiles_n, k, kpad, cols, pad;
 };
 
-// 4 rows per 256-thread block (64 threads x 8 elements per row pass)
+// One block per problem: its 8 warps take the problem's rows in turn, each
+// lane splitting 8 consecutive elements per pass (no per-row search of the
+// job table).
 template <int S>
-__global__ void __launch_bounds__(256) grouped_split_rows(const RowJob* __restrict__ jobs, int njobs, long long nrows,
+__global__ void __launch_bounds__(256) grouped_split_rows(const RowJob* __restrict__ jobs, int njobs,
                                                           __nv_bfloat16* __restrict__ out, long long pitch,
                                                           int plane_k)
 {
-    const long long row = (long long)blockIdx.x * 4 + (threadIdx.x >> 6);
-    if (row >= nrows) return;
-    const int lane = threadIdx.x & 63;
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (jobs[mid].row0 <= row) lo = mid; else hi = mid - 1;
-    }
-    const RowJob j = jobs[lo];
-    const float* x = j.src + (row - j.row0) * (long long)j.k;
-    __nv_bfloat16* o = out + row * pitch;
+    const RowJob j = jobs[blockIdx.x];
     constexpr int P = Planes<S>::P;
-    const bool vec = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
-    for (int k8 = lane; k8 * 8 < j.kpad; k8 += 64) {
-        const int kk = k8 * 8;
-        float a[8];
-        if (vec && kk + 8 <= j.k) {
-            const float4 u = __ldg(reinterpret_cast<const float4*>(x + kk));
-            const float4 w = __ldg(reinterpret_cast<const float4*>(x + kk) + 1);
-            a[0] = u.x; a[1] = u.y; a[2] = u.z; a[3] = u.w; a[4] = w.x; a[5] = w.y; a[6] = w.z; a[7] = w.w;
-        } else {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool vec = (reinterpret_cast<uintptr_t>(j.src) & 15) == 0 && (j.k & 3) == 0;
+    for (int r = warp; r < j.rows; r += 8) {
+        const float* x = j.src + (long long)r * j.k;
+        __nv_bfloat16* o = out + (j.row0 + r) * pitch;
+        for (int kk = lane * 8; kk < j.kpad; kk += 256) {
+            float a[8];
+            if (vec && kk + 8 <= j.k) {
+                const float4 u = __ldg(reinterpret_cast<const float4*>(x + kk));
+                const float4 w = __ldg(reinterpret_cast<const float4*>(x + kk) + 1);
+                a[0] = u.x; a[1] = u.y; a[2] = u.z; a[3] = u.w; a[4] = w.x; a[5] = w.y; a[6] = w.z; a[7] = w.w;
+            } else {
 #pragma unroll
-            for (int i = 0; i < 8; i++) a[i] = kk + i < j.k ? __ldg(x + kk + i) : 0.0f;
+                for (int i = 0; i < 8; i++) a[i] = kk + i < j.k ? __ldg(x + kk + i) : 0.0f;
+            }
+            uint4 q[3];
+            split8(a, q);
+#pragma unroll
+            for (int p = 0; p < P; p++) *reinterpret_cast<uint4*>(o + (long long)p * plane_k + kk) = q[p];
         }
-        uint4 q[3];
-        split8(a, q);
-#pragma unroll
-        for (int p = 0; p < P; p++) *reinterpret_cast<uint4*>(o + (long long)p * plane_k + kk) = q[p];
     }
 }
 
@@ -844,40 +840,44 @@ __global__ void __launch_bounds__(256) grouped_split_cols(const ColJob* __restri
                                                           __nv_bfloat16* __restrict__ out, long long pitch,
                                                           int plane_k)
 {
+    // one block per problem, looping over its 64 x 64 tiles (no per-tile search)
     __shared__ float tile[64][65];
-    const long long t = blockIdx.x;
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (jobs[mid].tile0 <= t) lo = mid; else hi = mid - 1;
-    }
-    const ColJob j = jobs[lo];
-    const int local = (int)(t - j.tile0);
-    const int kt = local / j.tiles_n, nt = local - kt * j.tiles_n;
-    const int k0 = kt * 64, c0 = nt * 64;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    for (int i = ty; i < 64; i += 16) {
-        const int kk = k0 + i;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int cc = c0 + tx * 4 + q;
-            tile[i][tx * 4 + q] = (kk < j.k && cc < j.cols) ? __ldg(j.src + (long long)kk * j.cols + cc) : 0.0f;
-        }
-    }
-    __syncthreads();
+    const ColJob j = jobs[blockIdx.x];
     constexpr int P = Planes<S>::P;
-    for (int item = threadIdx.x; item < 512; item += 256) {
-        const int c = item >> 3, r = item & 7;
-        const int cc = c0 + c, kk = k0 + r * 8;
-        if (cc >= j.cols || kk >= j.kpad) continue;
-        float a[8];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const bool vec = (reinterpret_cast<uintptr_t>(j.src) & 15) == 0 && (j.cols & 3) == 0;
+    for (int local = 0; local < j.tiles; local++) {
+        const int kt = local / j.tiles_n, nt = local - kt * j.tiles_n;
+        const int k0 = kt * 64, c0 = nt * 64;
+        for (int i = ty; i < 64; i += 16) {
+            const int kk = k0 + i, cc = c0 + tx * 4;
+            float v[4];
+            if (vec && kk < j.k && cc + 4 <= j.cols) {
+                const float4 u = __ldg(reinterpret_cast<const float4*>(j.src + (long long)kk * j.cols + cc));
+                v[0] = u.x; v[1] = u.y; v[2] = u.z; v[3] = u.w;
+            } else {
 #pragma unroll
-        for (int i = 0; i < 8; i++) a[i] = tile[r * 8 + i][c];
-        uint4 q[3];
-        split8(a, q);
-        __nv_bfloat16* o = out + (j.row0 + cc) * pitch;
+                for (int q = 0; q < 4; q++)
+                    v[q] = (kk < j.k && cc + q < j.cols) ? __ldg(j.src + (long long)kk * j.cols + cc + q) : 0.0f;
+            }
 #pragma unroll
-        for (int p = 0; p < P; p++) *reinterpret_cast<uint4*>(o + (long long)p * plane_k + kk) = q[p];
+            for (int q = 0; q < 4; q++) tile[i][tx * 4 + q] = v[q];
+        }
+        __syncthreads();
+        for (int item = threadIdx.x; item < 512; item += 256) {
+            const int c = item >> 3, r = item & 7;
+            const int cc = c0 + c, kk = k0 + r * 8;
+            if (cc >= j.cols || kk >= j.kpad) continue;
+            float a[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) a[i] = tile[r * 8 + i][c];
+            uint4 q[3];
+            split8(a, q);
+            __nv_bfloat16* o = out + (j.row0 + cc) * pitch;
+#pragma unroll
+            for (int p = 0; p < P; p++) *reinterpret_cast<uint4*>(o + (long long)p * plane_k + kk) = q[p];
+        }
+        __syncthreads();
     }
 }
 
@@ -1171,8 +1171,8 @@ int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_p
     CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(drj, rj.data(), r_bytes, cudaMemcpyHostToDevice, s));
     CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(dcj, cj.data(), c_bytes, cudaMemcpyHostToDevice, s));
 #define GSPLIT(SS)                                                                                      \
-    grouped_split_rows<SS><<<(unsigned)((ra + 3) / 4), 256, 0, s>>>(drj, count, ra, Ap, pitch, (int)kmax); \
-    grouped_split_cols<SS><<<(unsigned)coltiles, 256, 0, s>>>(dcj, count, Bp, pitch, (int)kmax)
+    grouped_split_rows<SS><<<(unsigned)count, 256, 0, s>>>(drj, count, Ap, pitch, (int)kmax);              \
+    grouped_split_cols<SS><<<(unsigned)count, 256, 0, s>>>(dcj, count, Bp, pitch, (int)kmax)
     if (S == 1) { GSPLIT(1); } else if (S == 3) { GSPLIT(3); } else { GSPLIT(6); }
 #undef GSPLIT
     CHAI_CUDA_TRY(ctx, cudaGetLastError());
