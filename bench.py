@@ -780,6 +780,34 @@ WORKLOADS = {"gemm": run_gemm, "mc": run_mc, "mc-hbm": run_mc_hbm, "kirsch": run
 
 # ---------------------------------------------------------------- reference arm
 
+def workload_desc(args):
+    """The workload names the two arms share (the same strings the GPU arm's
+    `config.workload` carries)."""
+    wl = args.workload
+    if wl == "gemm":
+        n = args.size or 16384
+        return ("square GEMM M=N=K=%d, f32 operands uniform[-1,1) (chai Philox seeds 1,2), %s"
+                % (n, args.precision)), args.precision
+    if wl == "mc":
+        return "Monte Carlo trace, 2^27 Philox4x32-10 Box-Muller normals, fused", "f32"
+    if wl == "mc-hbm":
+        return "Monte Carlo payoff over 2^27 f32 normals already in HBM (materialised Z), fused", "f32"
+    if wl == "kirsch":
+        W = args.size or 8192
+        return "Kirsch 8-direction compass filter via gather2_floor, %dx%d f32 uniform[0,1)" % (W, W), "f32"
+    if wl == "gemv":
+        m = args.size or 8192
+        p = "f64" if args.precision == "f64" else "f32"
+        return "GEMV y = A x, %dx%d %s" % (m, m, p), p
+    if wl == "mc-many":
+        return ("64 MC traces, lengths log-uniform in [2^12, 2^22] (seed 7), one persistent kernel + combine "
+                "captured in a CUDA graph"), "f32"
+    if wl == "grouped":
+        return ("4096 grouped f32 GEMMs, M,N,K multiples of 8 in [32,512] (seed 11), one persistent tcgen05 "
+                "launch"), "bf16x3"
+    return wl, "f32"
+
+
 def run_reference(args, steps=None):
     """The reference's own CPU implementation of the path -- its bytecode
     interpreter (runtime/Interpreter.cpp), built from the reference sources into
@@ -804,7 +832,7 @@ def run_reference(args, steps=None):
             cmd = [str(drv), "gemm_f32", str(n), str(n), str(n), td + "/A", td + "/B", td + "/C"]
             unit, metric = "TFLOP/s", "GEMM TFLOP/s at err vs FP32"
             conv = lambda ms: 2.0 * n ** 3 / (ms * 1e-3) / 1e12
-            sample = "interpreter matmul 512^3 f32 (double accumulation), inputs via make2"
+            sample = "interpreter matmul 512^3 f32 (f32 products summed in double), inputs via make2"
         elif wl == "grouped":
             cmd = None
             unit, metric = "TFLOP/s", "GEMM TFLOP/s at err vs FP32"
@@ -875,8 +903,13 @@ def run_reference(args, steps=None):
             times.append(float(r.stdout.split("ms=")[1].split()[0]))
     ms = statistics.median(times)
     v = conv(ms)
+    desc, _ = workload_desc(args)
     return {"impl": "reference", "metric": metric, "value": v, "unit": unit, "ms_per_step": ms,
-            "higher_is_better": True,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if (wl == "gemv" and args.precision == "f64") else "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": desc, "reference_sample": sample,
+                       "parallelism": "one interpreter device thread (runtime/DeviceMap.cpp:17-23)"},
             "cpu_baseline": {"value": v, "unit": unit, "cores": 1, "kind": "reference", "sample": sample},
             "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
