@@ -396,6 +396,11 @@ class Array(ArrayExp):
         return self
 
     def cells(self, out):
+        # a value from an earlier trace stays alive (with its device buffer)
+        # until the pending trace that reads it has run, as the reference's
+        # client trace holds its operands (common/ClientTrace.cpp RefSet)
+        if self._buffer is not None:
+            _Client.keep.append(self)
         out.append(_bc(L.BC_VARIABLE, self.var, self.version - 1))
 
     # read-backs (api/ArrayFP.cpp:86-228)
