@@ -516,6 +516,7 @@ def ones_u32(W, H=None): return _fill(L.U32, True, W, H)
 # ------------------------------------------------------------------ RNG
 
 RNG_PHILOX, RNG_THREEFRY = L.PHILOX, L.THREEFRY
+RNG_DEFAULT = RNG_PHILOX          # api/chai.h:416
 
 
 class _RNG:

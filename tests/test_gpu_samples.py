@@ -112,3 +112,60 @@ def test_loopsum_sample(ch):
             for k in range(3):
                 want = want + f32(5 + j)
         assert abs(got - float(want.astype(np.float64).sum())) <= 1e-5 * abs(got)
+
+
+def test_pi_sample(ch):
+    """sample/pi.cpp: two uniform fills from one generator (the second starts
+    where the first ended), sqrt(X^2 + Y^2) <= 1, 4 sum / NSET; exact."""
+    import oracle
+    NSET = 1000000
+    G = ch.RNGf32(ch.RNG_DEFAULT, 271828)
+    X = ch.Arrayf32(ch.rng_uniform_make(G, NSET, 1, 1, 0.0, 1.0))
+    Y = ch.Arrayf32(ch.rng_uniform_make(G, NSET, 1, 1, 0.0, 1.0))
+    distance_from_zero = ch.Arrayf32(ch.sqrt(X * X + Y * Y))
+    inside_circle = ch.Arrayf32(distance_from_zero <= f32(1.0))
+    pi = float(ch.Arrayf32(f32(4.0) * ch.sum(inside_circle) / NSET).read_scalar())
+    x = oracle.rng_fill(NSET, seed=271828, limits=(0.0, 1.0))
+    y = oracle.rng_fill(NSET, seed=271828 + NSET, limits=(0.0, 1.0))
+    count = f32(np.count_nonzero(np.sqrt(x * x + y * y) <= f32(1.0)))
+    assert pi == float(f32(f32(4.0) * count) / f32(NSET))
+    assert abs(pi - np.pi) < 0.01
+
+
+def test_american_option_sample(ch):
+    """sample/finance/american_option.cpp: binomial tree in f64, one trace per
+    step with a shrinking length, gather1_floor(option, IDX + 1) wrapping at
+    the end; exact against the same arithmetic in numpy."""
+    price, strike, vol, rate, maturity, steps = 100.0, 100.0, 0.25, 0.10, 1.0, 100
+    R = np.exp(rate * (maturity / steps))
+    up = np.exp(vol * np.sqrt(maturity / steps))
+    down = 1.0 / up
+    prUp = (R - down) / (up - down)
+    prDown = 1.0 - prUp
+    prices0 = np.empty(steps + 1)
+    prices0[0] = price * down ** steps
+    for i in range(1, steps + 1):
+        prices0[i] = prices0[i - 1] * up * up
+    option0 = np.maximum(prices0 - strike, 0.0)
+    pg, og = prices0.copy(), option0.copy()
+    pn, on = prices0.copy(), option0.copy()
+    disc = float(np.exp(rate * (maturity / steps)))
+    for i in range(steps):
+        N = steps + 1 - i
+        prices = ch.make1(pg[:N].copy())
+        option = ch.make1(og[:N].copy())
+        IDX = ch.index_f64(0, N)
+        no_exercise = ch.Arrayf64((float(prDown) * ch.gather1_floor(option, IDX)
+                                   + float(prUp) * ch.gather1_floor(option, IDX + 1)) / disc)
+        prices = ch.Arrayf64(float(up) * prices)
+        option = ch.Arrayf64(ch.max(no_exercise, prices - strike))
+        pg[:N] = prices.read1()
+        og[:N] = option.read1()
+        # numpy, same operations and order
+        o = on[:N]
+        ne = (float(prDown) * o + float(prUp) * np.roll(o, -1)) / disc
+        pn[:N] = float(up) * pn[:N]
+        b = pn[:N] - strike
+        on[:N] = np.where(ne < b, b, ne)
+    assert np.array_equal(og, on) and np.array_equal(pg, pn)
+    assert 10.0 < og[0] < 20.0
