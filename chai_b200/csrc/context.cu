@@ -158,6 +158,10 @@ static void parse_config(chai::Config& c, const char* text)
             c.stencil_rows = atoi(v.c_str());
         } else if (k == "StencilMinBlocks") {
             c.stencil_min_blocks = std::max(0, std::min(8, atoi(v.c_str())));
+        } else if (k == "GroupedSplit") {
+            c.grouped_fused = v != "prepass";
+        } else if (k == "PackF32") {
+            c.pack_f32 = v != "0" && v != "off";
         } else if (k == "PlanCache") {
             c.plan_cache = v != "0" && v != "off";
         } else if (k == "TuneJournal") {
@@ -245,6 +249,7 @@ int chai_cuda_shutdown(chai_cuda_ctx* ctx)
         if (kv.second.owned && kv.second.ptr) cudaFree(kv.second.ptr);
     ctx->buffers.clear();
     if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->gplan.dev) cudaFree(ctx->gplan.dev);
     if (ctx->status_word) cudaFree(ctx->status_word);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -262,6 +267,12 @@ int chai_cuda_kernel_stats(chai_cuda_ctx* ctx, const char* name, double* total_m
         if (total_ms) *total_ms = 0;
         if (launches) *launches = ctx->plan_hits;
         if (reset) ctx->plan_hits = 0;
+        return CHAI_OK;
+    }
+    if (std::string(name) == "grouped_fused") {    // grouped GEMMs split inside the GEMM kernel
+        if (total_ms) *total_ms = 0;
+        if (launches) *launches = ctx->fused_launches;
+        if (reset) ctx->fused_launches = 0;
         return CHAI_OK;
     }
     CHAI_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));

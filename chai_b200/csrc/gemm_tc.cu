@@ -881,6 +881,369 @@ __global__ void __launch_bounds__(256) grouped_split_cols(const ColJob* __restri
     }
 }
 
+// ------------------------------------------- grouped GEMM, split in-kernel
+//
+// The grouped problems are small (K of a few hundred), so the prepass's
+// round trip of the bf16 planes through HBM costs more than the MMAs.  This
+// kernel reads the f32 operands once and splits them in shared memory:
+//   host        driver-encoded tensor maps of each problem's A and B (cached
+//               per context), uploaded with one record per output tile
+//               (fs_tiles)
+//   warp 0      producer: TMA-loads each 64-element K chunk of A (2 boxes of
+//               128 rows x 32 f32) and B (4 boxes of 64 k x 32 f32,
+//               SWIZZLE_128B) through the tile's problem maps into one of two
+//               f32 stages; the maps zero-fill past M, N and K
+//   warp 1      TMEM owner; one thread issues the S product blocks of each
+//               chunk (4 x tcgen05.mma, M = N = 128, K = 16 each)
+//   warps 2-5   epilogue (TMEM lane quarter = warp % 4)
+//   warps 6-13  converters: f32 stage -> the P distinct bf16 planes of A and
+//               B (K-major, SWIZZLE_128B rows of 64 bf16)
+// The MMA sequence (planes, order, accumulators) is the one the prepass path
+// issues, so both paths give bit-identical C.
+constexpr int FS_BN = 128;
+constexpr int FS_KB = 64;                      // K elements per chunk
+constexpr int FS_NF = 2;                       // f32 stages
+constexpr int FS_CONV = 8;                     // converter warps
+constexpr int FS_CT = FS_CONV * 32;            // converter threads
+constexpr int FS_THREADS = (6 + FS_CONV) * 32;
+constexpr int FS_A_F32 = BM * FS_KB * 4;       // 32 KiB: 2 boxes [128 rows][32 f32]
+constexpr int FS_B_F32 = FS_KB * FS_BN * 4;    // 32 KiB: 4 boxes [64 k][32 f32]
+constexpr int FS_PLANE = BM * 128;             // 16 KiB: 128 rows x 64 bf16 (A and B planes alike)
+
+__host__ __device__ constexpr int fs_smem_bytes(int S)
+{
+    return FS_NF * (FS_A_F32 + FS_B_F32) + 2 * distinct_planes(S) * FS_PLANE + 1024 + 256;
+}
+
+struct FusedEntry {
+    long long tile_start;   // first tile of the problem in the global tile list
+    const float* a;         // m x k, row-major, leading dimension k
+    const float* b;         // k x n, row-major, leading dimension n
+    float* c;               // m x n, row-major, leading dimension n
+    int m, n, k, tiles_n, kblocks, vec_ok;
+};
+
+// Everything a role needs about one 128 x 128 output tile (one 64-byte
+// record per tile, written by fs_tiles before the GEMM).
+struct __align__(16) FsTile {
+    float* c;               // C(tile origin)
+    int prob;               // problem index: its tensor maps are at maps + 256 prob (A), + 128 (B)
+    int m, n, k;
+    int row0, col0;         // tile origin in C
+    int rows, cols;         // valid rows / columns of the tile (<= 128)
+    int kblocks, vec_ok;
+};
+
+__global__ void __launch_bounds__(128) fs_tiles(const FusedEntry* __restrict__ groups, FsTile* __restrict__ out)
+{
+    const FusedEntry g = groups[blockIdx.x];
+    const int tiles = ((g.m + BM - 1) / BM) * g.tiles_n;
+    for (int l = threadIdx.x; l < tiles; l += blockDim.x) {
+        const int tm = l / g.tiles_n, tn = l - tm * g.tiles_n;
+        FsTile t;
+        t.c = g.c + (long long)tm * BM * g.n + (long long)tn * FS_BN;
+        t.prob = blockIdx.x;
+        t.m = g.m;
+        t.n = g.n;
+        t.k = g.k;
+        t.row0 = tm * BM;
+        t.col0 = tn * FS_BN;
+        t.rows = min(BM, g.m - tm * BM);
+        t.cols = min(FS_BN, g.n - tn * FS_BN);
+        t.kblocks = g.kblocks;
+        t.vec_ok = g.vec_ok;
+        out[g.tile_start + l] = t;
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const void* map, unsigned bar, int x, int y)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+                 ::"r"(dst), "l"(map), "r"(bar), "r"(x), "r"(y)
+                 : "memory");
+}
+
+// Two consecutive-k values -> their P bf16 planes (the split of split3, two
+// lanes at a time): p0 = bf16(x), p1 = bf16(x - p0), p2 = bf16(x - p0 - p1).
+template <int P>
+__device__ __forceinline__ void split_pair(float x, float y, unsigned (&h)[3])
+{
+    __nv_bfloat162 b = __floats2bfloat162_rn(x, y);
+    h[0] = *reinterpret_cast<unsigned*>(&b);
+    if (P > 1) {
+        const float2 f = __bfloat1622float2(b);
+        x = x - f.x;
+        y = y - f.y;
+        b = __floats2bfloat162_rn(x, y);
+        h[1] = *reinterpret_cast<unsigned*>(&b);
+        if (P > 2) {
+            const float2 g = __bfloat1622float2(b);
+            b = __floats2bfloat162_rn(x - g.x, y - g.y);
+            h[2] = *reinterpret_cast<unsigned*>(&b);
+        }
+    }
+}
+
+// byte offset of (row, 16-byte chunk) in a SWIZZLE_128B tile of 128-byte rows
+__device__ __forceinline__ unsigned sw128(int row, int chunk)
+{
+    return (unsigned)(row * 128 + ((chunk ^ (row & 7)) << 4));
+}
+
+// f32 stage -> planes.  A: converter warp cw takes rows 16 cw .. + 15; per
+// step, lanes 8q .. 8q + 7 read the eight 16-byte chunks of one row of one
+// 32-k box.  B: thread ct takes column n = ct % 128 and four runs of 8 k.
+template <int P>
+__device__ __forceinline__ void fs_convert(const unsigned char* fa, const unsigned char* fb, unsigned char* pa,
+                                           unsigned char* pb, int cw, int lane, int ct)
+{
+    const int c = lane & 7;
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int row = cw * 16 + 4 * q + (lane >> 3);
+            const float4 x = *reinterpret_cast<const float4*>(fa + h * (BM * 128) + sw128(row, c));
+            unsigned h0[3], h1[3];
+            split_pair<P>(x.x, x.y, h0);
+            split_pair<P>(x.z, x.w, h1);
+            const unsigned off = sw128(row, 4 * h + (c >> 1)) + (c & 1) * 8;
+#pragma unroll
+            for (int p = 0; p < P; p++) *reinterpret_cast<uint2*>(pa + p * FS_PLANE + off) = make_uint2(h0[p], h1[p]);
+        }
+    const int n = ct & (FS_BN - 1);
+    const unsigned char* col = fb + (n >> 5) * (FS_KB * 128) + (n & 3) * 4;   // box of n, lane of its chunk
+    const int nc = (n & 31) >> 2;                                           // 16-byte chunk of n in a box row
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const int kc = (ct >> 7) * 4 + u;
+        unsigned h[3][4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int k0 = kc * 8 + 2 * i;
+            const float x = *reinterpret_cast<const float*>(col + sw128(k0, nc));
+            const float y = *reinterpret_cast<const float*>(col + sw128(k0 + 1, nc));
+            unsigned q[3];
+            split_pair<P>(x, y, q);
+#pragma unroll
+            for (int p = 0; p < P; p++) h[p][i] = q[p];
+        }
+        const unsigned off = sw128(n, kc);
+#pragma unroll
+        for (int p = 0; p < P; p++)
+            *reinterpret_cast<uint4*>(pb + p * FS_PLANE + off) = make_uint4(h[p][0], h[p][1], h[p][2], h[p][3]);
+    }
+}
+
+template <int S, bool ACC2>
+__global__ void __launch_bounds__(FS_THREADS, 1)
+chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const unsigned char* __restrict__ maps,
+                      int* status)
+{
+    constexpr int P = Planes<S>::P;
+    constexpr int SEL = S == 1 ? 0 : (S == 3 ? 1 : 2);
+    constexpr unsigned BUF_COLS = ACC2 ? 2 * FS_BN : FS_BN;
+    constexpr unsigned TMEM_COLS = 2 * BUF_COLS;                   // double-buffered accumulators
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* fa = smem;                                      // f32 A stages
+    unsigned char* fb = fa + FS_NF * FS_A_F32;                     // f32 B stages
+    unsigned char* pa = fb + FS_NF * FS_B_F32;                     // A planes p = 0..P-1
+    unsigned char* pb = pa + P * FS_PLANE;                         // B planes
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(pb + P * FS_PLANE);
+    unsigned long long* ffull = bars;                              // [FS_NF] TMA landed
+    unsigned long long* fempty = bars + FS_NF;                     // [FS_NF] stage read (per converter warp)
+    unsigned long long* pfull = bars + 2 * FS_NF;                  // planes written (per converter warp)
+    unsigned long long* pempty = bars + 2 * FS_NF + 1;             // planes consumed (tcgen05.commit)
+    unsigned long long* tfull = bars + 2 * FS_NF + 2;              // [2]
+    unsigned long long* tempty = bars + 2 * FS_NF + 4;             // [2]
+    unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * FS_NF + 6);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long G = gridDim.x;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < FS_NF; s++) {
+            mbar_init(smem_u32(&ffull[s]), 1);
+            mbar_init(smem_u32(&fempty[s]), FS_CONV);
+        }
+        mbar_init(smem_u32(pfull), FS_CONV);
+        mbar_init(smem_u32(pempty), 1);
+        for (int a = 0; a < 2; a++) {
+            mbar_init(smem_u32(&tfull[a]), 1);
+            mbar_init(smem_u32(&tempty[a]), 4);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            long long it = 0, issued = 0;
+            bool ok = true;
+            for (long long t = blockIdx.x; t < ntiles && ok && !*abort_flag; t += G) {
+                const FsTile ti = tiles[t];
+                const unsigned char* ga = maps + (size_t)ti.prob * 256;
+                const unsigned char* gb = ga + 128;
+                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(ga) : "memory");
+                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(gb) : "memory");
+                for (int kb = 0; kb < ti.kblocks; kb++, it++) {
+                    const int s = (int)(it % FS_NF);
+                    const long long r = it / FS_NF;
+                    if (r > 0 && !mbar_wait(smem_u32(&fempty[s]), (unsigned)((r - 1) & 1), status, 111)) {
+                        ok = false;
+                        break;
+                    }
+                    const unsigned bar = smem_u32(&ffull[s]);
+                    mbar_expect_tx(bar, FS_A_F32 + FS_B_F32);
+                    for (int h = 0; h < 2; h++)
+                        tma_load_2d(smem_u32(fa + s * FS_A_F32 + h * (BM * 128)), ga, bar, kb * FS_KB + 32 * h, ti.row0);
+                    for (int j = 0; j < 4; j++)
+                        tma_load_2d(smem_u32(fb + s * FS_B_F32 + j * (FS_KB * 128)), gb, bar, ti.col0 + 32 * j,
+                                    kb * FS_KB);
+                    issued = it + 1;
+                }
+            }
+            if (!ok) *abort_flag = 1;
+            // wait (bounded) until every copy this thread issued has landed
+            for (long long j = issued - FS_NF < 0 ? 0 : issued - FS_NF; j < issued; j++)
+                mbar_wait(smem_u32(&ffull[j % FS_NF]), (unsigned)((j / FS_NF) & 1), status, 112);
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------------------- MMA
+        if (lane == 0) {
+            const unsigned idesc = instr_desc<KIND_BF16, FS_BN>();
+            long long it = 0;
+            int lt = 0;
+            int kbs_next = blockIdx.x < ntiles ? tiles[blockIdx.x].kblocks : 0;
+            for (long long t = blockIdx.x; t < ntiles && !*abort_flag; t += G, lt++) {
+                const int kbs = kbs_next;              // loaded one tile ahead
+                if (t + G < ntiles) kbs_next = tiles[t + G].kblocks;
+                const int ab = lt & 1, use = lt >> 1;
+                if (use >= 1 && !mbar_wait(smem_u32(&tempty[ab]), (unsigned)((use - 1) & 1), status, 115)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const unsigned acc_main = tmem + (unsigned)ab * BUF_COLS;
+                const unsigned acc_corr = acc_main + (ACC2 ? FS_BN : 0);
+                bool ok = true;
+                for (int kb = 0; kb < kbs; kb++, it++) {
+                    if (!mbar_wait(smem_u32(pfull), (unsigned)(it & 1), status, 113)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+                    for (int blk = 0; blk < S; blk++) {
+                        const unsigned a0 = smem_u32(pa + kSelA[SEL][blk] * FS_PLANE);
+                        const unsigned b0 = smem_u32(pb + kSelB[SEL][blk] * FS_PLANE);
+                        const unsigned acc = (ACC2 && blk) ? acc_corr : acc_main;
+                        const bool first = ACC2 ? (kb == 0 && blk <= 1) : (kb == 0 && blk == 0);
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                            mma<KIND_BF16>(acc, smem_desc(a0 + 32 * k), smem_desc(b0 + 32 * k), idesc,
+                                           !(first && k == 0));
+                    }
+                    mma_commit(smem_u32(pempty));       // planes free once these MMAs finish
+                }
+                if (!ok) {
+                    *abort_flag = 1;
+                    break;
+                }
+                mma_commit(smem_u32(&tfull[ab]));      // accumulator ab complete
+            }
+        }
+    } else if (warp < 6) {
+        // ----------------------------------------------------------- epilogue
+        const int quarter = warp & 3;
+        const int r = quarter * 32 + lane;             // row of the tile this lane stores
+        int lt = 0;
+        for (long long t = blockIdx.x; t < ntiles; t += G, lt++) {
+            const FsTile ti = tiles[t];                // loaded while the accumulator fills
+            const int ab = lt & 1;
+            const bool ok = mbar_wait(smem_u32(&tfull[ab]), (unsigned)((lt >> 1) & 1), status, 114);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            float* crow = ti.c + (long long)r * ti.n;
+            const bool do_store = ok && !*abort_flag && r < ti.rows;
+            const unsigned tbase = tmem + ((unsigned)(quarter * 32) << 16) + (unsigned)ab * BUF_COLS;
+#pragma unroll 1
+            for (int c0 = 0; c0 < FS_BN; c0 += 32) {
+                unsigned r0[32];
+                tmem_ld32_nowait(tbase + (unsigned)c0, r0);              // warp-wide, always executed
+                float v[32];
+                if (ACC2) {
+                    unsigned q0[32];
+                    tmem_ld32_nowait(tbase + (unsigned)(FS_BN + c0), q0);
+                    tmem_wait();
+#pragma unroll
+                    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r0[i]) + __uint_as_float(q0[i]);
+                } else {
+                    tmem_wait();
+#pragma unroll
+                    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r0[i]);
+                }
+                if (!do_store || c0 >= ti.cols) continue;
+                if (ti.vec_ok && c0 + 32 <= ti.cols) {
+                    float4* p = reinterpret_cast<float4*>(crow + c0);
+#pragma unroll
+                    for (int q = 0; q < 8; q++) p[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 32; i++)
+                        if (c0 + i < ti.cols) crow[c0 + i] = v[i];
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&tempty[ab]));
+            if (!ok || *abort_flag) break;
+        }
+    } else {
+        // --------------------------------------------------------- converters
+        const int cw = warp - 6;                    // 0 .. FS_CONV-1
+        const int ct = threadIdx.x - 6 * 32;        // 0 .. FS_CT-1
+        long long it = 0;
+        bool ok = true;
+        int kbs_next = blockIdx.x < ntiles ? tiles[blockIdx.x].kblocks : 0;
+        for (long long t = blockIdx.x; t < ntiles && ok && !*abort_flag; t += G) {
+            const int kbs = kbs_next;
+            if (t + G < ntiles) kbs_next = tiles[t + G].kblocks;
+            for (int kb = 0; kb < kbs; kb++, it++) {
+                const int s = (int)(it % FS_NF);
+                ok = mbar_wait(smem_u32(&ffull[s]), (unsigned)((it / FS_NF) & 1), status, 116);
+                if (ok && it > 0) ok = mbar_wait(smem_u32(pempty), (unsigned)((it - 1) & 1), status, 117);
+                if (!ok) break;
+                fs_convert<P>(fa + s * FS_A_F32, fb + s * FS_B_F32, pa, pb, cw, lane, ct);
+                // the tensor core reads the planes through the async proxy
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(smem_u32(&fempty[s]));
+                    mbar_arrive(smem_u32(pfull));
+                }
+            }
+        }
+        if (!ok && lane == 0) *abort_flag = 1;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
 }  // namespace tc
 
 // ---------------------------------------------------------------- host side
@@ -972,6 +1335,11 @@ void preload_gemm_kernels()
     cudaFuncGetAttributes(&a, split_cols_bf16<6>);
     cudaFuncGetAttributes(&a, pad_rows_f32);
     cudaFuncGetAttributes(&a, transpose_pad_f32);
+    cudaFuncGetAttributes(&a, fs_tiles);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_split<1, false>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_split<3, false>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_split<3, true>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_split<6, true>);
 }
 
 int launch_wait_selftest(chai_cuda_ctx* ctx, double limit_ms)
@@ -1108,6 +1476,130 @@ namespace chai {
 // its first tile.  A tile that overhangs a problem's M or N reads rows of the
 // next problem (or TMA zero fill past the end): they only reach accumulator
 // rows / columns that the epilogue does not store.
+// In-kernel split (chai_gemm_fused_split): the operands' tensor maps need
+// 16-byte aligned bases and row pitches (K and N multiples of 4).
+static bool fused_split_ok(const chai_gemm_problem* p, int32_t count)
+{
+    for (int i = 0; i < count; i++) {
+        const chai_gemm_problem& q = p[i];
+        if ((reinterpret_cast<uintptr_t>(q.a) & 15) || (reinterpret_cast<uintptr_t>(q.b) & 15) || (q.k & 3) ||
+            (q.n & 3))
+            return false;
+    }
+    return true;
+}
+
+// 2-D f32 map of a row-major (rows x cols) array, box 32 x by, SWIZZLE_128B,
+// encoded by the driver; cached per context by (address, sizes, box).
+static int f32_map(chai_cuda_ctx* ctx, const void* base, long long cols, long long rows, int by,
+                   chai_cuda_ctx::RawMap* out)
+{
+    const chai_cuda_ctx::MapKey key{base, cols, rows, by};
+    auto it = ctx->map_cache.find(key);
+    if (it != ctx->map_cache.end()) {
+        *out = it->second;
+        return CHAI_OK;
+    }
+    PFN_encodeTiled enc = encode_fn(ctx);
+    if (!enc) return CHAI_ERR_NO_DEVICE;
+    CUtensorMap m;
+    memset(&m, 0, sizeof m);
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * 4};
+    cuuint32_t box[2] = {32, (cuuint32_t)by};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(ctx, CHAI_ERR_INVALID, "cuTensorMapEncodeTiled failed (grouped operand)");
+    static_assert(sizeof(CUtensorMap) == sizeof(chai_cuda_ctx::RawMap), "tensor map size");
+    memcpy(out->bytes, &m, sizeof m);
+    if (ctx->map_cache.size() >= (1u << 16)) ctx->map_cache.clear();
+    ctx->map_cache.emplace(key, *out);
+    return CHAI_OK;
+}
+
+// The tile records and tensor maps of a grouped call live in a per-context
+// buffer and are rebuilt only when the problem array (pointers, sizes) or the
+// precision changes; a repeated call launches the GEMM directly.
+static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_problem* p, int32_t count)
+{
+    using namespace tc;
+    chai_cuda_ctx::GroupedPlan& gp = ctx->gplan;
+    cudaStream_t s = ctx->stream;
+    const bool same = gp.dev && gp.S == S && gp.problems.size() == (size_t)count &&
+                      memcmp(gp.problems.data(), p, sizeof(chai_gemm_problem) * count) == 0;
+    if (!same) {
+        std::vector<FusedEntry> g(count);
+        std::vector<chai_cuda_ctx::RawMap> maps(2 * (size_t)count);
+        long long tiles = 0, kmax = 0;
+        for (int i = 0; i < count; i++) {
+            const chai_gemm_problem& q = p[i];
+            FusedEntry& e = g[i];
+            e.tile_start = tiles;
+            e.a = q.a;
+            e.b = q.b;
+            e.c = q.c;
+            e.m = q.m;
+            e.n = q.n;
+            e.k = q.k;
+            e.tiles_n = (q.n + FS_BN - 1) / FS_BN;
+            e.kblocks = (q.k + FS_KB - 1) / FS_KB;
+            e.vec_ok = ((reinterpret_cast<uintptr_t>(q.c) & 15) == 0 && q.n % 4 == 0) ? 1 : 0;
+            tiles += (long long)((q.m + BM - 1) / BM) * e.tiles_n;
+            kmax = std::max<long long>(kmax, (long long)e.kblocks * FS_KB);
+            int st = f32_map(ctx, q.a, q.k, q.m, BM, &maps[2 * i]);           // A: k x m, box 32 x 128
+            if (!st) st = f32_map(ctx, q.b, q.n, q.k, FS_KB, &maps[2 * i + 1]);  // B: n x k, box 32 x 64
+            if (st) return st;
+        }
+        if (tiles >= (1ll << 31)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "grouped gemm: too large");
+        const size_t t_bytes = ((size_t)tiles * sizeof(FsTile) + 255) & ~size_t(255);
+        const size_t need = t_bytes + maps.size() * sizeof(chai_cuda_ctx::RawMap);
+        if (gp.bytes < need) {
+            if (gp.dev) CHAI_CUDA_TRY(ctx, cudaFreeAsync(gp.dev, s));
+            gp.dev = nullptr;
+            gp.bytes = 0;
+            CHAI_CUDA_TRY(ctx, cudaMallocAsync(&gp.dev, need + need / 4, s));
+            gp.bytes = need + need / 4;
+        }
+        int st = ensure_scratch(ctx, g.size() * sizeof(FusedEntry));
+        if (st) return st;
+        FusedEntry* dg = static_cast<FusedEntry*>(ctx->scratch);
+        CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(dg, g.data(), g.size() * sizeof(FusedEntry), cudaMemcpyHostToDevice, s));
+        CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(static_cast<char*>(gp.dev) + t_bytes, maps.data(),
+                                           maps.size() * sizeof(chai_cuda_ctx::RawMap), cudaMemcpyHostToDevice, s));
+        fs_tiles<<<(unsigned)count, 128, 0, s>>>(dg, static_cast<FsTile*>(gp.dev));
+        CHAI_CUDA_TRY(ctx, cudaGetLastError());
+        gp.problems.assign(p, p + count);
+        gp.S = S;
+        gp.tiles = tiles;
+        gp.map_off = (long long)t_bytes;
+        // the same accumulator rule as the prepass path (see launch_gemm_grouped)
+        gp.acc2 = S == 6 || kmax > 2048;
+    }
+    const FsTile* dt = static_cast<const FsTile*>(gp.dev);
+    const unsigned char* dm = static_cast<const unsigned char*>(gp.dev) + gp.map_off;
+    const long long tiles = gp.tiles;
+    const unsigned grid = (unsigned)std::min<long long>(tiles, ctx->sm_count);
+    cudaEvent_t ev[2];
+    ktime_begin(ctx, "gemm_grouped", ev);
+#define CHAI_FS(SS, A2)                                                                              \
+    do {                                                                                             \
+        auto k = chai_gemm_fused_split<SS, A2>;                                                      \
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, fs_smem_bytes(SS));    \
+        k<<<grid, FS_THREADS, fs_smem_bytes(SS), s>>>(dt, tiles, dm, ctx->status_word);              \
+    } while (0)
+    if (S == 1) CHAI_FS(1, false);
+    else if (S == 3 && !gp.acc2) CHAI_FS(3, false);
+    else if (S == 3) CHAI_FS(3, true);
+    else CHAI_FS(6, true);
+#undef CHAI_FS
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    ktime_end(ctx, "gemm_grouped", ev);
+    ctx->fused_launches++;
+    return CHAI_OK;
+}
+
 int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_problem* p, int32_t count)
 {
     using namespace tc;
@@ -1122,6 +1614,12 @@ int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_p
     if (prec != CHAI_GEMM_BF16 && prec != CHAI_GEMM_BF16X3 && prec != CHAI_GEMM_BF16X6)
         return set_error(ctx, CHAI_ERR_UNSUPPORTED, "grouped gemm: bf16, bf16x3 or bf16x6");
     const int S = prec == CHAI_GEMM_BF16X3 ? 3 : prec == CHAI_GEMM_BF16X6 ? 6 : 1;
+    for (int i = 0; i < count; i++) {
+        const chai_gemm_problem& q = p[i];
+        if (q.m <= 0 || q.n <= 0 || q.k <= 0 || !q.a || !q.b || !q.c || q.m > 65535 || q.n > 65535)
+            return set_error(ctx, CHAI_ERR_INVALID, "grouped gemm: bad problem " + std::to_string(i));
+    }
+    if (ctx->cfg.grouped_fused && fused_split_ok(p, count)) return launch_grouped_fused(ctx, S, p, count);
     long long ra = 0, rb = 0, kmax = 0, tiles = 0, coltiles = 0;
     std::vector<GroupEntry> groups(count);
     std::vector<RowJob> rj(count);

@@ -342,7 +342,7 @@ int Translator::emit_group(const std::vector<int>& roots)
                 // fuses a packed mul.rn.f32x2 feeding a packed add / sub into a packed
                 // FMA (one rounding instead of two), which would change results;
                 // scalar mul.rn.f32 results feeding packed add / sub are not fused.
-                if (ar == 2 && nd.prec == CHAI_F32 && (nd.op == 11 || nd.op == 14) &&
+                if (ctx_->cfg.pack_f32 && ar == 2 && nd.prec == CHAI_F32 && (nd.op == 11 || nd.op == 14) &&
                     nodes_[nd.kids[0]].prec == CHAI_F32 && nodes_[nd.kids[1]].prec == CHAI_F32) {
                     os << "    f2x4<" << nd.op << ">(v" << nd.kids[0] << ", v" << nd.kids[1] << ", v" << i << ");\n";
                     break;

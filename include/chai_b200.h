@@ -95,7 +95,9 @@ const char* chai_cuda_last_error(chai_cuda_ctx* ctx);
  * "plan_replay" reports in *launches the number of evaluations replayed from
  * the plan cache (config PlanCache=1, the default: a trace whose cells,
  * scalars, shapes and bindings repeat an earlier one re-issues its recorded
- * device operations on its own buffers without translating again). */
+ * device operations on its own buffers without translating again);
+ * "grouped_fused" the number of grouped GEMMs whose f32 operands were split
+ * inside the GEMM kernel (config GroupedSplit=fused, the default). */
 int chai_cuda_kernel_stats(chai_cuda_ctx* ctx, const char* name, double* total_ms, uint64_t* launches,
                            int reset);
 /* Run subsequent work on an external cudaStream_t (NULL = the context's own). */

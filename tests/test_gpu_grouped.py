@@ -56,3 +56,48 @@ def test_grouped_gemm_4096_problems_sample(chai_dev):
         c64 = oracle.gemm_f64(As[i], Bs[i])
         bound = np.abs(As[i]).astype(np.float64) @ np.abs(Bs[i]).astype(np.float64)
         assert np.max(np.abs(Cs[i] - c64) / bound) <= BOUND[L.GEMM_BF16X3], i
+
+
+def fused_count(dev):
+    """Grouped GEMMs of this context that split their operands in-kernel."""
+    ms, n = C.c_double(), C.c_uint64()
+    L.check(L.lib().chai_cuda_kernel_stats(dev.ctx, b"grouped_fused", C.byref(ms), C.byref(n), 0), dev.ctx)
+    return n.value
+
+
+@pytest.fixture(scope="module")
+def prepass_dev(chai_dev):
+    """A second context whose grouped GEMM writes the bf16 planes in a prepass."""
+    import chai_b200.api as ch
+    dev = ch.Device(config="GroupedSplit=prepass")
+    yield dev
+    dev.close()
+
+
+@pytest.mark.parametrize("prec", [L.GEMM_BF16, L.GEMM_BF16X3, L.GEMM_BF16X6])
+def test_in_kernel_split_equals_prepass_planes(chai_dev, prepass_dev, prec):
+    """The fused kernel splits f32 tiles in shared memory; the prepass path
+    writes the planes to HBM first.  Both issue the same planes, products and
+    accumulators per element, so C must be bit-identical (K tails of 8, 36,
+    100 elements; M and N past a tile edge)."""
+    shapes = problems(40, seed=5) + [(8, 8, 8), (136, 260, 100), (129, 132, 36), (300, 4, 2056), (68, 44, 20),
+                                     (3, 128, 4)]
+    before = fused_count(chai_dev)
+    _, _, fused = run_grouped(chai_dev, shapes, prec, seed=3)
+    assert fused_count(chai_dev) == before + 1          # the in-kernel split ran
+    _, _, pre = run_grouped(prepass_dev, shapes, prec, seed=3)
+    assert fused_count(prepass_dev) == 0
+    for i, (a, b) in enumerate(zip(fused, pre)):
+        assert np.array_equal(a, b), (i, shapes[i])
+
+
+def test_unaligned_group_falls_back_to_prepass(chai_dev):
+    """K = 42 rows of A cannot be read in 16-byte loads: the whole group takes
+    the prepass path and stays within the bf16x3 bound."""
+    shapes = [(64, 40, 42), (96, 64, 72)]
+    before = fused_count(chai_dev)
+    As, Bs, Cs = run_grouped(chai_dev, shapes, L.GEMM_BF16X3)
+    assert fused_count(chai_dev) == before
+    for a, b, c in zip(As, Bs, Cs):
+        bound = np.abs(a).astype(np.float64) @ np.abs(b).astype(np.float64)
+        assert np.max(np.abs(c - oracle.gemm_f64(a, b)) / bound) <= BOUND[L.GEMM_BF16X3]
