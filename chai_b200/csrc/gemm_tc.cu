@@ -885,34 +885,40 @@ __global__ void __launch_bounds__(256) grouped_split_cols(const ColJob* __restri
 //
 // The grouped problems are small (K of a few hundred), so the prepass's
 // round trip of the bf16 planes through HBM costs more than the MMAs.  This
-// kernel reads the f32 operands once and splits them in shared memory:
-//   host        driver-encoded tensor maps of each problem's A and B (cached
-//               per context), uploaded with one record per output tile
-//               (fs_tiles)
-//   warp 0      producer: TMA-loads each 64-element K chunk of A (2 boxes of
-//               128 rows x 32 f32) and B (4 boxes of 64 k x 32 f32,
-//               SWIZZLE_128B) through the tile's problem maps into one of two
-//               f32 stages; the maps zero-fill past M, N and K
+// kernel reads the f32 operands once and splits them on the way into shared
+// memory:
+//   host        a driver-encoded tensor map of each problem's B (cached per
+//               context), uploaded with one record per output tile (fs_tiles)
+//   warp 0      producer: TMA-loads each 64-element K chunk of B (4 boxes of
+//               64 k x 32 f32, SWIZZLE_128B, zero fill past N and K) into one
+//               of two f32 stages
 //   warp 1      TMEM owner; one thread issues the S product blocks of each
 //               chunk (4 x tcgen05.mma, M = N = 128, K = 16 each)
 //   warps 2-5   epilogue (TMEM lane quarter = warp % 4)
-//   warps 6-13  converters: f32 stage -> the P distinct bf16 planes of A and
-//               B (K-major, SWIZZLE_128B rows of 64 bf16)
-// The MMA sequence (planes, order, accumulators) is the one the prepass path
-// issues, so both paths give bit-identical C.
+//   warps 6-13  converters: A rows straight from global memory (16-byte
+//               loads into registers, one chunk ahead) and the B stage ->
+//               the P distinct bf16 planes of A and B (K-major, SWIZZLE_128B
+//               rows of 64 bf16) in one of two plane buffers, so a chunk is
+//               converted while the MMAs of the previous one run
+// Shared memory carries only B's f32 stage, the planes and the tensor core's
+// operand reads.  The MMA sequence (planes, order, accumulators) is the one
+// the prepass path issues, so both paths give bit-identical C.
 constexpr int FS_BN = 128;
 constexpr int FS_KB = 64;                      // K elements per chunk
-constexpr int FS_NF = 2;                       // f32 stages
+constexpr int FS_NF = 2;                       // B f32 stages
 constexpr int FS_CONV = 8;                     // converter warps
 constexpr int FS_CT = FS_CONV * 32;            // converter threads
 constexpr int FS_THREADS = (6 + FS_CONV) * 32;
-constexpr int FS_A_F32 = BM * FS_KB * 4;       // 32 KiB: 2 boxes [128 rows][32 f32]
 constexpr int FS_B_F32 = FS_KB * FS_BN * 4;    // 32 KiB: 4 boxes [64 k][32 f32]
 constexpr int FS_PLANE = BM * 128;             // 16 KiB: 128 rows x 64 bf16 (A and B planes alike)
 
+// plane buffers: two (convert one chunk while the MMAs read the other), one
+// for bf16x6 whose three planes per operand leave no room for a second
+__host__ __device__ constexpr int fs_pbufs(int S) { return S == 6 ? 1 : 2; }
+
 __host__ __device__ constexpr int fs_smem_bytes(int S)
 {
-    return FS_NF * (FS_A_F32 + FS_B_F32) + 2 * distinct_planes(S) * FS_PLANE + 1024 + 256;
+    return FS_NF * FS_B_F32 + fs_pbufs(S) * 2 * distinct_planes(S) * FS_PLANE + 1024 + 256;
 }
 
 struct FusedEntry {
@@ -926,10 +932,11 @@ struct FusedEntry {
 // Everything a role needs about one 128 x 128 output tile (one 64-byte
 // record per tile, written by fs_tiles before the GEMM).
 struct __align__(16) FsTile {
+    const float* a;         // A rows of the tile (row0), k = 0
     float* c;               // C(tile origin)
-    int prob;               // problem index: its tensor maps are at maps + 256 prob (A), + 128 (B)
-    int m, n, k;
-    int row0, col0;         // tile origin in C
+    int prob;               // problem index: the tensor map of its B is at maps + 128 prob
+    int n, k;
+    int col0;               // tile origin column in C
     int rows, cols;         // valid rows / columns of the tile (<= 128)
     int kblocks, vec_ok;
 };
@@ -941,12 +948,11 @@ __global__ void __launch_bounds__(128) fs_tiles(const FusedEntry* __restrict__ g
     for (int l = threadIdx.x; l < tiles; l += blockDim.x) {
         const int tm = l / g.tiles_n, tn = l - tm * g.tiles_n;
         FsTile t;
+        t.a = g.a + (long long)tm * BM * g.k;
         t.c = g.c + (long long)tm * BM * g.n + (long long)tn * FS_BN;
         t.prob = blockIdx.x;
-        t.m = g.m;
         t.n = g.n;
         t.k = g.k;
-        t.row0 = tm * BM;
         t.col0 = tn * FS_BN;
         t.rows = min(BM, g.m - tm * BM);
         t.cols = min(FS_BN, g.n - tn * FS_BN);
@@ -990,27 +996,44 @@ __device__ __forceinline__ unsigned sw128(int row, int chunk)
     return (unsigned)(row * 128 + ((chunk ^ (row & 7)) << 4));
 }
 
-// f32 stage -> planes.  A: converter warp cw takes rows 16 cw .. + 15; per
-// step, lanes 8q .. 8q + 7 read the eight 16-byte chunks of one row of one
-// 32-k box.  B: thread ct takes column n = ct % 128 and four runs of 8 k.
+// A chunk in registers: converter warp cw, step i holds row 16 cw + 2 i +
+// lane / 16, k = 4 (lane % 16) .. + 3 (16-byte loads, two rows per warp step)
+struct FsA {
+    float4 v[BM / FS_CONV / 2];
+};
+
+__device__ __forceinline__ void fs_load_a(FsA& r, const FsTile& ti, int kb, int cw, int lane)
+{
+    const int kv = min(FS_KB, ti.k - kb * FS_KB);
+    const int kq = lane & 15;
+    const bool kok = 4 * kq < kv;                  // K is a multiple of 4: a chunk of 4 is all in or all out
+    const float* ap = ti.a + (long long)kb * FS_KB + 4 * kq;
+#pragma unroll
+    for (int i = 0; i < BM / FS_CONV / 2; i++) {
+        const int row = cw * (BM / FS_CONV) + 2 * i + (lane >> 4);
+        r.v[i] = (kok && row < ti.rows) ? __ldcg(reinterpret_cast<const float4*>(ap + (long long)row * ti.k))
+                                        : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// registers (A) and the f32 stage (B) -> planes.  A: lanes 0-15 write one
+// 128-byte plane row, lanes 16-31 the next.  B: thread ct takes column
+// n = ct % 128 and four runs of 8 k, reading the SWIZZLE_128B stage.
 template <int P>
-__device__ __forceinline__ void fs_convert(const unsigned char* fa, const unsigned char* fb, unsigned char* pa,
+__device__ __forceinline__ void fs_convert(const FsA& ra, const unsigned char* fb, unsigned char* pa,
                                            unsigned char* pb, int cw, int lane, int ct)
 {
-    const int c = lane & 7;
+    const int kq = lane & 15;
 #pragma unroll
-    for (int h = 0; h < 2; h++)
+    for (int i = 0; i < BM / FS_CONV / 2; i++) {
+        const int row = cw * (BM / FS_CONV) + 2 * i + (lane >> 4);
+        unsigned h0[3], h1[3];
+        split_pair<P>(ra.v[i].x, ra.v[i].y, h0);
+        split_pair<P>(ra.v[i].z, ra.v[i].w, h1);
+        const unsigned off = sw128(row, kq >> 1) + (kq & 1) * 8;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int row = cw * 16 + 4 * q + (lane >> 3);
-            const float4 x = *reinterpret_cast<const float4*>(fa + h * (BM * 128) + sw128(row, c));
-            unsigned h0[3], h1[3];
-            split_pair<P>(x.x, x.y, h0);
-            split_pair<P>(x.z, x.w, h1);
-            const unsigned off = sw128(row, 4 * h + (c >> 1)) + (c & 1) * 8;
-#pragma unroll
-            for (int p = 0; p < P; p++) *reinterpret_cast<uint2*>(pa + p * FS_PLANE + off) = make_uint2(h0[p], h1[p]);
-        }
+        for (int p = 0; p < P; p++) *reinterpret_cast<uint2*>(pa + p * FS_PLANE + off) = make_uint2(h0[p], h1[p]);
+    }
     const int n = ct & (FS_BN - 1);
     const unsigned char* col = fb + (n >> 5) * (FS_KB * 128) + (n & 3) * 4;   // box of n, lane of its chunk
     const int nc = (n & 31) >> 2;                                           // 16-byte chunk of n in a box row
@@ -1042,22 +1065,22 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const 
 {
     constexpr int P = Planes<S>::P;
     constexpr int SEL = S == 1 ? 0 : (S == 3 ? 1 : 2);
+    constexpr int NPB = fs_pbufs(S);
+    constexpr int PBUF = 2 * P * FS_PLANE;                         // one plane buffer: A planes, then B planes
     constexpr unsigned BUF_COLS = ACC2 ? 2 * FS_BN : FS_BN;
     constexpr unsigned TMEM_COLS = 2 * BUF_COLS;                   // double-buffered accumulators
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char* fa = smem;                                      // f32 A stages
-    unsigned char* fb = fa + FS_NF * FS_A_F32;                     // f32 B stages
-    unsigned char* pa = fb + FS_NF * FS_B_F32;                     // A planes p = 0..P-1
-    unsigned char* pb = pa + P * FS_PLANE;                         // B planes
-    unsigned long long* bars = reinterpret_cast<unsigned long long*>(pb + P * FS_PLANE);
-    unsigned long long* ffull = bars;                              // [FS_NF] TMA landed
-    unsigned long long* fempty = bars + FS_NF;                     // [FS_NF] stage read (per converter warp)
-    unsigned long long* pfull = bars + 2 * FS_NF;                  // planes written (per converter warp)
-    unsigned long long* pempty = bars + 2 * FS_NF + 1;             // planes consumed (tcgen05.commit)
-    unsigned long long* tfull = bars + 2 * FS_NF + 2;              // [2]
-    unsigned long long* tempty = bars + 2 * FS_NF + 4;             // [2]
-    unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * FS_NF + 6);
+    unsigned char* fb = smem;                                      // B f32 stages
+    unsigned char* planes = fb + FS_NF * FS_B_F32;                 // NPB plane buffers
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(planes + NPB * PBUF);
+    unsigned long long* ffull = bars;                              // [FS_NF] B stage landed
+    unsigned long long* fempty = bars + FS_NF;                     // [FS_NF] B stage read (per converter warp)
+    unsigned long long* pfull = bars + 2 * FS_NF;                  // [2] planes written (per converter warp)
+    unsigned long long* pempty = bars + 2 * FS_NF + 2;             // [2] planes consumed (tcgen05.commit)
+    unsigned long long* tfull = bars + 2 * FS_NF + 4;              // [2]
+    unsigned long long* tempty = bars + 2 * FS_NF + 6;             // [2]
+    unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * FS_NF + 8);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1067,11 +1090,11 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const 
             mbar_init(smem_u32(&ffull[s]), 1);
             mbar_init(smem_u32(&fempty[s]), FS_CONV);
         }
-        mbar_init(smem_u32(pfull), FS_CONV);
-        mbar_init(smem_u32(pempty), 1);
-        for (int a = 0; a < 2; a++) {
-            mbar_init(smem_u32(&tfull[a]), 1);
-            mbar_init(smem_u32(&tempty[a]), 4);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&pfull[b]), FS_CONV);
+            mbar_init(smem_u32(&pempty[b]), 1);
+            mbar_init(smem_u32(&tfull[b]), 1);
+            mbar_init(smem_u32(&tempty[b]), 4);
         }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -1093,9 +1116,7 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const 
             bool ok = true;
             for (long long t = blockIdx.x; t < ntiles && ok && !*abort_flag; t += G) {
                 const FsTile ti = tiles[t];
-                const unsigned char* ga = maps + (size_t)ti.prob * 256;
-                const unsigned char* gb = ga + 128;
-                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(ga) : "memory");
+                const unsigned char* gb = maps + (size_t)ti.prob * 128;
                 asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(gb) : "memory");
                 for (int kb = 0; kb < ti.kblocks; kb++, it++) {
                     const int s = (int)(it % FS_NF);
@@ -1105,9 +1126,7 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const 
                         break;
                     }
                     const unsigned bar = smem_u32(&ffull[s]);
-                    mbar_expect_tx(bar, FS_A_F32 + FS_B_F32);
-                    for (int h = 0; h < 2; h++)
-                        tma_load_2d(smem_u32(fa + s * FS_A_F32 + h * (BM * 128)), ga, bar, kb * FS_KB + 32 * h, ti.row0);
+                    mbar_expect_tx(bar, FS_B_F32);
                     for (int j = 0; j < 4; j++)
                         tma_load_2d(smem_u32(fb + s * FS_B_F32 + j * (FS_KB * 128)), gb, bar, ti.col0 + 32 * j,
                                     kb * FS_KB);
@@ -1139,11 +1158,14 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const 
                 const unsigned acc_corr = acc_main + (ACC2 ? FS_BN : 0);
                 bool ok = true;
                 for (int kb = 0; kb < kbs; kb++, it++) {
-                    if (!mbar_wait(smem_u32(pfull), (unsigned)(it & 1), status, 113)) {
+                    const int q = (int)(it % NPB);
+                    if (!mbar_wait(smem_u32(&pfull[q]), (unsigned)((it / NPB) & 1), status, 113)) {
                         ok = false;
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const unsigned char* pa = planes + q * PBUF;
+                    const unsigned char* pb = pa + P * FS_PLANE;
 #pragma unroll
                     for (int blk = 0; blk < S; blk++) {
                         const unsigned a0 = smem_u32(pa + kSelA[SEL][blk] * FS_PLANE);
@@ -1155,7 +1177,7 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const 
                             mma<KIND_BF16>(acc, smem_desc(a0 + 32 * k), smem_desc(b0 + 32 * k), idesc,
                                            !(first && k == 0));
                     }
-                    mma_commit(smem_u32(pempty));       // planes free once these MMAs finish
+                    mma_commit(smem_u32(&pempty[q]));  // buffer q free once these MMAs finish
                 }
                 if (!ok) {
                     *abort_flag = 1;
@@ -1213,25 +1235,48 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const 
         // --------------------------------------------------------- converters
         const int cw = warp - 6;                    // 0 .. FS_CONV-1
         const int ct = threadIdx.x - 6 * 32;        // 0 .. FS_CT-1
-        long long it = 0;
+        // A load cursor (tile lt_, chunk lkb), one chunk ahead of the chunk
+        // being converted; the record of the following tile is loaded one
+        // tile ahead
+        long long lt_ = blockIdx.x;
+        int lkb = 0;
+        FsTile lti, lnext;
+        if (lt_ < ntiles) lti = tiles[lt_];
+        if (lt_ + G < ntiles) lnext = tiles[lt_ + G];
+        auto advance = [&]() {
+            if (++lkb < lti.kblocks) return;
+            lkb = 0;
+            lt_ += G;
+            lti = lnext;
+            if (lt_ + G < ntiles) lnext = tiles[lt_ + G];
+        };
+        FsA ra;
+        bool have = lt_ < ntiles;                   // chunk `it` of A is in the registers
+        if (have) {
+            fs_load_a(ra, lti, 0, cw, lane);
+            advance();
+        }
         bool ok = true;
-        int kbs_next = blockIdx.x < ntiles ? tiles[blockIdx.x].kblocks : 0;
-        for (long long t = blockIdx.x; t < ntiles && ok && !*abort_flag; t += G) {
-            const int kbs = kbs_next;
-            if (t + G < ntiles) kbs_next = tiles[t + G].kblocks;
-            for (int kb = 0; kb < kbs; kb++, it++) {
-                const int s = (int)(it % FS_NF);
-                ok = mbar_wait(smem_u32(&ffull[s]), (unsigned)((it / FS_NF) & 1), status, 116);
-                if (ok && it > 0) ok = mbar_wait(smem_u32(pempty), (unsigned)((it - 1) & 1), status, 117);
-                if (!ok) break;
-                fs_convert<P>(fa + s * FS_A_F32, fb + s * FS_B_F32, pa, pb, cw, lane, ct);
-                // the tensor core reads the planes through the async proxy
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                __syncwarp();
-                if (lane == 0) {
-                    mbar_arrive(smem_u32(&fempty[s]));
-                    mbar_arrive(smem_u32(pfull));
-                }
+        for (long long it = 0; have && !*abort_flag; it++) {
+            const int s = (int)(it % FS_NF), q = (int)(it % NPB);
+            ok = mbar_wait(smem_u32(&ffull[s]), (unsigned)((it / FS_NF) & 1), status, 116);
+            // plane buffer q was last read by the MMAs of chunk it - NPB
+            if (ok && it >= NPB) ok = mbar_wait(smem_u32(&pempty[q]), (unsigned)((it / NPB - 1) & 1), status, 117);
+            if (!ok) break;
+            unsigned char* pa = planes + q * PBUF;
+            fs_convert<P>(ra, fb + s * FS_B_F32, pa, pa + P * FS_PLANE, cw, lane, ct);
+            // the tensor core reads the planes through the async proxy
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(smem_u32(&fempty[s]));
+                mbar_arrive(smem_u32(&pfull[q]));
+            }
+            // next chunk of A into the registers while the MMAs run
+            have = lt_ < ntiles;
+            if (have) {
+                fs_load_a(ra, lti, lkb, cw, lane);
+                advance();
             }
         }
         if (!ok && lane == 0) *abort_flag = 1;
@@ -1476,8 +1521,8 @@ namespace chai {
 // its first tile.  A tile that overhangs a problem's M or N reads rows of the
 // next problem (or TMA zero fill past the end): they only reach accumulator
 // rows / columns that the epilogue does not store.
-// In-kernel split (chai_gemm_fused_split): the operands' tensor maps need
-// 16-byte aligned bases and row pitches (K and N multiples of 4).
+// In-kernel split (chai_gemm_fused_split): A rows are read in 16-byte loads
+// and B through a tensor map: 16-byte aligned bases, K and N multiples of 4.
 static bool fused_split_ok(const chai_gemm_problem* p, int32_t count)
 {
     for (int i = 0; i < count; i++) {
@@ -1531,7 +1576,7 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
                       memcmp(gp.problems.data(), p, sizeof(chai_gemm_problem) * count) == 0;
     if (!same) {
         std::vector<FusedEntry> g(count);
-        std::vector<chai_cuda_ctx::RawMap> maps(2 * (size_t)count);
+        std::vector<chai_cuda_ctx::RawMap> maps((size_t)count);
         long long tiles = 0, kmax = 0;
         for (int i = 0; i < count; i++) {
             const chai_gemm_problem& q = p[i];
@@ -1548,8 +1593,7 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
             e.vec_ok = ((reinterpret_cast<uintptr_t>(q.c) & 15) == 0 && q.n % 4 == 0) ? 1 : 0;
             tiles += (long long)((q.m + BM - 1) / BM) * e.tiles_n;
             kmax = std::max<long long>(kmax, (long long)e.kblocks * FS_KB);
-            int st = f32_map(ctx, q.a, q.k, q.m, BM, &maps[2 * i]);           // A: k x m, box 32 x 128
-            if (!st) st = f32_map(ctx, q.b, q.n, q.k, FS_KB, &maps[2 * i + 1]);  // B: n x k, box 32 x 64
+            const int st = f32_map(ctx, q.b, q.n, q.k, FS_KB, &maps[i]);         // B: n x k, box 32 x 64
             if (st) return st;
         }
         if (tiles >= (1ll << 31)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "grouped gemm: too large");
