@@ -906,7 +906,8 @@ __global__ void __launch_bounds__(256) grouped_split_cols(const ColJob* __restri
 constexpr int FS_BN = 128;
 constexpr int FS_KB = 64;                      // K elements per chunk
 constexpr int FS_NF = 2;                       // B f32 stages
-constexpr int FS_CONV = 8;                     // converter warps
+constexpr int FS_CONV = 16;                    // converter warps
+constexpr int FS_BRUNS = 8 * 128 / (FS_CONV * 32);   // B: runs of 8 k per converter thread
 constexpr int FS_CT = FS_CONV * 32;            // converter threads
 constexpr int FS_THREADS = (6 + FS_CONV) * 32;
 constexpr int FS_B_F32 = FS_KB * FS_BN * 4;    // 32 KiB: 4 boxes [64 k][32 f32]
@@ -1018,7 +1019,7 @@ __device__ __forceinline__ void fs_load_a(FsA& r, const FsTile& ti, int kb, int 
 
 // registers (A) and the f32 stage (B) -> planes.  A: lanes 0-15 write one
 // 128-byte plane row, lanes 16-31 the next.  B: thread ct takes column
-// n = ct % 128 and four runs of 8 k, reading the SWIZZLE_128B stage.
+// n = ct % 128 and FS_BRUNS runs of 8 k, reading the SWIZZLE_128B stage.
 template <int P>
 __device__ __forceinline__ void fs_convert(const FsA& ra, const unsigned char* fb, unsigned char* pa,
                                            unsigned char* pb, int cw, int lane, int ct)
@@ -1038,8 +1039,8 @@ __device__ __forceinline__ void fs_convert(const FsA& ra, const unsigned char* f
     const unsigned char* col = fb + (n >> 5) * (FS_KB * 128) + (n & 3) * 4;   // box of n, lane of its chunk
     const int nc = (n & 31) >> 2;                                           // 16-byte chunk of n in a box row
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-        const int kc = (ct >> 7) * 4 + u;
+    for (int u = 0; u < FS_BRUNS; u++) {
+        const int kc = (ct >> 7) * FS_BRUNS + u;
         unsigned h[3][4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
