@@ -930,7 +930,7 @@ struct FusedEntry {
     int m, n, k, tiles_n, kblocks, vec_ok;
 };
 
-// Everything a role needs about one 128 x 128 output tile (one 64-byte
+// Everything a role needs about one 128 x 128 output tile (one 48-byte
 // record per tile, written by fs_tiles before the GEMM).
 struct __align__(16) FsTile {
     const float* a;         // A rows of the tile (row0), k = 0
@@ -941,6 +941,8 @@ struct __align__(16) FsTile {
     int rows, cols;         // valid rows / columns of the tile (<= 128)
     int kblocks, vec_ok;
 };
+
+static_assert(sizeof(FsTile) == 48, "tile record size");
 
 __global__ void __launch_bounds__(128) fs_tiles(const FusedEntry* __restrict__ groups, FsTile* __restrict__ out)
 {
