@@ -4,7 +4,7 @@
 
 Workloads (synthetic, seeded; shapes from the reference's benchmark configs):
   gemm    square f32 GEMM through the trace path's GEMM entry point
-          (chai_cuda_gemm), M = N = K = 8192 by default, split-precision bf16x3
+          (chai_cuda_gemm), M = N = K = 16384 by default, split-precision bf16x3
           on tcgen05 (--precision to change), the GEMM/GEMV precision sweep case
   mc      Monte Carlo trace: 2^27 Philox4x32-10 Box-Muller normals,
           S = 100 exp(0.03 + 0.2 Z), payoff = mean(max(S - 100, 0)), fully
@@ -12,6 +12,11 @@ Workloads (synthetic, seeded; shapes from the reference's benchmark configs):
   kirsch  8-direction Kirsch compass filter through gather2_floor over an
           8192 x 8192 f32 image (HBM-bound element trace)
   gemv    y = A x, 8192 x 8192 f32 (HBM-bound)
+  mc-hbm  the materialised Monte Carlo payoff over 2^27 normals in HBM
+  mc-many 64 Monte Carlo traces of uneven lengths in one persistent launch
+  grouped 4096 grouped f32 GEMMs (M, N, K multiples of 8 in [32, 512])
+  tuner   learned vs exhaustive GEMM/GEMV tuning on held-out shapes
+  c1      512^3 matmul + sum(C*C) as one traced program (latency-bound)
 
 `value` is device-resident throughput (inputs already in HBM, CUDA events on
 the context stream, max over ranks); `e2e` is the same metric through the
@@ -371,6 +376,90 @@ def run_mc(args, L, ctx, stream):
         "e2e": {"value": n / (e_ms * 1e-3) / 1e9, "unit": "Gnormals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 16},
         "roofline": None, "clocks": clk.summary(), "gpu_launches": args.steps * 2,
+    }
+
+
+C1_N = 512
+
+
+def c1_expr(ch, g, n=C1_N):
+    """The C1 trace: A, B uniform[-1, 1) from one chai Philox generator (seed 0,
+    the second fill continues the first's counters), C = matmul(A, B),
+    s = sum(C * C)."""
+    a = ch.Arrayf32(ch.rng_uniform_make(g, n, n, 1, -1.0, 1.0))
+    b = ch.Arrayf32(ch.rng_uniform_make(g, n, n, 1, -1.0, 1.0))
+    c = ch.Arrayf32(ch.matmul(a, b))
+    return ch.sum(c * c)
+
+
+def count_launches(step):
+    """Kernels one call of `step` launches (torch profiler, outside any timed
+    region); None where the profiler cannot see CUDA activity."""
+    import torch
+    try:
+        from torch.profiler import ProfilerActivity, profile
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            step()
+            torch.cuda.synchronize()
+        return sum(1 for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA
+                   and "memcpy" not in e.name.lower() and "memset" not in e.name.lower())
+    except Exception:
+        return None
+
+
+def run_c1(args, L, ctx, stream):
+    """C1: 512^3 matmul + sum(C * C) as one traced program (latency-bound at
+    this size: the line reports microseconds per evaluation beside TFLOP/s)."""
+    import torch
+    import chai_b200.api as ch
+    n = C1_N
+    dev = ch.vm()
+    flops = 2.0 * n ** 3 + 2.0 * n * n
+    stmts, s_arr = record(ch, lambda: ch.Arrayf32(c1_expr(ch, ch.RNGf32(ch.RNG_PHILOX, 0))))
+    bid = 77201
+    desc, keep = ch.build_desc(stmts)
+    barr = (L.chai_buffer_binding * 1)(L.chai_buffer_binding(s_arr.var, 4, 1, 1, 1, 0, bid))
+
+    def step():
+        L.check(L.lib().chai_cuda_evaluate(dev.ctx, C.byref(desc), barr, 1), dev.ctx)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    with Clocks(torch.cuda.current_device()) as clk:
+        ts = time_events(step, args.steps, stream)
+    ms = sum(ts) / len(ts)
+    per_step = count_launches(step)
+    # e2e: A and B from pinned host memory through make2 every evaluation,
+    # the scalar read back
+    rng = np.random.default_rng(0)
+    Ah = torch.from_numpy(rng.uniform(-1, 1, (n, n)).astype(np.float32)).pin_memory().numpy()
+    Bh = torch.from_numpy(rng.uniform(-1, 1, (n, n)).astype(np.float32)).pin_memory().numpy()
+
+    def e2e():
+        c = ch.Arrayf32(ch.matmul(ch.make2(Ah), ch.make2(Bh)))
+        return float(ch.Arrayf32(ch.sum(c * c)).read_scalar())
+
+    for _ in range(3):
+        e2e()
+    torch.cuda.synchronize()
+    reps = max(5, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        sv = e2e()
+    e_ms = (time.perf_counter() - t0) * 1e3 / reps
+    return {
+        "metric": "C1 trace TFLOP/s (512^3 matmul + sum(C*C))", "unit": "TFLOP/s",
+        "value": flops / (ms * 1e-3) / 1e12, "ms_per_step": ms, "dtype": "f32", "higher_is_better": True,
+        "config": {"workload": "C1: A, B = chai Philox uniform[-1,1) 512x512 (seed 0), C = matmul(A, B), "
+                               "s = sum(C*C), one traced evaluation (plan replay)",
+                   "us_per_evaluation": ms * 1e3, "e2e_us_per_evaluation": e_ms * 1e3, "s_e2e": sv,
+                   "gemm_precision": "context default", "l2": "inputs generated in the trace (no HBM inputs)"},
+        "e2e": {"value": flops / (e_ms * 1e-3) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": 2 * n * n * 4,
+                "d2h_bytes_per_step": 4},
+        "roofline": None, "clocks": clk.summary(),
+        "gpu_launches": (per_step * args.steps) if per_step is not None else args.steps * 6,
     }
 
 
@@ -775,7 +864,7 @@ def run_tuner(args, L, ctx, stream):
 
 
 WORKLOADS = {"gemm": run_gemm, "mc": run_mc, "mc-hbm": run_mc_hbm, "kirsch": run_kirsch, "gemv": run_gemv,
-             "mc-many": run_mc_many, "grouped": run_grouped, "tuner": run_tuner}
+             "mc-many": run_mc_many, "grouped": run_grouped, "tuner": run_tuner, "c1": run_c1}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -790,6 +879,9 @@ def workload_desc(args):
                 % (n, args.precision)), args.precision
     if wl == "mc":
         return "Monte Carlo trace, 2^27 Philox4x32-10 Box-Muller normals, fused", "f32"
+    if wl == "c1":
+        return ("C1: A, B = chai Philox uniform[-1,1) 512x512 (seed 0), C = matmul(A, B), s = sum(C*C), one traced "
+                "evaluation (plan replay)"), "f32"
     if wl == "mc-hbm":
         return "Monte Carlo payoff over 2^27 f32 normals already in HBM (materialised Z), fused", "f32"
     if wl == "kirsch":
@@ -833,6 +925,14 @@ def run_reference(args, steps=None):
             unit, metric = "TFLOP/s", "GEMM TFLOP/s at err vs FP32"
             conv = lambda ms: 2.0 * n ** 3 / (ms * 1e-3) / 1e12
             sample = "interpreter matmul 512^3 f32 (f32 products summed in double), inputs via make2"
+        elif wl == "c1":
+            n = C1_N
+            rng.uniform(-1, 1, (n, n)).astype(np.float32).tofile(td + "/A")
+            rng.uniform(-1, 1, (n, n)).astype(np.float32).tofile(td + "/B")
+            cmd = [str(drv), "matmul_sum", str(n), td + "/A", td + "/B", td + "/C", td + "/s"]
+            unit, metric = "TFLOP/s", "C1 trace TFLOP/s (512^3 matmul + sum(C*C))"
+            conv = lambda ms: (2.0 * n ** 3 + 2.0 * n * n) / (ms * 1e-3) / 1e12
+            sample = "the whole C1 trace in the interpreter (make2 inputs, matmul 512^3, sum(C*C), read-back)"
         elif wl == "grouped":
             cmd = None
             unit, metric = "TFLOP/s", "GEMM TFLOP/s at err vs FP32"

@@ -113,10 +113,23 @@ int launch_gemm_simt(chai_cuda_ctx* ctx, const chai_gemm_desc* d)
             (const double*)d->a, (const double*)d->b, (double*)d->c, d->m, d->n, d->k, d->lda, d->ldb, d->ldc,
             d->alpha, d->beta, d->stride_a, d->stride_b, d->stride_c);
     } else {
-        dim3 grid((unsigned)((d->n + 127) / 128), (unsigned)((d->m + 127) / 128), (unsigned)batch);
-        chai_gemm_simt<float, 128, 128, 8, 8, 8><<<grid, 256, 0, ctx->stream>>>(
-            (const float*)d->a, (const float*)d->b, (float*)d->c, d->m, d->n, d->k, d->lda, d->ldb, d->ldc,
-            (float)d->alpha, (float)d->beta, d->stride_a, d->stride_b, d->stride_c);
+        // Small products (C1's 512 x 512 gives 16 tiles of 128 x 128) leave most
+        // SMs idle: take 64 x 64, then 32 x 64 tiles until the grid covers the
+        // SMs; their K step is 32 wide, so a short K loop waits on fewer
+        // rounds of global loads.  Every variant runs each output's FMA chain in the same k order,
+        // so the results are bit-identical whichever tile is chosen.
+        auto tiles = [&](long long bm, long long bn) { return ((d->m + bm - 1) / bm) * ((d->n + bn - 1) / bn) * batch; };
+#define CHAI_SIMT(BMV, BNV, BKV, TMV, TNV)                                                                  \
+        do {                                                                                                \
+            dim3 grid((unsigned)((d->n + BNV - 1) / BNV), (unsigned)((d->m + BMV - 1) / BMV), (unsigned)batch); \
+            chai_gemm_simt<float, BMV, BNV, BKV, TMV, TNV><<<grid, (BMV / TMV) * (BNV / TNV), 0, ctx->stream>>>( \
+                (const float*)d->a, (const float*)d->b, (float*)d->c, d->m, d->n, d->k, d->lda, d->ldb, d->ldc,  \
+                (float)d->alpha, (float)d->beta, d->stride_a, d->stride_b, d->stride_c);                     \
+        } while (0)
+        if (tiles(128, 128) >= ctx->sm_count) CHAI_SIMT(128, 128, 8, 8, 8);
+        else if (tiles(64, 64) >= ctx->sm_count) CHAI_SIMT(64, 64, 32, 4, 4);
+        else CHAI_SIMT(32, 64, 32, 4, 4);                  // 128 threads, 4 x 4 outputs each
+#undef CHAI_SIMT
     }
     CHAI_CUDA_TRY(ctx, cudaGetLastError());
     return CHAI_OK;

@@ -150,3 +150,20 @@ def test_gemv_bulk_copy_path(chai_dev, dtype, shape):
     bound = 0.5 * (np.abs(A).astype(np.float64) @ np.abs(x).astype(np.float64)) + 2.0 * np.abs(y0)
     err = np.max(np.abs(y.cpu().numpy().astype(np.float64) - want) / bound)
     assert err <= (2.0 ** -20 if dtype == np.float32 else 2.0 ** -45), err
+
+
+@pytest.mark.parametrize("shape", [(512, 512, 512), (256, 264, 40), (1024, 512, 96)])
+def test_fp32_gemm_tile_choice_is_bit_identical(chai_dev, shape):
+    """The FP32 CUDA-core GEMM picks 128x128, 64x64 or 32x64 tiles by how many
+    tiles cover the SMs; each output's FMA chain runs in the same k order in
+    every variant, so a small product (few tiles, small-tile kernel) equals
+    the same product as entry 0 of a 10-problem batch (enough tiles for the
+    128x128 kernel) bit for bit."""
+    M, N, K = shape
+    rng = np.random.default_rng(M + N + K)
+    A = rng.uniform(-1, 1, (M, K)).astype(np.float32)
+    B = rng.uniform(-1, 1, (K, N)).astype(np.float32)
+    one = run_gemm(chai_dev, A, B, L.GEMM_FP32)
+    many = run_gemm(chai_dev, np.repeat(A[None], 10, 0), np.repeat(B[None], 10, 0), L.GEMM_FP32)
+    assert np.array_equal(one, many[0]) and np.array_equal(many[0], many[9])
+    assert norm_err(one, A, B) <= BOUND[L.GEMM_FP32]

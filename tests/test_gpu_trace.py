@@ -325,3 +325,24 @@ def test_stencil_with_reduction(ch):
     s = float(ch.Arrayf64(ch.sum(ch.convert_f64(ch.gather2_floor(A, X + f32(1), Y) - A))).read_scalar())
     want = (np.roll(img, -1, axis=1).astype(np.float32) - img).astype(np.float64).sum()
     assert abs(s - want) <= 1e-9 * max(1.0, np.abs(img).sum())
+
+
+def test_c1_trace_with_generated_inputs(ch):
+    """C1 as the bench runs it: A and B filled inside the trace by one chai
+    Philox generator (seed 0; the second fill starts 512*512 counters later),
+    C = matmul(A, B), s = sum(C * C).  The inputs are bit-exact against the
+    oracle's fills; s within 1e-4 relative of the FP64 product's (bf16x3
+    products: normalised element error <= 2^-14)."""
+    import bench
+    n = bench.C1_N
+    g = ch.RNGf32(ch.RNG_PHILOX, 0)
+    a = ch.Arrayf32(ch.rng_uniform_make(g, n, n, 1, -1.0, 1.0))
+    b = ch.Arrayf32(ch.rng_uniform_make(g, n, n, 1, -1.0, 1.0))
+    c = ch.Arrayf32(ch.matmul(a, b))
+    s = ch.Arrayf32(ch.sum(c * c))
+    A = oracle.rng_fill(n * n, seed=0, limits=(-1.0, 1.0)).reshape(n, n)
+    B = oracle.rng_fill(n * n, seed=n * n, limits=(-1.0, 1.0)).reshape(n, n)
+    assert np.array_equal(a.read2(), A) and np.array_equal(b.read2(), B)
+    C64 = A.astype(np.float64) @ B.astype(np.float64)
+    s64 = float((C64 ** 2).sum())
+    assert abs(float(s.read_scalar()) - s64) <= 1e-4 * s64
