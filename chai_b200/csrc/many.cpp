@@ -7,7 +7,8 @@
 // (api/chai.h:551-600).  Here traces that share one program -- the same cells
 // except for scalar values (W, H, seeds, literals) -- are compiled once, with
 // the per-trace scalars read from a device table, and run as ONE kernel over a
-// global list of 8192-element tiles:
+// global list of 4096-element tiles (256 threads x 4 chunks of 4; small
+// enough that the last of ~15 tiles per CTA leaves little of the grid idle):
 //   tab[0] = number of tiles, tab[1] = number of traces, then per trace:
 //   { n, W, H, first tile, seed of each RNG node, bits of each varying scalar }.
 // Every CTA walks tiles blockIdx.x, +gridDim.x, ...; a tile finds its trace
@@ -39,6 +40,9 @@
 #include "trace.h"
 
 namespace chai {
+
+constexpr int kManySubs = 4;                       // chunks of 4 elements per thread and tile
+constexpr long long kManyTile = 256 * 4 * kManySubs;
 
 int launch_many_combine(chai_cuda_ctx* ctx, const long long* tab, int stride, const double* partials, double* out,
                         int ntr, int mean, int prec);
@@ -76,6 +80,8 @@ std::map<std::pair<uint64_t, size_t>, ManyGraph>& graphs(chai_cuda_ctx* ctx)
 }  // namespace
 
 // Free the graphs and buffers of a context (chai_cuda_shutdown).
+void clear_last_batch(chai_cuda_ctx* ctx);
+
 void many_release(chai_cuda_ctx* ctx)
 {
     auto& m = graphs(ctx);
@@ -89,6 +95,7 @@ void many_release(chai_cuda_ctx* ctx)
         if (g.partials) cudaFree(g.partials);
     }
     m.clear();
+    clear_last_batch(ctx);
 }
 
 // Program description shared by all traces (built from trace 0).
@@ -99,6 +106,57 @@ struct ManyProgram {
     std::vector<int> var_scalars;   // table column 4 + nrng + k
     int red_op = 132, red_prec = CHAI_F32;
 };
+
+// The last persistent batch of a context: its traces' statements and cells
+// (scalars included) byte for byte, and what parsing them produced.  A call
+// whose batch repeats it skips parsing, program generation and the table
+// build, and goes straight to the captured graph.
+struct ManyLast {
+    bool valid = false;
+    std::string content;
+    ManyProgram prog;
+    std::vector<long long> tab;
+    void* fn = nullptr;
+    uint64_t key = 0;
+};
+
+ManyLast& last_batch(chai_cuda_ctx* ctx)
+{
+    static std::map<chai_cuda_ctx*, ManyLast> all;
+    return all[ctx];
+}
+
+void clear_last_batch(chai_cuda_ctx* ctx) { last_batch(ctx) = ManyLast(); }
+
+// Statements and cells of a batch as bytes; false for batches with inline
+// kernels (their program text is not part of the statements).
+bool batch_content(const chai_trace_desc* const* traces, size_t n, std::string& out)
+{
+    out.clear();
+    auto put = [&](const void* p, size_t b) { out.append(static_cast<const char*>(p), b); };
+    for (size_t t = 0; t < n; t++) {
+        const chai_trace_desc* d = traces[t];
+        if (!d || d->n_kernels || (d->n_stmts && !d->stmts)) return false;
+        put(&d->num_traces, 4);
+        put(&d->n_stmts, 4);
+        for (uint32_t i = 0; i < d->n_stmts; i++) {
+            const chai_stmt& st = d->stmts[i];
+            if (st.n_cells && !st.cells) return false;
+            put(&st.lhs_variable, 4);
+            put(&st.lhs_version, 4);
+            put(&st.n_cells, 4);
+            for (uint32_t c = 0; c < st.n_cells; c++) {
+                const chai_bc& b = st.cells[c];
+                put(&b.kind, 4);
+                put(&b.code, 4);
+                put(&b.version, 4);
+                put(&b.scalar, 8);
+                put(&b.buffer, 8);
+            }
+        }
+    }
+    return true;
+}
 
 static bool same_structure(const std::vector<Node>& a, const std::vector<Node>& b)
 {
@@ -178,8 +236,8 @@ static bool build_program(const std::vector<std::vector<Node>>& all, int root, d
        << "    const long long* tp = rows + (long long)lo * " << p.stride << ";\n"
        << "    const long long n = tp[0], W = tp[1];\n"
        << "    double red[1] = {0};\n"
-       << "    for (int sub = 0; sub < 8; sub++) {\n"
-       << "    const long long c = ((tile - tp[3]) * 8 + sub) * 256 + threadIdx.x;\n"
+       << "    for (int sub = 0; sub < " << kManySubs << "; sub++) {\n"
+       << "    const long long c = ((tile - tp[3]) * " << kManySubs << " + sub) * 256 + threadIdx.x;\n"
        << "    if (c * 4 >= n) break;\n"
        << "    const long long e0 = c * 4;\n"
        << "    long long xx[4], yy[4]; { const long long y0 = e0 / W, x0 = e0 - y0 * W; "
@@ -297,6 +355,8 @@ static bool build_program(const std::vector<std::vector<Node>>& all, int root, d
 
 using namespace chai;
 
+static int launch_batch(chai_cuda_ctx* ctx, ManyLast& b, size_t n_traces, double* results);
+
 extern "C" int chai_cuda_evaluate_many(chai_cuda_ctx* ctx, const chai_trace_desc* const* traces, size_t n_traces,
                                        double* results)
 {
@@ -304,6 +364,12 @@ extern "C" int chai_cuda_evaluate_many(chai_cuda_ctx* ctx, const chai_trace_desc
     if (n_traces == 0) return CHAI_OK;
     if (fault_injected("evaluate")) return set_error(ctx, CHAI_ERR_INJECTED, "injected evaluate failure");
     cudaSetDevice(ctx->device);
+    std::string content;
+    const bool cacheable = batch_content(traces, n_traces, content);
+    ManyLast& last = last_batch(ctx);
+    if (cacheable && last.valid && last.content == content)
+        return launch_batch(ctx, last, n_traces, results);
+    last.valid = false;
     // parse every trace (dry: no storage, no launches) to compare structures
     std::vector<std::vector<Node>> all;
     all.reserve(n_traces);
@@ -335,8 +401,6 @@ extern "C" int chai_cuda_evaluate_many(chai_cuda_ctx* ctx, const chai_trace_desc
     void* fn = nullptr;
     int st = ctx->jit->get(prog.source, "chai_many", &fn);
     if (st) return st;
-    const uint64_t key = fnv1a64(prog.source.data(), prog.source.size());
-    ManyGraph& g = graphs(ctx)[std::make_pair(key, n_traces)];
     // per-trace table
     const int it = all[0][root].kids[0];
     std::vector<long long> tab(2 + n_traces * prog.stride);
@@ -348,7 +412,7 @@ extern "C" int chai_cuda_evaluate_many(chai_cuda_ctx* ctx, const chai_trace_desc
         row[1] = (long long)r.W;
         row[2] = (long long)r.H;
         row[3] = tiles;
-        tiles += (row[0] + 8191) / 8192;      // 8192-element tiles: 256 threads x 8 chunks of 4
+        tiles += (row[0] + kManyTile - 1) / kManyTile;
         for (size_t k = 0; k < prog.rng_nodes.size(); k++) {
             const Node& rn = all[t][prog.rng_nodes[k]];
             row[4 + k] = (long long)(rn.prec == CHAI_F64 ? rn.seed : (uint32_t)rn.seed);
@@ -358,6 +422,24 @@ extern "C" int chai_cuda_evaluate_many(chai_cuda_ctx* ctx, const chai_trace_desc
     }
     tab[0] = tiles;
     tab[1] = (long long)n_traces;
+    last.content.swap(content);
+    last.prog = prog;
+    last.tab.swap(tab);
+    last.fn = fn;
+    last.key = fnv1a64(prog.source.data(), prog.source.size());
+    last.valid = cacheable;
+    return launch_batch(ctx, last, n_traces, results);
+}
+
+// Run a parsed batch: upload its table through the (program, trace count)
+// graph, capturing the graph first when there is none or it is too small.
+static int launch_batch(chai_cuda_ctx* ctx, ManyLast& b, size_t n_traces, double* results)
+{
+    const ManyProgram& prog = b.prog;
+    void* fn = b.fn;
+    const std::vector<long long>& tab = b.tab;
+    const long long tiles = tab[0];
+    ManyGraph& g = graphs(ctx)[std::make_pair(b.key, n_traces)];
     const size_t words = tab.size();
     if (!g.exec || g.cap_tiles < tiles || g.tab_words != words) {
         // (re)build the buffers and the graph

@@ -57,3 +57,19 @@ def test_many_falls_back_for_other_programs(chai_dev):
     traces = [ch.record(lambda s=s: ch.Arrayf32(ch.sum(ch.make1(x * s))))[0] for s in (1, 2)]
     r = ch.evaluate_many(traces)
     assert np.allclose(r, [x.sum(), 2 * x.sum()])
+
+
+def test_repeated_batch_reuses_parse_but_sees_changed_scalars(chai_dev):
+    """A batch identical to the previous call's is launched without parsing
+    again; a batch that differs only in one trace's seed is parsed again and
+    that trace's result follows the new seed."""
+    import chai_b200.api as ch
+    Ls = [4096, 65536, 12288]
+    a = [ch.record(lambda L=L, s=s: mc(ch, 300 + s, L))[0] for s, L in enumerate(Ls)]
+    b = [ch.record(lambda L=L, s=s: mc(ch, (900 if s == 1 else 300 + s), L))[0] for s, L in enumerate(Ls)]
+    ra = ch.evaluate_many(a)
+    assert np.array_equal(ch.evaluate_many(a), ra)
+    rb = ch.evaluate_many(b)
+    assert rb[0] == ra[0] and rb[2] == ra[2] and rb[1] != ra[1]
+    assert close(rb[1], float(mc(ch, 900, 65536).read_scalar()))
+    assert np.array_equal(ch.evaluate_many(a), ra)
