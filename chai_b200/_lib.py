@@ -109,6 +109,7 @@ SIGNATURES = {
                                           C.POINTER(C.c_double)]),
     "chai_cuda_rng_fill": (C.c_int, [P, C.POINTER(chai_rng_desc), P]),
     "chai_cuda_gemm": (C.c_int, [P, C.POINTER(chai_gemm_desc)]),
+    "chai_cuda_gemm_host": (C.c_int, [P, C.POINTER(chai_gemm_desc), C.c_int64]),
     "chai_cuda_gemv": (C.c_int, [P, C.c_uint32, C.c_int, C.c_int64, C.c_int64, C.c_double, P, C.c_int64, P,
                                  C.c_double, P]),
     "chai_cuda_gemm_grouped": (C.c_int, [P, C.c_int32, C.POINTER(chai_gemm_problem), C.c_int32]),

@@ -240,6 +240,7 @@ int chai_cuda_shutdown(chai_cuda_ctx* ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     many_release(ctx);
+    host_gemm_release(ctx);
     ctx->tuner.reset();
     ctx->jit.reset();
     for (auto& kv : ctx->kstats)

@@ -120,6 +120,7 @@ int launch_reduce(chai_cuda_ctx* ctx, uint32_t op, uint32_t prec, const void* a,
 int launch_gemv(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha,
                 const void* a, int64_t lda, const void* x, double beta, void* y);
 int launch_gemm(chai_cuda_ctx* ctx, const chai_gemm_desc* d);
+void host_gemm_release(chai_cuda_ctx* ctx);
 int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_problem* p, int32_t count);
 
 }  // namespace chai

@@ -255,6 +255,17 @@ typedef struct chai_gemm_desc {
 } chai_gemm_desc;
 int chai_cuda_gemm(chai_cuda_ctx* ctx, const chai_gemm_desc* d);
 
+/* The same GEMM with a, b and c in HOST memory (pinned memory copies fastest):
+ * the host-resident matmul operands and read-back of the reference's memory
+ * manager (memmgr/MemTransJIT.cpp:18-327) overlapped with the GEMM.  B is
+ * uploaded once; A goes up in blocks of `block_rows` rows (0: about an eighth
+ * of M, whole 128-row tiles) on a copy stream, each block's GEMM runs on the
+ * context stream as its rows land, and its rows of C come back on a second
+ * copy stream during the next block.  C is bit-identical to uploading the
+ * operands and calling chai_cuda_gemm.  One problem (batch <= 1), no
+ * transposes; returns when C is in host memory. */
+int chai_cuda_gemm_host(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int64_t block_rows);
+
 /* y = alpha * op(A) x + beta * y, f32 or f64 (autotune/EvergreenMatmulMV.cpp). */
 int chai_cuda_gemv(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha,
                    const void* a, int64_t lda, const void* x, double beta, void* y);
