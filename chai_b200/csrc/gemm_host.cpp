@@ -8,7 +8,8 @@
 // uploaded in blocks of rows on a copy stream, each block's GEMM runs on the
 // context stream as soon as its rows have landed, and each block of C goes
 // back on a second copy stream while the next block computes.  Two device
-// buffers per operand block alternate.  Every block is an ordinary
+// buffers per operand block alternate; for the tensor-core precisions B's
+// operand planes are written once and shared by the block GEMMs.  Every block is an ordinary
 // chai_cuda_gemm call on device buffers, and a row of C depends only on the
 // same row of A, so C is bit-identical to uploading everything first.
 #include <cuda_runtime.h>
@@ -16,6 +17,7 @@
 #include <algorithm>
 
 #include "internal.h"
+#include "tuner.h"
 
 namespace chai {
 
@@ -110,15 +112,18 @@ extern "C" int chai_cuda_gemm_host(chai_cuda_ctx* ctx, const chai_gemm_desc* d, 
     mb = std::max<long long>(128, (mb + 127) / 128 * 128);
     mb = std::min(mb, M);
     const size_t b_bytes = (size_t)K * N * es, a_blk = (size_t)mb * K * es, c_blk = (size_t)mb * N * es;
+    // tensor-core precisions: B is split into its operand planes once, not per block
+    const size_t p_bytes = gemm_b_planes_bytes(prec, K, N);
     auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
     HostGemm& h = host_gemms()[ctx];
     cudaSetDevice(ctx->device);
-    int st = host_gemm_setup(ctx, h, up(b_bytes) + 2 * up(a_blk) + 2 * up(c_blk));
+    int st = host_gemm_setup(ctx, h, up(b_bytes) + 2 * up(a_blk) + 2 * up(c_blk) + up(p_bytes));
     if (st) return st;
     char* base = static_cast<char*>(h.dev);
     char* db = base;
     char* da[2] = {base + up(b_bytes), base + up(b_bytes) + up(a_blk)};
     char* dc[2] = {da[1] + up(a_blk), da[1] + up(a_blk) + up(c_blk)};
+    char* bplanes = p_bytes ? dc[1] + up(c_blk) : nullptr;
     const bool with_c = d->beta != 0.0;
     // the copies must not start before earlier work on the context stream
     // that may still read these buffers
@@ -128,6 +133,10 @@ extern "C" int chai_cuda_gemm_host(chai_cuda_ctx* ctx, const chai_gemm_desc* d, 
     if (st) return st;
     CHAI_CUDA_TRY(ctx, cudaEventRecord(h.ev_b, h.in));
     CHAI_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, h.ev_b, 0));
+    if (bplanes) {
+        st = gemm_split_b(ctx, prec, reinterpret_cast<const float*>(db), N, K, N, bplanes);
+        if (st) return st;
+    }
     const char* ha = static_cast<const char*>(d->a);
     char* hc = static_cast<char*>(d->c);
     long long blk = 0;
@@ -158,7 +167,7 @@ extern "C" int chai_cuda_gemm_host(chai_cuda_ctx* ctx, const chai_gemm_desc* d, 
         bd.ldc = N;
         bd.batch = 1;
         bd.stride_a = bd.stride_b = bd.stride_c = 0;
-        st = launch_gemm(ctx, &bd);
+        st = bplanes ? launch_gemm_tc_cfg(ctx, &bd, prec, nullptr, bplanes) : launch_gemm(ctx, &bd);
         if (st) return st;
         CHAI_CUDA_TRY(ctx, cudaEventRecord(h.ev_comp[q], ctx->stream));
         CHAI_CUDA_TRY(ctx, cudaStreamWaitEvent(h.out, h.ev_comp[q], 0));

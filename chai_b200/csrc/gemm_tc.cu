@@ -1402,7 +1402,49 @@ int launch_gemm_tc(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision)
     return launch_gemm_tc_cfg(ctx, d, precision, nullptr);
 }
 
-int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision, const TcCfg* cfg_in)
+// Bytes of B's operand planes for a K x N B (N rows of the distinct planes
+// side by side along K, as the GEMM's prepass writes them); 0 for fp8, whose
+// planes come with per-call scales.
+size_t gemm_b_planes_bytes(int precision, long long k, long long n)
+{
+    using namespace tc;
+    if (precision == CHAI_GEMM_FP8 || precision == CHAI_GEMM_FP32 || precision == CHAI_GEMM_FP64) return 0;
+    const bool tf32 = precision == CHAI_GEMM_TF32;
+    const int S = precision == CHAI_GEMM_BF16X3 ? 3 : precision == CHAI_GEMM_BF16X6 ? 6 : 1;
+    const int kblk = tf32 ? 32 : 64;
+    const long long kpad = (k + kblk - 1) / kblk * kblk;
+    return (size_t)n * distinct_planes(S) * kpad * (tf32 ? 4 : 2);
+}
+
+// B's prepass alone, into `out` (gemm_b_planes_bytes bytes): lets a caller
+// that multiplies many row blocks of A by one B split B once and pass the
+// planes to launch_gemm_tc_cfg.
+int gemm_split_b(chai_cuda_ctx* ctx, int precision, const float* b, long long ldb, long long k, long long n, void* out)
+{
+    using namespace tc;
+    if (!gemm_b_planes_bytes(precision, k, n)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "gemm_split_b: precision");
+    const bool tf32 = precision == CHAI_GEMM_TF32;
+    const int S = precision == CHAI_GEMM_BF16X3 ? 3 : precision == CHAI_GEMM_BF16X6 ? 6 : 1;
+    const int kblk = tf32 ? 32 : 64;
+    const long long kpad = (k + kblk - 1) / kblk * kblk;
+    const long long kp = distinct_planes(S) * kpad;
+    cudaStream_t s = ctx->stream;
+    if (tf32) {
+        dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((kpad + 31) / 32), 1);
+        transpose_pad_f32<<<tgrid, dim3(32, 8), 0, s>>>(b, ldb, 0, (int)k, (int)n, (int)kpad, (float*)out, n * kp);
+    } else {
+        dim3 sgrid((unsigned)((n + 63) / 64), (unsigned)(kpad / 64), 1);
+        __nv_bfloat16* b2 = (__nv_bfloat16*)out;
+        if (S == 1) split_cols_bf16<1><<<sgrid, 256, 0, s>>>(b, ldb, 0, (int)k, (int)n, (int)kpad, b2, n * kp);
+        else if (S == 3) split_cols_bf16<3><<<sgrid, 256, 0, s>>>(b, ldb, 0, (int)k, (int)n, (int)kpad, b2, n * kp);
+        else split_cols_bf16<6><<<sgrid, 256, 0, s>>>(b, ldb, 0, (int)k, (int)n, (int)kpad, b2, n * kp);
+    }
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    return CHAI_OK;
+}
+
+int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision, const TcCfg* cfg_in,
+                       const void* b_planes)
 {
     using namespace tc;
     if (d->trans_a || d->trans_b) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: transposed operands");
@@ -1427,7 +1469,8 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     if (st) return st;
     char* base = static_cast<char*>(ctx->scratch);
     void* Ap = base;
-    void* Bp = base + b_off;
+    void* Bp = b_planes && !fp8 && batch == 1 ? const_cast<void*>(b_planes) : base + b_off;
+    const bool b_ready = Bp == b_planes;
     unsigned* amax_a = reinterpret_cast<unsigned*>(base + s_off);
     unsigned* amax_b = amax_a + batch * tiles_m128;
     const float* A = static_cast<const float*>(d->a);
@@ -1453,14 +1496,16 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
             scales_from_amax<<<(ns + 255) / 256, 256, 0, s>>>(amax_a, ns);
         } else if (tf32) {
             pad_rows_f32<<<rgrid, 256, 0, s>>>(A, d->lda, d->stride_a, (int)M, (int)K, (int)kpad, (float*)Ap, M * kp);
-            transpose_pad_f32<<<tgrid, dim3(32, 8), 0, s>>>(B, d->ldb, d->stride_b, (int)K, (int)N, (int)kpad,
-                                                            (float*)Bp, N * kp);
+            if (!b_ready)
+                transpose_pad_f32<<<tgrid, dim3(32, 8), 0, s>>>(B, d->ldb, d->stride_b, (int)K, (int)N, (int)kpad,
+                                                                (float*)Bp, N * kp);
         } else {
             __nv_bfloat16* a2 = (__nv_bfloat16*)Ap;
             __nv_bfloat16* b2 = (__nv_bfloat16*)Bp;
 #define SPLIT(SS)                                                                                                   \
     split_rows_bf16<SS><<<rgrid, 256, 0, s>>>(A, d->lda, d->stride_a, (int)M, (int)K, (int)kpad, a2, M * kp);    \
-    split_cols_bf16<SS><<<sgrid, 256, 0, s>>>(B, d->ldb, d->stride_b, (int)K, (int)N, (int)kpad, b2, N * kp)
+    if (!b_ready)                                                                                                   \
+        split_cols_bf16<SS><<<sgrid, 256, 0, s>>>(B, d->ldb, d->stride_b, (int)K, (int)N, (int)kpad, b2, N * kp)
             if (S == 1) { SPLIT(1); } else if (S == 3) { SPLIT(3); } else { SPLIT(6); }
 #undef SPLIT
         }

@@ -31,7 +31,12 @@ struct GemvCfg {
 };
 bool tuned_gemv_cfg(chai_cuda_ctx* ctx, long long m, long long n, int prec, GemvCfg* out);
 
-int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision, const TcCfg* cfg);
+// b_planes: B already split by gemm_split_b (one problem, not fp8), or null
+int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precision, const TcCfg* cfg,
+                       const void* b_planes = nullptr);
+size_t gemm_b_planes_bytes(int precision, long long k, long long n);
+int gemm_split_b(chai_cuda_ctx* ctx, int precision, const float* b, long long ldb, long long k, long long n,
+                 void* out);
 int launch_gemv_cfg(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha, const void* a,
                     int64_t lda, const void* x, double beta, void* y, const GemvCfg* cfg);
 

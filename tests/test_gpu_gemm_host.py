@@ -43,7 +43,7 @@ def host_gemm(dev, A, B, C0, prec, alpha, beta, block_rows, pad=0):
     return Ch[:, :N].numpy().copy()
 
 
-@pytest.mark.parametrize("prec", [L.GEMM_FP32, L.GEMM_BF16X3])
+@pytest.mark.parametrize("prec", [L.GEMM_FP32, L.GEMM_TF32, L.GEMM_BF16X3, L.GEMM_BF16X6])
 @pytest.mark.parametrize("shape,block_rows,pad,beta", [((1000, 384, 200), 256, 0, 0.0),
                                                          ((700, 260, 96), 128, 4, -2.0),
                                                          ((2048, 512, 512), 0, 0, 0.0),
