@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "internal.h"
 #include "tuner.h"
@@ -31,10 +33,13 @@ struct HostGemm {
     size_t bytes = 0;
 };
 
-std::map<chai_cuda_ctx*, HostGemm>& host_gemms()
+std::map<chai_cuda_ctx*, HostGemm> g_host_gemms;     // by context
+std::mutex g_host_gemms_mu;                          // guards finding / inserting / erasing an entry
+
+HostGemm& host_gemm_of(chai_cuda_ctx* ctx)
 {
-    static std::map<chai_cuda_ctx*, HostGemm> all;
-    return all;
+    std::lock_guard<std::mutex> g(g_host_gemms_mu);
+    return g_host_gemms[ctx];
 }
 
 int host_gemm_setup(chai_cuda_ctx* ctx, HostGemm& h, size_t need)
@@ -77,10 +82,14 @@ int copy_rows(chai_cuda_ctx* ctx, void* dst, size_t dpitch, const void* src, siz
 
 void host_gemm_release(chai_cuda_ctx* ctx)
 {
-    auto& all = host_gemms();
-    auto it = all.find(ctx);
-    if (it == all.end()) return;
-    HostGemm& h = it->second;
+    HostGemm h;
+    {
+        std::lock_guard<std::mutex> g(g_host_gemms_mu);
+        auto it = g_host_gemms.find(ctx);
+        if (it == g_host_gemms.end()) return;
+        h = it->second;
+        g_host_gemms.erase(it);
+    }
     if (h.in) cudaStreamSynchronize(h.in);
     if (h.out) cudaStreamSynchronize(h.out);
     if (h.dev) cudaFree(h.dev);
@@ -88,7 +97,6 @@ void host_gemm_release(chai_cuda_ctx* ctx)
         if (e) cudaEventDestroy(e);
     if (h.in) cudaStreamDestroy(h.in);
     if (h.out) cudaStreamDestroy(h.out);
-    all.erase(it);
 }
 
 }  // namespace chai
@@ -115,7 +123,7 @@ extern "C" int chai_cuda_gemm_host(chai_cuda_ctx* ctx, const chai_gemm_desc* d, 
     // tensor-core precisions: B is split into its operand planes once, not per block
     const size_t p_bytes = gemm_b_planes_bytes(prec, K, N);
     auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
-    HostGemm& h = host_gemms()[ctx];
+    HostGemm& h = host_gemm_of(ctx);
     cudaSetDevice(ctx->device);
     int st = host_gemm_setup(ctx, h, up(b_bytes) + 2 * up(a_blk) + 2 * up(c_blk) + up(p_bytes));
     if (st) return st;

@@ -31,6 +31,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <mutex>
 #include <set>
 #include <sstream>
 #include <vector>
@@ -71,9 +72,15 @@ struct ManyGraph {
     size_t tab_words = 0;
 };
 
+// Per-context state lives in maps keyed by the context; the lock covers
+// finding or inserting a context's entry (contexts may be driven from
+// different threads), after which only that context's thread touches it.
+std::mutex g_many_mu;
+
 std::map<std::pair<uint64_t, size_t>, ManyGraph>& graphs(chai_cuda_ctx* ctx)
 {
     static std::map<chai_cuda_ctx*, std::map<std::pair<uint64_t, size_t>, ManyGraph>> all;
+    std::lock_guard<std::mutex> g(g_many_mu);
     return all[ctx];
 }
 
@@ -123,6 +130,7 @@ struct ManyLast {
 ManyLast& last_batch(chai_cuda_ctx* ctx)
 {
     static std::map<chai_cuda_ctx*, ManyLast> all;
+    std::lock_guard<std::mutex> g(g_many_mu);
     return all[ctx];
 }
 
