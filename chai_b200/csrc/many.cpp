@@ -12,9 +12,10 @@
 //   tab[0] = number of tiles, tab[1] = number of traces, then per trace:
 //   { n, W, H, first tile, seed of each RNG node, bits of each varying scalar }.
 // Every CTA walks tiles blockIdx.x, +gridDim.x, ...; a tile finds its trace
-// by binary search on the first-tile column; its block partial goes to
-// partials[tile]; a second kernel adds each trace's partials in tile order in
-// FP64.  The H2D copy of the table, both kernels and the D2H copy of the
+// by binary search on the first-tile column; a CTA keeps its running sum over
+// consecutive tiles of one trace in registers and writes its block partial at
+// its last tile of that trace (0 for the others) to partials[tile]; a second
+// kernel adds each trace's partials in tile order in FP64.  The H2D copy of the table, both kernels and the D2H copy of the
 // results are captured once into a CUDA graph per (program, trace count) and
 // replayed afterwards.
 //
@@ -237,13 +238,16 @@ static bool build_program(const std::vector<std::vector<Node>>& all, int root, d
           "double* __restrict__ partials)\n{\n  using namespace chai_ops; using namespace chai_rng;\n"
        << "  const long long ntiles = tab[0]; const int ntr = (int)tab[1];\n"
        << "  const long long* rows = tab + 2;\n"
+       << "  double red[1] = {0};\n"
        << "  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
        << "    int lo = 0, hi = ntr - 1;\n"
        << "    while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (rows[(long long)mid * " << p.stride
        << " + 3] <= tile) lo = mid; else hi = mid - 1; }\n"
        << "    const long long* tp = rows + (long long)lo * " << p.stride << ";\n"
        << "    const long long n = tp[0], W = tp[1];\n"
-       << "    double red[1] = {0};\n"
+       << "    const long long next = tile + gridDim.x;\n"
+       << "    const bool flush = next >= ntiles || (lo + 1 < ntr && rows[(long long)(lo + 1) * " << p.stride
+       << " + 3] <= next);\n"
        << "    for (int sub = 0; sub < " << kManySubs << "; sub++) {\n"
        << "    const long long c = ((tile - tp[3]) * " << kManySubs << " + sub) * 256 + threadIdx.x;\n"
        << "    if (c * 4 >= n) break;\n"
@@ -351,9 +355,14 @@ static bool build_program(const std::vector<std::vector<Node>>& all, int root, d
                 return false;
         }
     }
+    // the CTA's running sum stays in registers over its tiles of one trace
+    // and is reduced at its last tile of that trace; its other tiles of the
+    // trace contribute 0 to the trace's partials (the combine adds all)
     os << "    for (int j = 0; j < 4; j++) red[0] += (double)v" << it << "[j];\n    }\n"
+       << "    if (!flush) { if (threadIdx.x == 0) partials[tile] = 0.0; continue; }\n"
        << "    chai_k::block_sum<1, 256>(red);\n"
        << "    if (threadIdx.x == 0) partials[tile] = red[0];\n"
+       << "    red[0] = 0;\n"
        << "    __syncthreads();\n  }\n}\n";
     p.source = os.str();
     return true;
@@ -470,7 +479,7 @@ static int launch_batch(chai_cuda_ctx* ctx, ManyLast& b, size_t n_traces, double
         cudaGraph_t graph;
         CHAI_CUDA_TRY(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         cudaMemcpyAsync(g.dev_tab, g.host_tab, words * sizeof(long long), cudaMemcpyHostToDevice, s);
-        const unsigned grid = (unsigned)(ctx->sm_count * 4);
+        const unsigned grid = (unsigned)(ctx->sm_count * 8);     // as the single-trace kernels
         void* args[2] = {&g.dev_tab, &g.partials};
         int lst = ctx->jit->launch(fn, dim3(grid), dim3(256), 0, args);
         int cst = launch_many_combine(ctx, g.dev_tab, prog.stride, g.partials, g.dev_res, (int)n_traces,
