@@ -86,3 +86,48 @@ def test_random_elementwise_traces_bit_exact(chai_dev, dt, shape):
         got, want = _run(ch, ops, ins, dt)
         assert got.dtype == dt and got.shape == (H, W)
         assert np.array_equal(got, want, equal_nan=True), (seed, ops)
+
+
+def _int_program(rng, nops=14):
+    ops = []
+    n = 3
+    choices = ["add", "sub", "mul", "xor", "and", "or", "shl", "shr", "max", "min", "gt"]
+    for _ in range(nops):
+        pick = lambda: int(n - 1 - min(rng.geometric(0.35) - 1, n - 1))
+        ops.append((choices[rng.integers(len(choices))], (pick(), pick())))
+        n += 1
+    return ops
+
+
+def _run_int(ops, ins, dt):
+    import chai_b200.api as api
+    ex = [api.make2(x) for x in ins]
+    nv = list(ins)
+    with np.errstate(all="ignore"):
+        for op, (i, j) in ops:
+            x, y, u, w = ex[i], ex[j], nv[i], nv[j]
+            s = (w & dt(31)).astype(dt)             # shift counts are taken modulo 32
+            e, r = {"add": (x + y, u + w), "sub": (x - y, u - w), "mul": (x * y, u * w), "xor": (x ^ y, u ^ w),
+                    "and": (x & y, u & w), "or": (x | y, u | w), "shl": (x << y, u << s), "shr": (x >> y, u >> s),
+                    "max": (api.max(x, y), np.where(u < w, w, u)), "min": (api.min(x, y), np.where(u < w, u, w)),
+                    "gt": (x > y, (u > w).astype(dt))}[op]
+            ex.append(e)
+            nv.append(np.asarray(r, dtype=dt))
+    arr = api.Arrayu32(ex[-1]) if dt == np.uint32 else api.Arrayi32(ex[-1])
+    return arr.read2(), nv[-1]
+
+
+@pytest.mark.parametrize("dt", [np.uint32, np.int32])
+def test_random_integer_traces_bit_exact(chai_dev, dt):
+    """u32 / i32 programs: add, sub, mul wrap modulo 2^32; shifts use the
+    count modulo 32 (arithmetic right shift for i32); max / min / greater-than
+    compare as the type does."""
+    H, W = 40, 52
+    info = np.iinfo(dt)
+    for seed in range(8):
+        rng = np.random.default_rng(77 + seed)
+        ins = [rng.integers(info.min, info.max, (H, W), dtype=dt, endpoint=True) for _ in range(3)]
+        ins[1][:, :4] = rng.integers(0, 40, (H, 4)).astype(dt)      # small shift counts too
+        ops = _int_program(rng)
+        got, want = _run_int(ops, ins, dt)
+        assert got.dtype == dt and np.array_equal(got, want), (seed, ops)
