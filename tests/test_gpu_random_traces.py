@@ -131,3 +131,33 @@ def test_random_integer_traces_bit_exact(chai_dev, dt):
         ops = _int_program(rng)
         got, want = _run_int(ops, ins, dt)
         assert got.dtype == dt and np.array_equal(got, want), (seed, ops)
+
+
+@pytest.mark.parametrize("shape", [(70, 200), (33, 129), (300, 1024), (8, 12)])
+def test_random_stencil_traces_bit_exact(chai_dev, shape):
+    """Random constant-offset stencils: sums, differences and products of
+    gather2_floor(A, X + dx, Y + dy) with |dx|, |dy| <= 4 (the 2-D tiled path:
+    TMA-staged interior tiles, wrapped border tiles, shared row windows),
+    against numpy's periodic roll with the same per-operation rounding."""
+    import chai_b200.api as ch
+    f32 = np.float32
+    H, W = shape
+    for seed in range(5):
+        rng = np.random.default_rng(500 + 7 * seed + W)
+        img = rng.standard_normal((H, W)).astype(f32)
+        A = ch.make2(img)
+        X, Y = ch.index_f32(0, W, H), ch.index_f32(1, W, H)
+        roll = lambda dx, dy: np.roll(np.roll(img, -dy, axis=0), -dx, axis=1)
+        e, r = None, None
+        for _ in range(int(rng.integers(3, 9))):
+            dx, dy = (int(v) for v in rng.integers(-4, 5, 2))
+            g = ch.gather2_floor(A, X + f32(dx), Y + f32(dy))
+            gv = roll(dx, dy)
+            k = f32(rng.choice([1.0, 2.0, -0.5, 3.0]))
+            if e is None:
+                e, r = g * k, gv * k
+                continue
+            op = int(rng.integers(3))
+            e, r = [(e + g * k, r + gv * k), (e - g, r - gv), (e * g, r * gv)][op]
+        got = ch.Arrayf32(e).read2()
+        assert np.array_equal(got, r), (seed, shape)
