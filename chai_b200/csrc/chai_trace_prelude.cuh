@@ -148,6 +148,16 @@ __device__ __forceinline__ long long wrapi(long long v, long long n)
     return v < 0 ? v + n : v;
 }
 
+// wrapi for the coordinates a stencil tile reaches (at most one period
+// outside [0, n)) without a division; farther values (images narrower than
+// a tile and its halo) take the general path
+__device__ __forceinline__ long long wrapn(long long v, long long n)
+{
+    if (v < 0) v += n;
+    else if (v >= n) v -= n;
+    return (v >= 0 && v < n) ? v : wrapi(v, n);
+}
+
 }  // namespace chai_k
 
 #endif

@@ -130,7 +130,7 @@ int ensure_scratch(chai_cuda_ctx* ctx, size_t bytes)
     return CHAI_OK;
 }
 
-static void parse_config(chai::Config& c, const char* text)
+void parse_config(chai::Config& c, const char* text)
 {
     if (!text) return;
     std::istringstream is(text);

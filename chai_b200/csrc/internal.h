@@ -37,6 +37,9 @@ struct Config {
     std::string jit_cache;
 };
 
+// "Key=value" tokens of an init configuration string into `c` (context.cu)
+void parse_config(Config& c, const char* text);
+
 class Jit;      // runtime compilation cache (jit.cpp)
 class Tuner;    // learned / exhaustive GEMM tuner (tuner.cpp)
 struct Plan;    // recorded device operations of a trace (plan.h)

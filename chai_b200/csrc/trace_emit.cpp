@@ -104,6 +104,8 @@ int Translator::emit_group(const std::vector<int>& roots)
     // body nodes in dependency order; loads for values computed elsewhere
     std::vector<int> body;
     std::set<int> loads, seen;
+    struct Sten { int src, cx, cy; };
+    std::map<int, Sten> sten;
     std::function<void(int)> dfs = [&](int i) {
         if (seen.count(i)) return;
         seen.insert(i);
@@ -116,7 +118,10 @@ int Translator::emit_group(const std::vector<int>& roots)
             return;
         }
         if (nd.kind == Node::GATHER) {
-            for (size_t k = 1; k < nd.kids.size(); k++) dfs(nd.kids[k]);
+            // a stencil gather reads its staged window: its index expressions
+            // are not evaluated
+            if (!sten.count(i))
+                for (size_t k = 1; k < nd.kids.size(); k++) dfs(nd.kids[k]);
         } else {
             for (int k : nd.kids) dfs(k);
         }
@@ -131,8 +136,6 @@ int Translator::emit_group(const std::vector<int>& roots)
     // gather of the group is one, the group runs as 2-D tiles of TX x TY outputs
     // whose source tile plus halo is staged in shared memory: by one TMA load for
     // interior tiles, by wrapped (periodic) loads for border tiles.
-    struct Sten { int src, cx, cy; };
-    std::map<int, Sten> sten;
     std::vector<int> srcs;
     int R = 0;
     bool mode2d = W >= 16 && H >= 4 && W < (1u << 24) && H < (1u << 24) && S <= 65535;
@@ -181,6 +184,12 @@ int Translator::emit_group(const std::vector<int>& roots)
     for (int src : srcs) tile_bytes += (size_t)(ST_TY + 2 * R) * (ST_TX + 2 * ST_PX) * prec_bytes(nodes_[src].prec);
     mode2d = mode2d && any_gather && srcs.size() <= 2 && tile_bytes <= 46 * 1024;
     if (!mode2d) sten.clear();
+    if (mode2d) {
+        body.clear();
+        loads.clear();
+        seen.clear();
+        for (int r : roots) dfs(r);
+    }
     const int SH = ST_TY + 2 * R, SW = ST_TX + 2 * ST_PX;
     std::map<std::pair<int, int>, int> win_lo, win_hi;   // (source tile, row offset) -> column range
     std::set<std::pair<int, int>> win_done;
@@ -281,7 +290,7 @@ int Translator::emit_group(const std::vector<int>& roots)
                 if (kv.second.src == srcs[k]) { gsrc = kv.first; break; }
             os << "      for (int idx = threadIdx.x; idx < " << SH * SW << "; idx += 256) { const int r = idx / " << SW
                << ", c = idx - r * " << SW << "; tile" << k << "[idx] = g" << gsrc << "[(long long)(slot % "
-               << a.slots << ") * " << sl << " + chai_k::wrapi(ty0 - " << R << " + r, H) * W + chai_k::wrapi(tx0 - "
+               << a.slots << ") * " << sl << " + chai_k::wrapn(ty0 - " << R << " + r, H) * W + chai_k::wrapn(tx0 - "
                << ST_PX << " + c, W)]; }\n";
         }
         os << "    }\n    __syncthreads();\n  }\n";
@@ -342,7 +351,10 @@ int Translator::emit_group(const std::vector<int>& roots)
                 // fuses a packed mul.rn.f32x2 feeding a packed add / sub into a packed
                 // FMA (one rounding instead of two), which would change results;
                 // scalar mul.rn.f32 results feeding packed add / sub are not fused.
-                if (ctx_->cfg.pack_f32 && ar == 2 && nd.prec == CHAI_F32 && (nd.op == 11 || nd.op == 14) &&
+                // Flat kernels only: a stencil's operands come from windows shifted
+                // by the gather's column offset, whose pairs straddle register
+                // pairs, and the moves that re-pair them cost what packing saves.
+                if (ctx_->cfg.pack_f32 && !mode2d && ar == 2 && nd.prec == CHAI_F32 && (nd.op == 11 || nd.op == 14) &&
                     nodes_[nd.kids[0]].prec == CHAI_F32 && nodes_[nd.kids[1]].prec == CHAI_F32) {
                     os << "    f2x4<" << nd.op << ">(v" << nd.kids[0] << ", v" << nd.kids[1] << ", v" << i << ");\n";
                     break;
@@ -820,13 +832,7 @@ extern "C" int chai_cuda_trace_source(const chai_trace_desc* t, const chai_buffe
     static thread_local std::string last_err;
     chai_cuda_ctx ctx;
     ctx.device = -1;
-    if (config) {
-        // reuse the context parser through a throwaway init-free path
-        std::string c(config);
-        if (c.find("RngLayout=counter") != std::string::npos) ctx.cfg.rng_layout = 1;
-        size_t p = c.find("RngPi=");
-        if (p != std::string::npos) ctx.cfg.rng_pi = atof(c.c_str() + p + 6);
-    }
+    parse_config(ctx.cfg, config);
     ctx.jit.reset(new Jit(&ctx));
     ctx.jit->set_compile_only(true);
     Translator tr(&ctx, true);

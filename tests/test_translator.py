@@ -22,14 +22,15 @@ def record(build):
     return stmts, keep
 
 
-def source(stmts, binds=()):
+def source(stmts, binds=(), config=None):
     desc, keep = ch.build_desc(stmts)
     b = (L.chai_buffer_binding * max(1, len(binds)))()
     for i, x in enumerate(binds):
         b[i] = L.chai_buffer_binding(*x)
     buf = C.create_string_buffer(1 << 21)
     need = C.c_size_t()
-    st = L.lib().chai_cuda_trace_source(C.byref(desc), b, len(binds), None, buf, len(buf), C.byref(need))
+    st = L.lib().chai_cuda_trace_source(C.byref(desc), b, len(binds), config.encode() if config else None, buf,
+                                        len(buf), C.byref(need))
     return st, buf.value.decode()
 
 
@@ -76,9 +77,23 @@ def test_kirsch_trace_is_one_kernel_with_gathers():
     # the 8 gathers read 3 row windows (row offsets -1, 0, +1), each one
     # 16-byte shared load plus two edge elements
     assert src.count("const float* rowp = tile0") == 3 and src.count("chai_k::lds_vec(rowp") == 3
-    # f32 add / sub run as packed f32x2 pairs; multiplies stay scalar (a packed
-    # multiply feeding a packed add would be contracted into one rounding)
-    assert src.count("f2x4<11>") >= 20 and src.count("f2x4<14>") >= 8 and src.count("f2x4<13>") == 0
+    # the index arithmetic under the stencil gathers is not emitted; f32 ops
+    # stay scalar in stencil kernels
+    body = src.split("chai_group")[1]
+    assert "% 64)" not in body and "f2x4" not in body
+
+
+def test_flat_kernel_packs_f32_add_sub():
+    """Element-wise kernels issue f32 add / sub as f32x2 pairs of neighbouring
+    elements (registers of one 16-byte load); PackF32=0 keeps them scalar."""
+    def build():
+        a = ch.index_f32(0, 64, 4)
+        return ch.Arrayf32((a + f32(1)) * f32(3) - a)
+    stmts, a = record(build)
+    st, src = source(stmts, [(a.var, 4, 64, 4, 1, 0, 5)])
+    assert st == 0 and "f2x4<11>" in src and "f2x4<14>" in src and "f2x4<13>" not in src
+    st0, src0 = source(stmts, [(a.var, 4, 64, 4, 1, 0, 5)], "PackF32=0")
+    assert st0 == 0 and "f2x4" not in src0.split("chai_group")[1]
 
 
 def test_data_dependent_gather_stays_generic():
