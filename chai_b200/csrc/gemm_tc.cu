@@ -887,39 +887,39 @@ __global__ void __launch_bounds__(256) grouped_split_cols(const ColJob* __restri
 // round trip of the bf16 planes through HBM costs more than the MMAs.  This
 // kernel reads the f32 operands once and splits them on the way into shared
 // memory:
-//   host        a driver-encoded tensor map of each problem's B (cached per
-//               context), uploaded with one record per output tile (fs_tiles)
-//   warp 0      producer: TMA-loads each 64-element K chunk of B (4 boxes of
-//               64 k x 32 f32, SWIZZLE_128B, zero fill past N and K) into one
-//               of two f32 stages
+//   host        one 64-byte record per output tile (fs_tiles)
+//   warp 0      idle (keeps the role numbering of the other GEMM kernels)
 //   warp 1      TMEM owner; one thread issues the S product blocks of each
 //               chunk (4 x tcgen05.mma, M = N = 128, K = 16 each)
 //   warps 2-5   epilogue (TMEM lane quarter = warp % 4)
-//   warps 6-13  converters: A rows straight from global memory (16-byte
-//               loads into registers, one chunk ahead) and the B stage ->
-//               the P distinct bf16 planes of A and B (K-major, SWIZZLE_128B
-//               rows of 64 bf16) in one of two plane buffers, so a chunk is
-//               converted while the MMAs of the previous one run
-// Shared memory carries only B's f32 stage, the planes and the tensor core's
-// operand reads.  The MMA sequence (planes, order, accumulators) is the one
-// the prepass path issues, so both paths give bit-identical C.
+//   warps 6-21  converters: each 64-element K chunk of A (rows, 16-byte loads
+//               along k) and of B (rows of k, 16-byte loads along n) straight
+//               from global memory into registers, one chunk ahead, then the
+//               P distinct bf16 planes into one of two plane buffers, so a
+//               chunk is converted while the MMAs of the previous one run.
+//               A planes are K-major (SWIZZLE_128B rows of 64 bf16); B planes
+//               are MN-major (SWIZZLE_128B atoms of 8 k x 64 n), which a
+//               row-major B converts into without a transpose.
+// Shared memory carries only the planes and the tensor core's operand reads.
+// The MMA sequence (planes, order, accumulators) is the one the prepass path
+// issues, so both paths give bit-identical C.
 constexpr int FS_BN = 128;
 constexpr int FS_KB = 64;                      // K elements per chunk
-constexpr int FS_NF = 2;                       // B f32 stages
 constexpr int FS_CONV = 16;                    // converter warps
-constexpr int FS_BRUNS = 8 * 128 / (FS_CONV * 32);   // B: runs of 8 k per converter thread
 constexpr int FS_CT = FS_CONV * 32;            // converter threads
 constexpr int FS_THREADS = (6 + FS_CONV) * 32;
-constexpr int FS_B_F32 = FS_KB * FS_BN * 4;    // 32 KiB: 4 boxes [64 k][32 f32]
-constexpr int FS_PLANE = BM * 128;             // 16 KiB: 128 rows x 64 bf16 (A and B planes alike)
+constexpr int FS_PLANE = BM * 128;             // 16 KiB: 128 x 64 bf16 (A and B planes alike)
+constexpr int FS_BV = FS_KB * FS_BN / 4 / FS_CT;   // B: 16-byte loads per converter thread and chunk
+// MN-major B plane: [n block of 64][k group of 8][8 k rows x 128 bytes]
+constexpr int FS_B_LBO = 8 * 1024;             // bytes between n blocks
+constexpr int FS_B_SBO = 1024;                 // bytes between k groups
 
-// plane buffers: two (convert one chunk while the MMAs read the other), one
-// for bf16x6 whose three planes per operand leave no room for a second
-__host__ __device__ constexpr int fs_pbufs(int S) { return S == 6 ? 1 : 2; }
+// plane buffers: convert one chunk while the MMAs read the other
+__host__ __device__ constexpr int fs_pbufs(int) { return 2; }
 
 __host__ __device__ constexpr int fs_smem_bytes(int S)
 {
-    return FS_NF * FS_B_F32 + fs_pbufs(S) * 2 * distinct_planes(S) * FS_PLANE + 1024 + 256;
+    return fs_pbufs(S) * 2 * distinct_planes(S) * FS_PLANE + 1024 + 256;
 }
 
 struct FusedEntry {
@@ -930,19 +930,20 @@ struct FusedEntry {
     int m, n, k, tiles_n, kblocks, vec_ok;
 };
 
-// Everything a role needs about one 128 x 128 output tile (one 48-byte
+// Everything a role needs about one 128 x 128 output tile (one 64-byte
 // record per tile, written by fs_tiles before the GEMM).
 struct __align__(16) FsTile {
     const float* a;         // A rows of the tile (row0), k = 0
+    const float* b;         // B columns of the tile (col0), k = 0
     float* c;               // C(tile origin)
-    int prob;               // problem index: the tensor map of its B is at maps + 128 prob
+    int prob;               // problem index
     int n, k;
     int col0;               // tile origin column in C
     int rows, cols;         // valid rows / columns of the tile (<= 128)
     int kblocks, vec_ok;
 };
 
-static_assert(sizeof(FsTile) == 48, "tile record size");
+static_assert(sizeof(FsTile) == 64, "tile record size");
 
 __global__ void __launch_bounds__(128) fs_tiles(const FusedEntry* __restrict__ groups, FsTile* __restrict__ out)
 {
@@ -952,6 +953,7 @@ __global__ void __launch_bounds__(128) fs_tiles(const FusedEntry* __restrict__ g
         const int tm = l / g.tiles_n, tn = l - tm * g.tiles_n;
         FsTile t;
         t.a = g.a + (long long)tm * BM * g.k;
+        t.b = g.b + (long long)tn * FS_BN;
         t.c = g.c + (long long)tm * BM * g.n + (long long)tn * FS_BN;
         t.prob = blockIdx.x;
         t.n = g.n;
@@ -963,13 +965,6 @@ __global__ void __launch_bounds__(128) fs_tiles(const FusedEntry* __restrict__ g
         t.vec_ok = g.vec_ok;
         out[g.tile_start + l] = t;
     }
-}
-
-__device__ __forceinline__ void tma_load_2d(unsigned dst, const void* map, unsigned bar, int x, int y)
-{
-    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
-                 ::"r"(dst), "l"(map), "r"(bar), "r"(x), "r"(y)
-                 : "memory");
 }
 
 // Two consecutive-k values -> their P bf16 planes (the split of split3, two
@@ -1019,12 +1014,32 @@ __device__ __forceinline__ void fs_load_a(FsA& r, const FsTile& ti, int kb, int 
     }
 }
 
-// registers (A) and the f32 stage (B) -> planes.  A: lanes 0-15 write one
-// 128-byte plane row, lanes 16-31 the next.  B: thread ct takes column
-// n = ct % 128 and FS_BRUNS runs of 8 k, reading the SWIZZLE_128B stage.
+// B chunk in registers: converter thread ct holds n = 4 (ct % 32) .. + 3 of
+// k rows ct / 32 + 16 u (u < FS_BV); a warp reads 512 contiguous bytes of a row
+struct FsB {
+    float4 v[FS_BV];
+};
+
+__device__ __forceinline__ void fs_load_b(FsB& r, const FsTile& ti, int kb, int ct)
+{
+    const int n4 = ct & 31, kr = ct >> 5;
+    const bool nok = 4 * n4 < ti.cols;             // N is a multiple of 4: a group of 4 is all in or all out
+    const float* bp = ti.b + 4 * n4;
+#pragma unroll
+    for (int u = 0; u < FS_BV; u++) {
+        const int k = kb * FS_KB + kr + 16 * u;
+        r.v[u] = (nok && k < ti.k) ? __ldcg(reinterpret_cast<const float4*>(bp + (long long)k * ti.n))
+                                   : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// registers -> planes.  A: lanes 0-15 write one 128-byte K-major plane row,
+// lanes 16-31 the next.  B: each thread writes its 4 n of a k row as 8 bytes
+// of the MN-major plane; lanes 0-15 fill one 128-byte atom row, lanes 16-31
+// the same row of the next n block.
 template <int P>
-__device__ __forceinline__ void fs_convert(const FsA& ra, const unsigned char* fb, unsigned char* pa,
-                                           unsigned char* pb, int cw, int lane, int ct)
+__device__ __forceinline__ void fs_convert(const FsA& ra, const FsB& rb, unsigned char* pa, unsigned char* pb,
+                                           int cw, int lane, int ct)
 {
     const int kq = lane & 15;
 #pragma unroll
@@ -1037,34 +1052,38 @@ __device__ __forceinline__ void fs_convert(const FsA& ra, const unsigned char* f
 #pragma unroll
         for (int p = 0; p < P; p++) *reinterpret_cast<uint2*>(pa + p * FS_PLANE + off) = make_uint2(h0[p], h1[p]);
     }
-    const int n = ct & (FS_BN - 1);
-    const unsigned char* col = fb + (n >> 5) * (FS_KB * 128) + (n & 3) * 4;   // box of n, lane of its chunk
-    const int nc = (n & 31) >> 2;                                           // 16-byte chunk of n in a box row
+    const int n4 = ct & 31, kr = ct >> 5;
+    const int nb = n4 >> 4;                        // n block of 64
+    const int ch = (n4 & 15) >> 1;                 // 16-byte chunk of the n block's 128-byte row
+    const int half = (n4 & 1) * 8;                 // byte offset of the 4 n in the chunk
 #pragma unroll
-    for (int u = 0; u < FS_BRUNS; u++) {
-        const int kc = (ct >> 7) * FS_BRUNS + u;
-        unsigned h[3][4];
+    for (int u = 0; u < FS_BV; u++) {
+        const int k = kr + 16 * u;
+        unsigned h0[3], h1[3];
+        split_pair<P>(rb.v[u].x, rb.v[u].y, h0);
+        split_pair<P>(rb.v[u].z, rb.v[u].w, h1);
+        const unsigned off = (unsigned)(nb * FS_B_LBO + (k >> 3) * FS_B_SBO) + sw128(k & 7, ch) + half;
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int k0 = kc * 8 + 2 * i;
-            const float x = *reinterpret_cast<const float*>(col + sw128(k0, nc));
-            const float y = *reinterpret_cast<const float*>(col + sw128(k0 + 1, nc));
-            unsigned q[3];
-            split_pair<P>(x, y, q);
-#pragma unroll
-            for (int p = 0; p < P; p++) h[p][i] = q[p];
-        }
-        const unsigned off = sw128(n, kc);
-#pragma unroll
-        for (int p = 0; p < P; p++)
-            *reinterpret_cast<uint4*>(pb + p * FS_PLANE + off) = make_uint4(h[p][0], h[p][1], h[p][2], h[p][3]);
+        for (int p = 0; p < P; p++) *reinterpret_cast<uint2*>(pb + p * FS_PLANE + off) = make_uint2(h0[p], h1[p]);
     }
+}
+
+// MN-major SWIZZLE_128B descriptor: LBO between 64-element n blocks, SBO
+// between 8-row k groups
+__device__ __forceinline__ unsigned long long smem_desc_mn(unsigned addr)
+{
+    unsigned long long d = 0;
+    d |= (unsigned long long)((addr & 0x3FFFF) >> 4);          // start address
+    d |= (unsigned long long)(FS_B_LBO >> 4) << 16;            // LBO
+    d |= (unsigned long long)(FS_B_SBO >> 4) << 32;            // SBO
+    d |= (unsigned long long)1 << 46;                          // version
+    d |= (unsigned long long)2 << 61;                          // SWIZZLE_128B
+    return d;
 }
 
 template <int S, bool ACC2>
 __global__ void __launch_bounds__(FS_THREADS, 1)
-chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const unsigned char* __restrict__ maps,
-                      int* status)
+chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* status)
 {
     constexpr int P = Planes<S>::P;
     constexpr int SEL = S == 1 ? 0 : (S == 3 ? 1 : 2);
@@ -1074,25 +1093,18 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const 
     constexpr unsigned TMEM_COLS = 2 * BUF_COLS;                   // double-buffered accumulators
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char* fb = smem;                                      // B f32 stages
-    unsigned char* planes = fb + FS_NF * FS_B_F32;                 // NPB plane buffers
+    unsigned char* planes = smem;                                  // NPB plane buffers
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(planes + NPB * PBUF);
-    unsigned long long* ffull = bars;                              // [FS_NF] B stage landed
-    unsigned long long* fempty = bars + FS_NF;                     // [FS_NF] B stage read (per converter warp)
-    unsigned long long* pfull = bars + 2 * FS_NF;                  // [2] planes written (per converter warp)
-    unsigned long long* pempty = bars + 2 * FS_NF + 2;             // [2] planes consumed (tcgen05.commit)
-    unsigned long long* tfull = bars + 2 * FS_NF + 4;              // [2]
-    unsigned long long* tempty = bars + 2 * FS_NF + 6;             // [2]
-    unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * FS_NF + 8);
+    unsigned long long* pfull = bars;                              // [2] planes written (per converter warp)
+    unsigned long long* pempty = bars + 2;                         // [2] planes consumed (tcgen05.commit)
+    unsigned long long* tfull = bars + 4;                          // [2]
+    unsigned long long* tempty = bars + 6;                         // [2]
+    unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 8);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long G = gridDim.x;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < FS_NF; s++) {
-            mbar_init(smem_u32(&ffull[s]), 1);
-            mbar_init(smem_u32(&fempty[s]), FS_CONV);
-        }
         for (int b = 0; b < 2; b++) {
             mbar_init(smem_u32(&pfull[b]), FS_CONV);
             mbar_init(smem_u32(&pempty[b]), 1);
@@ -1113,38 +1125,11 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const 
     const unsigned tmem = *tmem_slot;
 
     if (warp == 0) {
-        // ------------------------------------------------------------ producer
-        if (lane == 0) {
-            long long it = 0, issued = 0;
-            bool ok = true;
-            for (long long t = blockIdx.x; t < ntiles && ok && !*abort_flag; t += G) {
-                const FsTile ti = tiles[t];
-                const unsigned char* gb = maps + (size_t)ti.prob * 128;
-                asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(gb) : "memory");
-                for (int kb = 0; kb < ti.kblocks; kb++, it++) {
-                    const int s = (int)(it % FS_NF);
-                    const long long r = it / FS_NF;
-                    if (r > 0 && !mbar_wait(smem_u32(&fempty[s]), (unsigned)((r - 1) & 1), status, 111)) {
-                        ok = false;
-                        break;
-                    }
-                    const unsigned bar = smem_u32(&ffull[s]);
-                    mbar_expect_tx(bar, FS_B_F32);
-                    for (int j = 0; j < 4; j++)
-                        tma_load_2d(smem_u32(fb + s * FS_B_F32 + j * (FS_KB * 128)), gb, bar, ti.col0 + 32 * j,
-                                    kb * FS_KB);
-                    issued = it + 1;
-                }
-            }
-            if (!ok) *abort_flag = 1;
-            // wait (bounded) until every copy this thread issued has landed
-            for (long long j = issued - FS_NF < 0 ? 0 : issued - FS_NF; j < issued; j++)
-                mbar_wait(smem_u32(&ffull[j % FS_NF]), (unsigned)((j / FS_NF) & 1), status, 112);
-        }
+        // idle: both operands reach shared memory through the converters
     } else if (warp == 1) {
         // ---------------------------------------------------------------- MMA
         if (lane == 0) {
-            const unsigned idesc = instr_desc<KIND_BF16, FS_BN>();
+            const unsigned idesc = instr_desc<KIND_BF16, FS_BN>() | (1u << 16);   // B MN-major
             long long it = 0;
             int lt = 0;
             int kbs_next = blockIdx.x < ntiles ? tiles[blockIdx.x].kblocks : 0;
@@ -1177,8 +1162,8 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const 
                         const bool first = ACC2 ? (kb == 0 && blk <= 1) : (kb == 0 && blk == 0);
 #pragma unroll
                         for (int k = 0; k < 4; k++)
-                            mma<KIND_BF16>(acc, smem_desc(a0 + 32 * k), smem_desc(b0 + 32 * k), idesc,
-                                           !(first && k == 0));
+                            mma<KIND_BF16>(acc, smem_desc(a0 + 32 * k), smem_desc_mn(b0 + 2 * FS_B_SBO * k),
+                                           idesc, !(first && k == 0));
                     }
                     mma_commit(smem_u32(&pempty[q]));  // buffer q free once these MMAs finish
                 }
@@ -1254,31 +1239,30 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, const 
             if (lt_ + G < ntiles) lnext = tiles[lt_ + G];
         };
         FsA ra;
-        bool have = lt_ < ntiles;                   // chunk `it` of A is in the registers
+        FsB rb;
+        bool have = lt_ < ntiles;                   // chunk `it` of A and B is in the registers
         if (have) {
             fs_load_a(ra, lti, 0, cw, lane);
+            fs_load_b(rb, lti, 0, ct);
             advance();
         }
         bool ok = true;
         for (long long it = 0; have && !*abort_flag; it++) {
-            const int s = (int)(it % FS_NF), q = (int)(it % NPB);
-            ok = mbar_wait(smem_u32(&ffull[s]), (unsigned)((it / FS_NF) & 1), status, 116);
+            const int q = (int)(it % NPB);
             // plane buffer q was last read by the MMAs of chunk it - NPB
-            if (ok && it >= NPB) ok = mbar_wait(smem_u32(&pempty[q]), (unsigned)((it / NPB - 1) & 1), status, 117);
+            if (it >= NPB) ok = mbar_wait(smem_u32(&pempty[q]), (unsigned)((it / NPB - 1) & 1), status, 117);
             if (!ok) break;
             unsigned char* pa = planes + q * PBUF;
-            fs_convert<P>(ra, fb + s * FS_B_F32, pa, pa + P * FS_PLANE, cw, lane, ct);
+            fs_convert<P>(ra, rb, pa, pa + P * FS_PLANE, cw, lane, ct);
             // the tensor core reads the planes through the async proxy
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0) {
-                mbar_arrive(smem_u32(&fempty[s]));
-                mbar_arrive(smem_u32(&pfull[q]));
-            }
-            // next chunk of A into the registers while the MMAs run
+            if (lane == 0) mbar_arrive(smem_u32(&pfull[q]));
+            // next chunk of A and B into the registers while the MMAs run
             have = lt_ < ntiles;
             if (have) {
                 fs_load_a(ra, lti, lkb, cw, lane);
+                fs_load_b(rb, lti, lkb, ct);
                 advance();
             }
         }
@@ -1569,8 +1553,8 @@ namespace chai {
 // its first tile.  A tile that overhangs a problem's M or N reads rows of the
 // next problem (or TMA zero fill past the end): they only reach accumulator
 // rows / columns that the epilogue does not store.
-// In-kernel split (chai_gemm_fused_split): A rows are read in 16-byte loads
-// and B through a tensor map: 16-byte aligned bases, K and N multiples of 4.
+// In-kernel split (chai_gemm_fused_split): A rows and B rows are read in
+// 16-byte loads: 16-byte aligned bases, K and N multiples of 4.
 static bool fused_split_ok(const chai_gemm_problem* p, int32_t count)
 {
     for (int i = 0; i < count; i++) {
@@ -1582,39 +1566,9 @@ static bool fused_split_ok(const chai_gemm_problem* p, int32_t count)
     return true;
 }
 
-// 2-D f32 map of a row-major (rows x cols) array, box 32 x by, SWIZZLE_128B,
-// encoded by the driver; cached per context by (address, sizes, box).
-static int f32_map(chai_cuda_ctx* ctx, const void* base, long long cols, long long rows, int by,
-                   chai_cuda_ctx::RawMap* out)
-{
-    const chai_cuda_ctx::MapKey key{base, cols, rows, by};
-    auto it = ctx->map_cache.find(key);
-    if (it != ctx->map_cache.end()) {
-        *out = it->second;
-        return CHAI_OK;
-    }
-    PFN_encodeTiled enc = encode_fn(ctx);
-    if (!enc) return CHAI_ERR_NO_DEVICE;
-    CUtensorMap m;
-    memset(&m, 0, sizeof m);
-    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)cols * 4};
-    cuuint32_t box[2] = {32, (cuuint32_t)by};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return set_error(ctx, CHAI_ERR_INVALID, "cuTensorMapEncodeTiled failed (grouped operand)");
-    static_assert(sizeof(CUtensorMap) == sizeof(chai_cuda_ctx::RawMap), "tensor map size");
-    memcpy(out->bytes, &m, sizeof m);
-    if (ctx->map_cache.size() >= (1u << 16)) ctx->map_cache.clear();
-    ctx->map_cache.emplace(key, *out);
-    return CHAI_OK;
-}
-
-// The tile records and tensor maps of a grouped call live in a per-context
-// buffer and are rebuilt only when the problem array (pointers, sizes) or the
-// precision changes; a repeated call launches the GEMM directly.
+// The tile records of a grouped call live in a per-context buffer and are
+// rebuilt only when the problem array (pointers, sizes) or the precision
+// changes; a repeated call launches the GEMM directly.
 static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_problem* p, int32_t count)
 {
     using namespace tc;
@@ -1624,7 +1578,6 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
                       memcmp(gp.problems.data(), p, sizeof(chai_gemm_problem) * count) == 0;
     if (!same) {
         std::vector<FusedEntry> g(count);
-        std::vector<chai_cuda_ctx::RawMap> maps((size_t)count);
         long long tiles = 0, kmax = 0;
         for (int i = 0; i < count; i++) {
             const chai_gemm_problem& q = p[i];
@@ -1641,12 +1594,9 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
             e.vec_ok = ((reinterpret_cast<uintptr_t>(q.c) & 15) == 0 && q.n % 4 == 0) ? 1 : 0;
             tiles += (long long)((q.m + BM - 1) / BM) * e.tiles_n;
             kmax = std::max<long long>(kmax, (long long)e.kblocks * FS_KB);
-            const int st = f32_map(ctx, q.b, q.n, q.k, FS_KB, &maps[i]);         // B: n x k, box 32 x 64
-            if (st) return st;
         }
         if (tiles >= (1ll << 31)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "grouped gemm: too large");
-        const size_t t_bytes = ((size_t)tiles * sizeof(FsTile) + 255) & ~size_t(255);
-        const size_t need = t_bytes + maps.size() * sizeof(chai_cuda_ctx::RawMap);
+        const size_t need = ((size_t)tiles * sizeof(FsTile) + 255) & ~size_t(255);
         if (gp.bytes < need) {
             if (gp.dev) CHAI_CUDA_TRY(ctx, cudaFreeAsync(gp.dev, s));
             gp.dev = nullptr;
@@ -1658,19 +1608,15 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
         if (st) return st;
         FusedEntry* dg = static_cast<FusedEntry*>(ctx->scratch);
         CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(dg, g.data(), g.size() * sizeof(FusedEntry), cudaMemcpyHostToDevice, s));
-        CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(static_cast<char*>(gp.dev) + t_bytes, maps.data(),
-                                           maps.size() * sizeof(chai_cuda_ctx::RawMap), cudaMemcpyHostToDevice, s));
         fs_tiles<<<(unsigned)count, 128, 0, s>>>(dg, static_cast<FsTile*>(gp.dev));
         CHAI_CUDA_TRY(ctx, cudaGetLastError());
         gp.problems.assign(p, p + count);
         gp.S = S;
         gp.tiles = tiles;
-        gp.map_off = (long long)t_bytes;
         // the same accumulator rule as the prepass path (see launch_gemm_grouped)
         gp.acc2 = S == 6 || kmax > 2048;
     }
     const FsTile* dt = static_cast<const FsTile*>(gp.dev);
-    const unsigned char* dm = static_cast<const unsigned char*>(gp.dev) + gp.map_off;
     const long long tiles = gp.tiles;
     const unsigned grid = (unsigned)std::min<long long>(tiles, ctx->sm_count);
     cudaEvent_t ev[2];
@@ -1679,7 +1625,7 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
     do {                                                                                             \
         auto k = chai_gemm_fused_split<SS, A2>;                                                      \
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, fs_smem_bytes(SS));    \
-        k<<<grid, FS_THREADS, fs_smem_bytes(SS), s>>>(dt, tiles, dm, ctx->status_word);              \
+        k<<<grid, FS_THREADS, fs_smem_bytes(SS), s>>>(dt, tiles, ctx->status_word);                  \
     } while (0)
     if (S == 1) CHAI_FS(1, false);
     else if (S == 3 && !gp.acc2) CHAI_FS(3, false);

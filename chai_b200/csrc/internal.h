@@ -72,28 +72,14 @@ struct chai_cuda_ctx {
     std::vector<cudaEvent_t> event_pool;
     std::unordered_map<uint64_t, std::shared_ptr<chai::Plan>> plans;   // plan cache, by key hash
     uint64_t plan_hits = 0;
-    // grouped GEMM with the in-kernel split: driver-encoded tensor maps by
-    // (address, columns, rows, box rows), and the device arrays of the last
-    // call, reused while the problem array repeats
-    struct RawMap { alignas(64) unsigned char bytes[128]; };
-    struct MapKey {
-        const void* base; long long cols, rows; int box;
-        bool operator==(const MapKey& o) const { return base == o.base && cols == o.cols && rows == o.rows && box == o.box; }
-    };
-    struct MapKeyHash {
-        size_t operator()(const MapKey& k) const {
-            size_t h = std::hash<const void*>()(k.base);
-            h ^= std::hash<long long>()(k.cols * 1000003 + k.rows) + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
-            return h ^ (size_t)k.box;
-        }
-    };
-    std::unordered_map<MapKey, RawMap, MapKeyHash> map_cache;
+    // grouped GEMM with the in-kernel split: the device tile records of the
+    // last call, reused while the problem array repeats
     struct GroupedPlan {
         std::vector<chai_gemm_problem> problems;
         int S = 0;
-        void* dev = nullptr;         // tile records, then 2 maps per problem
+        void* dev = nullptr;         // tile records
         size_t bytes = 0;
-        long long tiles = 0, map_off = 0;
+        long long tiles = 0;
         bool acc2 = false;
     } gplan;
     uint64_t fused_launches = 0;
