@@ -891,7 +891,9 @@ __global__ void __launch_bounds__(256) grouped_split_cols(const ColJob* __restri
 //   warp 0      idle (keeps the role numbering of the other GEMM kernels)
 //   warp 1      TMEM owner; one thread issues the S product blocks of each
 //               chunk (4 x tcgen05.mma, M = N = 128, K = 16 each)
-//   warps 2-5   epilogue (TMEM lane quarter = warp % 4)
+//   warps 2-5   epilogue (TMEM lane quarter = warp % 4): each 32 x 32 block
+//               of the accumulator through a shared-memory stage, so that 8
+//               lanes store 128 contiguous bytes of a C row
 //   warps 6-21  converters: each 64-element K chunk of A (rows, 16-byte loads
 //               along k) and of B (rows of k, 16-byte loads along n) straight
 //               from global memory into registers, one chunk ahead, then the
@@ -913,13 +915,15 @@ constexpr int FS_BV = FS_KB * FS_BN / 4 / FS_CT;   // B: 16-byte loads per conve
 // MN-major B plane: [n block of 64][k group of 8][8 k rows x 128 bytes]
 constexpr int FS_B_LBO = 8 * 1024;             // bytes between n blocks
 constexpr int FS_B_SBO = 1024;                 // bytes between k groups
+constexpr int FS_EP = 36;                      // epilogue stage row pitch (floats; 16-byte rows, 4-bank skew)
+constexpr int FS_ESTAGE = 4 * 32 * FS_EP * 4;  // four epilogue warps x 32 rows
 
 // plane buffers: convert one chunk while the MMAs read the other
 __host__ __device__ constexpr int fs_pbufs(int) { return 2; }
 
 __host__ __device__ constexpr int fs_smem_bytes(int S)
 {
-    return fs_pbufs(S) * 2 * distinct_planes(S) * FS_PLANE + 1024 + 256;
+    return fs_pbufs(S) * 2 * distinct_planes(S) * FS_PLANE + FS_ESTAGE + 1024 + 256;
 }
 
 struct FusedEntry {
@@ -1094,7 +1098,8 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char* planes = smem;                                  // NPB plane buffers
-    unsigned long long* bars = reinterpret_cast<unsigned long long*>(planes + NPB * PBUF);
+    float* estage = reinterpret_cast<float*>(planes + NPB * PBUF);  // epilogue stages
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(planes + NPB * PBUF + FS_ESTAGE);
     unsigned long long* pfull = bars;                              // [2] planes written (per converter warp)
     unsigned long long* pempty = bars + 2;                         // [2] planes consumed (tcgen05.commit)
     unsigned long long* tfull = bars + 4;                          // [2]
@@ -1177,7 +1182,8 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
     } else if (warp < 6) {
         // ----------------------------------------------------------- epilogue
         const int quarter = warp & 3;
-        const int r = quarter * 32 + lane;             // row of the tile this lane stores
+        const int r = quarter * 32 + lane;             // row of the tile this lane holds
+        float* es = estage + quarter * (32 * FS_EP);
         int lt = 0;
         for (long long t = blockIdx.x; t < ntiles; t += G, lt++) {
             const FsTile ti = tiles[t];                // loaded while the accumulator fills
@@ -1203,12 +1209,25 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
 #pragma unroll
                     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r0[i]);
                 }
-                if (!do_store || c0 >= ti.cols) continue;
-                if (ti.vec_ok && c0 + 32 <= ti.cols) {
-                    float4* p = reinterpret_cast<float4*>(crow + c0);
+                if (c0 >= ti.cols) continue;               // uniform across the warp
+                if (ti.vec_ok) {
+                    // lane = row into the stage, then 4 rows x 8 lanes x 16 bytes per store
+                    __syncwarp();
+                    float4* er = reinterpret_cast<float4*>(es + lane * FS_EP);
 #pragma unroll
-                    for (int q = 0; q < 8; q++) p[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                    for (int q = 0; q < 8; q++) er[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                    __syncwarp();
+                    const bool go = ok && !*abort_flag;
+                    const int col = c0 + 4 * (lane & 7);   // N is a multiple of 4: a group of 4 is all in or all out
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const int row = 4 * i + (lane >> 3);
+                        const float4 x = *reinterpret_cast<const float4*>(es + row * FS_EP + 4 * (lane & 7));
+                        if (go && quarter * 32 + row < ti.rows && col < ti.cols)
+                            *reinterpret_cast<float4*>(ti.c + (long long)(quarter * 32 + row) * ti.n + col) = x;
+                    }
                 } else {
+                    if (!do_store) continue;
 #pragma unroll
                     for (int i = 0; i < 32; i++)
                         if (c0 + i < ti.cols) crow[c0 + i] = v[i];
