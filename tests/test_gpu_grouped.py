@@ -101,3 +101,29 @@ def test_unaligned_group_falls_back_to_prepass(chai_dev):
     for a, b, c in zip(As, Bs, Cs):
         bound = np.abs(a).astype(np.float64) @ np.abs(b).astype(np.float64)
         assert np.max(np.abs(c - oracle.gemm_f64(a, b)) / bound) <= BOUND[L.GEMM_BF16X3]
+
+
+def test_unaligned_c_uses_scalar_stores(chai_dev, prepass_dev):
+    """C one float past a 16-byte boundary (A and B aligned, K and N multiples
+    of 4): the in-kernel split still runs, its epilogue stores C element by
+    element instead of through the shared-memory stage, and C equals the
+    prepass path's bit for bit; the float before C is left alone."""
+    import torch
+    shapes = [(136, 260, 100), (40, 128, 36), (300, 44, 64)]
+    rng = np.random.default_rng(8)
+    outs = []
+    for dev in (chai_dev, prepass_dev):
+        ta = [torch.from_numpy(rng.uniform(-1, 1, (m, k)).astype(np.float32)).cuda() for m, n, k in shapes]
+        tb = [torch.from_numpy(rng.uniform(-1, 1, (k, n)).astype(np.float32)).cuda() for m, n, k in shapes]
+        rng = np.random.default_rng(8)                      # same operands for both paths
+        tc = [torch.full((m * n + 1,), -7.0, device="cuda") for m, n, k in shapes]
+        arr = (L.chai_gemm_problem * len(shapes))()
+        for i, (m, n, k) in enumerate(shapes):
+            arr[i] = L.chai_gemm_problem(m, n, k, 0, ta[i].data_ptr(), tb[i].data_ptr(), tc[i].data_ptr() + 4)
+        before = fused_count(dev)
+        L.check(L.lib().chai_cuda_gemm_grouped(dev.ctx, L.GEMM_BF16X3, arr, len(shapes)), dev.ctx)
+        L.check(L.lib().chai_cuda_synchronize(dev.ctx), dev.ctx)
+        assert fused_count(dev) == before + (1 if dev is chai_dev else 0)
+        outs.append([c.cpu().numpy() for c in tc])
+    for (m, n, k), a, b in zip(shapes, outs[0], outs[1]):
+        assert a[0] == -7.0 and np.array_equal(a, b), (m, n, k)
