@@ -11,8 +11,9 @@
 // enough that the last of ~15 tiles per CTA leaves little of the grid idle):
 //   tab[0] = number of tiles, tab[1] = number of traces, then per trace:
 //   { n, W, H, first tile, seed of each RNG node, bits of each varying scalar }.
-// Every CTA walks tiles blockIdx.x, +gridDim.x, ...; a tile finds its trace
-// by binary search on the first-tile column; a CTA keeps its running sum over
+// Every CTA walks a contiguous run of tiles (equal runs to within one tile);
+// its first tile finds its trace by binary search on the first-tile column
+// and later tiles follow the column; a CTA keeps its running sum over
 // consecutive tiles of one trace in registers and writes its block partial at
 // its last tile of that trace (0 for the others) to partials[tile]; a second
 // kernel adds each trace's partials in tile order in FP64.  The H2D copy of the table, both kernels and the D2H copy of the
@@ -239,14 +240,19 @@ static bool build_program(const std::vector<std::vector<Node>>& all, int root, d
        << "  const long long ntiles = tab[0]; const int ntr = (int)tab[1];\n"
        << "  const long long* rows = tab + 2;\n"
        << "  double red[1] = {0};\n"
-       << "  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {\n"
-       << "    int lo = 0, hi = ntr - 1;\n"
-       << "    while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (rows[(long long)mid * " << p.stride
-       << " + 3] <= tile) lo = mid; else hi = mid - 1; }\n"
+       // each CTA takes a contiguous run of tiles, so consecutive tiles mostly
+       // share a trace (one reduction per trace and CTA); the trace is found
+       // by binary search at the run's first tile and followed from there
+       << "  const long long t0 = ntiles * blockIdx.x / gridDim.x, t1 = ntiles * (blockIdx.x + 1) / gridDim.x;\n"
+       << "  int lo = 0;\n"
+       << "  { int hi = ntr - 1; while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (rows[(long long)mid * "
+       << p.stride << " + 3] <= t0) lo = mid; else hi = mid - 1; } }\n"
+       << "  for (long long tile = t0; tile < t1; tile++) {\n"
+       << "    while (lo + 1 < ntr && rows[(long long)(lo + 1) * " << p.stride << " + 3] <= tile) lo++;\n"
        << "    const long long* tp = rows + (long long)lo * " << p.stride << ";\n"
        << "    const long long n = tp[0], W = tp[1];\n"
-       << "    const long long next = tile + gridDim.x;\n"
-       << "    const bool flush = next >= ntiles || (lo + 1 < ntr && rows[(long long)(lo + 1) * " << p.stride
+       << "    const long long next = tile + 1;\n"
+       << "    const bool flush = next >= t1 || (lo + 1 < ntr && rows[(long long)(lo + 1) * " << p.stride
        << " + 3] <= next);\n"
        << "    for (int sub = 0; sub < " << kManySubs << "; sub++) {\n"
        << "    const long long c = ((tile - tp[3]) * " << kManySubs << " + sub) * 256 + threadIdx.x;\n"
