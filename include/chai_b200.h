@@ -271,7 +271,13 @@ int chai_cuda_gemv(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int6
                    const void* a, int64_t lda, const void* x, double beta, void* y);
 
 /* Many independent f32 GEMMs of different shapes in one persistent
- * tensor-core launch (C_i = A_i B_i, row-major, packed). */
+ * tensor-core launch (C_i = A_i B_i, row-major, packed; the reference runs
+ * one matmul statement per trace, enqueue/EnqueueMatmulAuto.cpp:21-404).
+ * precision: bf16, bf16x3 or bf16x6 (fp32 and AUTO-with-fp32 mean bf16x3).
+ * When every A and B is 16-byte aligned and every K and N is a multiple of 4,
+ * the kernel splits the f32 operands into bf16 planes itself; otherwise the
+ * planes go through HBM first.  Both paths give bit-identical C.  The tile
+ * records are rebuilt only when the problem array changes. */
 typedef struct chai_gemm_problem {
     int32_t m, n, k, reserved;
     const float* a; const float* b; float* c;
