@@ -123,6 +123,9 @@ __global__ void __launch_bounds__((GB_CONSUMERS + 1) * 32) chai_gemv_bulk(const 
                 }
             }
         }
+        // the producer's next bulk copy into this stage (async proxy) must
+        // follow these generic reads of it
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
         if (lane == 0 && !bad) mbar_arrive(&empty[s]);
         if (c == cpr - 1) {
