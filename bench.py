@@ -32,6 +32,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -139,6 +140,22 @@ def time_events(fn, steps, stream, flush=None):
     return [a.elapsed_time(b) for a, b in evs]
 
 
+def timed_region(fn, args, stream):
+    """The timed region of a workload: `args.steps` steps, or -- when
+    `args.min_timed_s` is set (the secondary measurements of the default run)
+    -- as many steps as fill that many seconds, so that the clock sampler
+    (one sample per 100 ms) sees the region.  Returns the per-step CUDA-event
+    times, the clock summary and the number of timed steps."""
+    import torch
+    steps = args.steps
+    if getattr(args, "min_timed_s", 0):
+        per = max(1e-3, statistics.median(time_events(fn, 3, stream)))
+        steps = max(steps, int(math.ceil(args.min_timed_s * 1e3 / per)))
+    with Clocks(torch.cuda.current_device()) as clk:
+        ts = time_events(fn, steps, stream)
+    return ts, clk.summary(), steps
+
+
 def l2_flusher():
     import torch
     buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -162,6 +179,25 @@ def traffic(name):
     if p.exists():
         return json.loads(p.read_text()).get(name)
     return None
+
+
+def issue_roofline(kernel_ms, units, key, kernel):
+    """Roofline of an instruction-issue-bound kernel (the fused MC trace: no
+    HBM traffic, Philox integer multiplies and transcendental math):
+    achieved = warp instructions per launch (units x the per-unit count from
+    the committed ncu summary, smsp__inst_executed.sum) / launch time; peak =
+    148 SMs x 4 schedulers x one warp instruction per clock at the maximum SM
+    clock of MEASURED_PEAKS.json."""
+    P, kind = peaks()
+    per_unit = traffic(key)
+    if not kernel_ms or not per_unit:
+        return None
+    mhz = P.get("sm_max_mhz", 1965.0)
+    peak = 148 * 4 * mhz * 1e6 / 1e12          # warp instructions per second, in T/s
+    ach = units * per_unit / (kernel_ms * 1e-3) / 1e12
+    return {"bound": "issue", "achieved": ach, "peak": peak, "unit": "Twarp-inst/s", "frac": ach / peak,
+            "traffic": None, "peak_source": "148 SMs x 4 issue slots x %s max SM clock (%s)" % (mhz, kind),
+            "kernel": kernel, "kernel_ms": kernel_ms, "warp_inst_per_unit": per_unit}
 
 
 GEMM_PREC = {"fp32": 0, "tf32": 1, "bf16": 2, "bf16x3": 3, "bf16x6": 4, "fp8": 5}
@@ -231,8 +267,7 @@ def run_gemm(args, L, ctx, stream):
     torch.cuda.synchronize()
     kstats(L, ctx, "gemm_tc")
     flops = 2.0 * n ** 3
-    with Clocks(torch.cuda.current_device()) as clk:
-        ts = time_events(step, args.steps, stream)
+    ts, clk, steps = timed_region(step, args, stream)
     ms = sum(ts) / len(ts)
     k_ms, k_n = kstats(L, ctx, "gemm_tc")
     kern_ms = k_ms / k_n if k_n else None
@@ -284,7 +319,7 @@ def run_gemm(args, L, ctx, stream):
                                "blocks with the copies overlapped with the block GEMMs"},
         "e2e": {"value": flops / (e_ms * 1e-3) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": 2 * n * n * 4,
                 "d2h_bytes_per_step": n * n * 4},
-        "roofline": roof, "clocks": clk.summary(), "gpu_launches": args.steps * {0: 1, 5: 6}.get(prec, 3),
+        "roofline": roof, "clocks": clk, "steps": steps, "gpu_launches": steps * {0: 1, 5: 6}.get(prec, 3),
     }
 
 
@@ -352,8 +387,7 @@ def run_mc(args, L, ctx, stream):
         step()
     torch.cuda.synchronize()
     kstats(L, ctx, "trace")
-    with Clocks(torch.cuda.current_device()) as clk:
-        ts = time_events(step, args.steps, stream)
+    ts, clk, steps = timed_region(step, args, stream)
     ms = sum(ts) / len(ts)
     k_ms, k_n = kstats(L, ctx, "trace")
 
@@ -366,6 +400,8 @@ def run_mc(args, L, ctx, stream):
     for _ in range(max(1, args.steps)):
         payoff = e2e()
     e_ms = (time.perf_counter() - t0) * 1e3 / max(1, args.steps)
+    roof = issue_roofline(k_ms / k_n if k_n else None, n, "trace_mc_warp_inst_per_normal",
+                          "chai_group (MC trace, RNG in registers)")
     return {
         "metric": "trace throughput (MC: Philox normals -> exp -> mean)", "unit": "Gnormals/s",
         "value": n / (ms * 1e-3) / 1e9, "ms_per_step": ms, "dtype": "f32", "higher_is_better": True,
@@ -374,7 +410,7 @@ def run_mc(args, L, ctx, stream):
                    "kernel_ms": (k_ms / k_n) if k_n else None},
         "e2e": {"value": n / (e_ms * 1e-3) / 1e9, "unit": "Gnormals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 16},
-        "roofline": None, "clocks": clk.summary(), "gpu_launches": args.steps * 2,
+        "roofline": roof, "clocks": clk, "steps": steps, "gpu_launches": steps * 2,
     }
 
 
@@ -426,8 +462,7 @@ def run_c1(args, L, ctx, stream):
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
-    with Clocks(torch.cuda.current_device()) as clk:
-        ts = time_events(step, args.steps, stream)
+    ts, clk, steps = timed_region(step, args, stream)
     ms = sum(ts) / len(ts)
     per_step = count_launches(step)
     # e2e: A and B from pinned host memory through make2 every evaluation,
@@ -457,8 +492,8 @@ def run_c1(args, L, ctx, stream):
                    "gemm_precision": "context default", "l2": "inputs generated in the trace (no HBM inputs)"},
         "e2e": {"value": flops / (e_ms * 1e-3) / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": 2 * n * n * 4,
                 "d2h_bytes_per_step": 4},
-        "roofline": None, "clocks": clk.summary(),
-        "gpu_launches": (per_step * args.steps) if per_step is not None else args.steps * 6,
+        "roofline": None, "clocks": clk, "steps": steps,
+        "gpu_launches": (per_step * steps) if per_step is not None else steps * 6,
     }
 
 
@@ -496,8 +531,7 @@ def run_mc_hbm(args, L, ctx, stream):
     torch.cuda.synchronize()
     kstats(L, ctx, "trace")
     # Z (512 MiB) is four times L2: streamed from HBM each step without a flush
-    with Clocks(torch.cuda.current_device()) as clk:
-        ts = time_events(step, args.steps, stream)
+    ts, clk, steps = timed_region(step, args, stream)
     ms = sum(ts) / len(ts)
     k_ms, k_n = kstats(L, ctx, "trace")
     kern_ms = k_ms / k_n if k_n else None
@@ -534,7 +568,7 @@ def run_mc_hbm(args, L, ctx, stream):
                    "normals": n, "payoff": float(out[0]), "l2": "Z (512 MiB) larger than L2, no flush"},
         "e2e": {"value": nbytes / (e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": 4},
-        "roofline": roof, "clocks": clk.summary(), "gpu_launches": args.steps * 2,
+        "roofline": roof, "clocks": clk, "steps": steps, "gpu_launches": steps * 2,
     }
 
 
@@ -585,8 +619,7 @@ def run_kirsch(args, L, ctx, stream):
         step()
     torch.cuda.synchronize()
     kstats(L, ctx, "trace")
-    with Clocks(torch.cuda.current_device()) as clk:
-        ts = time_events(step, args.steps, stream)
+    ts, clk, steps = timed_region(step, args, stream)
     ms = sum(ts) / len(ts)
     k_ms, k_n = kstats(L, ctx, "trace")
     nbytes = 2 * 4 * W * H
@@ -623,7 +656,7 @@ def run_kirsch(args, L, ctx, stream):
                    % (W, H), "l2": "image (%d MiB) larger than L2" % (W * H * 4 >> 20)},
         "e2e": {"value": nbytes / (e_ms * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": W * H * 4,
                 "d2h_bytes_per_step": W * H * 4},
-        "roofline": roof, "clocks": clk.summary(), "gpu_launches": args.steps,
+        "roofline": roof, "clocks": clk, "steps": steps, "gpu_launches": steps,
     }
 
 
@@ -648,8 +681,7 @@ def run_gemv(args, L, ctx, stream):
     # A (>= 256 MiB at the default size) is at least twice L2: each step
     # streams it from HBM without a flush (a written flush buffer would leave
     # dirty L2 lines whose write-back the next step would pay for)
-    with Clocks(torch.cuda.current_device()) as clk:
-        ts = time_events(step, args.steps, stream)
+    ts, clk, steps = timed_region(step, args, stream)
     ms = sum(ts) / len(ts)
     k_ms, k_n = kstats(L, ctx, "gemv")
     nbytes = (m * n + m + n) * eb
@@ -665,7 +697,7 @@ def run_gemv(args, L, ctx, stream):
         "roofline": {"bound": "hbm", "achieved": ach, "peak": P["hbm_gbs"], "unit": "GB/s",
                      "frac": ach / P["hbm_gbs"], "traffic": traffic("gemv_%d" % m), "peak_source": kind,
                      "kernel": "chai_gemv_n", "kernel_ms": kern_ms, "algorithmic_bytes": nbytes},
-        "clocks": clk.summary(), "gpu_launches": args.steps,
+        "clocks": clk, "steps": steps, "gpu_launches": steps,
     }
 
 
@@ -699,11 +731,19 @@ def run_mc_many(args, L, ctx, stream):
         step()
     torch.cuda.synchronize()
     kstats(L, ctx, "many")
+    steps = args.steps
+    if getattr(args, "min_timed_s", 0):
+        t0 = time.perf_counter()
+        for _ in range(3):
+            step()
+        per = max(1e-3, (time.perf_counter() - t0) * 1e3 / 3)
+        steps = max(steps, int(math.ceil(args.min_timed_s * 1e3 / per)))
     with Clocks(torch.cuda.current_device()) as clk:
         t0 = time.perf_counter()
-        for _ in range(args.steps):
+        for _ in range(steps):
             step()
-        wall = (time.perf_counter() - t0) * 1e3 / args.steps
+        wall = (time.perf_counter() - t0) * 1e3 / steps
+    clk = clk.summary()
     k_ms, k_n = kstats(L, ctx, "many")
     kern = k_ms / k_n if k_n else wall
 
@@ -723,7 +763,7 @@ def run_mc_many(args, L, ctx, stream):
                    "host_ms_per_call": wall, "l2": "no HBM inputs (RNG in registers)"},
         "e2e": {"value": total / (e_ms * 1e-3) / 1e9, "unit": "Gnormals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 8 * len(Ls)},
-        "roofline": None, "clocks": clk.summary(), "gpu_launches": args.steps * 2,
+        "roofline": None, "clocks": clk, "steps": steps, "gpu_launches": steps * 2,
     }
 
 
@@ -762,8 +802,7 @@ def run_grouped(args, L, ctx, stream):
         step()
     torch.cuda.synchronize()
     kstats(L, ctx, "gemm_grouped")
-    with Clocks(torch.cuda.current_device()) as clk:
-        ts = time_events(step, args.steps, stream)
+    ts, clk, steps = timed_region(step, args, stream)
     ms = sum(ts) / len(ts)
     k_ms, k_n = kstats(L, ctx, "gemm_grouped")
     kern = k_ms / k_n if k_n else ms
@@ -795,7 +834,7 @@ def run_grouped(args, L, ctx, stream):
         "roofline": {"bound": "tensor", "achieved": ach, "peak": P["bf16_tflops"], "unit": "TFLOP/s",
                      "frac": ach / P["bf16_tflops"], "traffic": traffic("gemm_grouped"), "peak_source": kind,
                      "kernel": "chai_gemm_fused_split (grouped, operands split in-kernel)", "kernel_ms": kern},
-        "clocks": clk.summary(), "gpu_launches": args.steps * 3,
+        "clocks": clk, "steps": steps, "gpu_launches": steps * 3,
     }
 
 
@@ -822,6 +861,9 @@ def run_tuner(args, L, ctx, stream):
     with tempfile.TemporaryDirectory() as td, Clocks(torch.cuda.current_device()) as clk:
         db = os.path.join(td, "tune.db")
         L.check(L.lib().chai_cuda_tune_db_save(ctx, db.encode()), ctx)
+        if getattr(args, "save_db", False):     # the committed cost model the default run evaluates
+            TUNER_DB.parent.mkdir(exist_ok=True)
+            L.check(L.lib().chai_cuda_tune_db_save(ctx, str(TUNER_DB).encode()), ctx)
         for k in (1, 2, 3):     # a fresh context per k: cold DB, the trained weights
             dev = ch.Device(config="TuneDB=%s TopK=%d" % (db, k))
             try:
@@ -858,12 +900,56 @@ def run_tuner(args, L, ctx, stream):
                   "default_vs_best_geomean": gm(qd), "learned_s_total": ls, "exhaustive_s_total": es,
                   "train_samples": len(samples), "train_loss": loss, "train_s": train_s, "sweep_s": sweep_s,
                   "by_kind": part, "top_k": topk},
+        "e2e": None, "roofline": None, "clocks": clk.summary(), "steps": len(rows), "gpu_launches": None,
+    }
+
+
+TUNER_DB = ROOT / "chai_b200" / "data" / "tuner.db"     # trained by --workload tuner --save-db
+
+
+def run_tuner_eval(args, L, ctx, stream):
+    """The learned tuner on held-out keys with the committed cost model
+    (chai_b200/data/tuner.db + .mlp, trained by `--workload tuner --save-db`
+    on the 2000 training keys): the first TUNER_EVAL_KEYS of the 200 held-out
+    keys (seed 13) are swept exhaustively, then tuned from cold by the learned
+    method (rank every configuration, time the top 2) and by the exhaustive
+    one; quality is judged on each key's own sweep."""
+    import torch
+    from chai_b200 import tuner as T
+    import chai_b200.api as ch
+    if not (TUNER_DB.exists() and TUNER_DB.with_name(TUNER_DB.name + ".mlp").exists()):
+        raise RuntimeError("no trained cost model committed at chai_b200/data/tuner.db")
+    n_eval = getattr(args, "tuner_eval_keys", 0) or TUNER_EVAL_KEYS
+    held_keys = T.shapes(2200, seed=13)[2000:2000 + n_eval]
+    held, _ = T.collect(ctx, held_keys)
+    with Clocks(torch.cuda.current_device()) as clk:
+        dev = ch.Device(config="TuneDB=%s TopK=2" % TUNER_DB)
+        try:
+            rows = T.evaluate(dev.ctx, held)
+        finally:
+            dev.close()
+    gm = lambda v: float(np.exp(np.mean(np.log(v)))) if len(v) else None
+    q = np.array([r["best_us"] / r["pick_us"] for r in rows])
+    qd = np.array([r["best_us"] / r["default_us"] for r in rows])
+    ls = sum(r["learned_s"] for r in rows)
+    es = sum(r["exhaustive_s"] for r in rows)
+    return {
+        "metric": "tune time learned vs exhaustive", "unit": "x (cold-start speedup)", "value": es / ls,
+        "ms_per_step": 1e3 * ls / len(rows), "steps": len(rows), "dtype": "f32/bf16", "higher_is_better": True,
+        "config": {"workload": "learned GEMM/GEMV tuner, committed cost model, %d of the 200 held-out keys "
+                               "(M,N,K log-uniform [64,16384], seed 13), top 2 timed" % len(rows)},
+        "tuner": {"pick_vs_best_geomean": gm(q), "within_5pct": float(np.mean(q >= 1 / 1.05)),
+                  "default_vs_best_geomean": gm(qd), "learned_s_total": ls, "exhaustive_s_total": es},
         "e2e": None, "roofline": None, "clocks": clk.summary(), "gpu_launches": None,
     }
 
 
+TUNER_EVAL_KEYS = 40
+
+
 WORKLOADS = {"gemm": run_gemm, "mc": run_mc, "mc-hbm": run_mc_hbm, "kirsch": run_kirsch, "gemv": run_gemv,
-             "mc-many": run_mc_many, "grouped": run_grouped, "tuner": run_tuner, "c1": run_c1}
+             "mc-many": run_mc_many, "grouped": run_grouped, "tuner": run_tuner, "c1": run_c1,
+             "tuner-eval": run_tuner_eval}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -910,7 +996,7 @@ def run_reference(args, steps=None):
         return {"impl": "reference", "unavailable": "oracle/_ref/ref_driver not built (reference sources absent)"}
     steps = steps or max(1, args.steps)
     wl = args.workload
-    if wl == "tuner":
+    if wl in ("tuner", "tuner-eval"):
         return {"impl": "reference", "unavailable": "the reference tuner (StandardEM over generated OpenCL "
                                                    "kernels) needs an OpenCL GPU device; none on this host"}
     times = []
@@ -1020,6 +1106,44 @@ def cpu_baseline(args):
 
 # ---------------------------------------------------------------- main
 
+# The other parts of the benchmark metric, measured in the default run after
+# the headline GEMM: trace HBM GB/s (materialised MC, Kirsch), the fused MC
+# trace (issue-bound), the 64 uneven traces, the grouped GEMM, GEMV f32 / f64,
+# the C1 trace and the learned tuner's held-out evaluation.  Each timed region
+# lasts at least SECONDARY_MIN_S seconds so the clock sampler records it.
+SECONDARY = [("mc_hbm", "mc-hbm", {}), ("kirsch", "kirsch", {}), ("mc", "mc", {}), ("mc_many", "mc-many", {}),
+             ("grouped", "grouped", {"precision": "bf16x3"}), ("gemv_f32", "gemv", {"precision": "f32"}),
+             ("gemv_f64", "gemv", {"precision": "f64"}), ("c1", "c1", {}), ("tuner", "tuner-eval", {})]
+SECONDARY_MIN_S = 1.2
+
+
+def secondary(args, L, ctx, stream):
+    import torch
+    out = {}
+    for key, wl, over in SECONDARY:
+        a = argparse.Namespace(**vars(args))
+        a.workload, a.size, a.precision, a.min_timed_s = wl, 0, "bf16x3", SECONDARY_MIN_S
+        for k, v in over.items():
+            setattr(a, k, v)
+        t0 = time.perf_counter()
+        try:
+            r = WORKLOADS[wl](a, L, ctx, stream)
+        except Exception as e:          # one failed part must not hide the others
+            out[key] = {"error": "%s: %s" % (type(e).__name__, str(e)[:300])}
+            continue
+        finally:
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+        item = {k: r.get(k) for k in ("metric", "value", "unit", "ms_per_step", "steps", "dtype", "e2e", "roofline",
+                                     "clocks", "gpu_launches", "tuner") if r.get(k) is not None}
+        item["config"] = r.get("config")
+        if not args.no_cpu_baseline and wl != "tuner-eval":
+            item["cpu_baseline"] = cpu_baseline(a)
+        item["wall_s"] = time.perf_counter() - t0
+        out[key] = item
+    return out
+
+
 def aggregate_ranks(res, world, reduce_max):
     """Whole-job figures from one rank's result under weak scaling: every rank
     processes the same per-GPU workload, the job's step time is the maximum
@@ -1043,6 +1167,10 @@ def main():
     ap.add_argument("--size", type=int, default=0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--save-db", action="store_true",
+                    help="tuner: write the trained cost model to chai_b200/data/tuner.db")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="default run: skip the secondary measurements after the headline GEMM")
     ap.add_argument("--config", default=None, help="back-end configuration string (chai_cuda_init)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -1095,6 +1223,8 @@ def main():
             line["tuner"] = res["tuner"]
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args)
+        if world == 1 and args.workload == "gemm" and not args.no_secondary and not args.sweep:
+            line["secondary"] = secondary(args, L, dev.ctx, stream)
         print(json.dumps(line))
     if pg:
         pg.barrier()

@@ -140,7 +140,8 @@ void parse_config(chai::Config& c, const char* text)
         if (eq == std::string::npos) continue;   // devspec.cfg keywords without values
         const std::string k = tok.substr(0, eq), v = tok.substr(eq + 1);
         if (k == "GemmPrecision") {
-            if (v == "fp32") c.gemm_precision = CHAI_GEMM_FP32;
+            if (v == "auto") c.gemm_precision = CHAI_GEMM_AUTO;
+            else if (v == "fp32") c.gemm_precision = CHAI_GEMM_FP32;
             else if (v == "tf32") c.gemm_precision = CHAI_GEMM_TF32;
             else if (v == "bf16") c.gemm_precision = CHAI_GEMM_BF16;
             else if (v == "bf16x3") c.gemm_precision = CHAI_GEMM_BF16X3;

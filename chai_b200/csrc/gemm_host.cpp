@@ -112,7 +112,7 @@ extern "C" int chai_cuda_gemm_host(chai_cuda_ctx* ctx, const chai_gemm_desc* d, 
     if (d->m == 0 || d->n == 0) return CHAI_OK;
     if (!d->a || !d->b || !d->c || d->lda < d->k || d->ldb < d->n || d->ldc < d->n)
         return set_error(ctx, CHAI_ERR_INVALID, "gemm_host: bad operand pointers or leading dimensions");
-    const int prec = d->precision == CHAI_GEMM_AUTO ? ctx->cfg.gemm_precision : d->precision;
+    const int prec = resolve_precision(ctx, d->precision, d->m, d->n, d->k);
     const size_t es = prec == CHAI_GEMM_FP64 ? 8 : 4;
     const long long M = d->m, N = d->n, K = d->k;
     // about eight blocks, whole 128-row tiles

@@ -359,6 +359,7 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
     unsigned long long* tempty = bars + 2 * STAGES + 2;
     unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * STAGES + 4);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    unsigned long long* drain = bars + 2 * STAGES + 5;   // every MMA of this CTA complete (before dealloc)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntiles = tg.tiles_m * tg.tiles_n * tg.batch;
@@ -372,6 +373,7 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
             mbar_init(smem_u32(&tfull[a]), 1);
             mbar_init(smem_u32(&tempty[a]), 4);
         }
+        mbar_init(smem_u32(drain), 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -452,6 +454,10 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
                 }
                 mma_commit(smem_u32(&tfull[ab]));      // accumulator ab complete
             }
+            // Every MMA this thread issued must finish before TMEM is freed --
+            // also when a wait gave up and no accumulator commit was waited on
+            mma_commit(smem_u32(drain));
+            mbar_wait(smem_u32(drain), 0, status, 106);
         }
     } else {
         // ----------------------------------------------------------- epilogue
@@ -1106,6 +1112,7 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
     unsigned long long* tempty = bars + 6;                         // [2]
     unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 8);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    unsigned long long* drain = bars + 9;                          // every MMA complete (before dealloc)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long G = gridDim.x;
@@ -1116,6 +1123,7 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
             mbar_init(smem_u32(&tfull[b]), 1);
             mbar_init(smem_u32(&tempty[b]), 4);
         }
+        mbar_init(smem_u32(drain), 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -1178,6 +1186,9 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
                 }
                 mma_commit(smem_u32(&tfull[ab]));      // accumulator ab complete
             }
+            // Every MMA this thread issued must finish before TMEM is freed
+            mma_commit(smem_u32(drain));
+            mbar_wait(smem_u32(drain), 0, status, 116);
         }
     } else if (warp < 6) {
         // ----------------------------------------------------------- epilogue
@@ -1667,7 +1678,7 @@ int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_p
     const int BN = cfg.bn;
     if (count <= 0) return CHAI_OK;
     int prec = precision == CHAI_GEMM_AUTO ? ctx->cfg.gemm_precision : precision;
-    if (prec == CHAI_GEMM_FP32) prec = CHAI_GEMM_BF16X3;   // f32 accuracy on the tensor cores
+    if (prec == CHAI_GEMM_FP32 || prec == CHAI_GEMM_AUTO) prec = CHAI_GEMM_BF16X3;   // f32 accuracy on the tensor cores
     if (prec != CHAI_GEMM_BF16 && prec != CHAI_GEMM_BF16X3 && prec != CHAI_GEMM_BF16X6)
         return set_error(ctx, CHAI_ERR_UNSUPPORTED, "grouped gemm: bf16, bf16x3 or bf16x6");
     const int S = prec == CHAI_GEMM_BF16X3 ? 3 : prec == CHAI_GEMM_BF16X6 ? 6 : 1;

@@ -22,7 +22,7 @@ struct Buffer {
 };
 
 struct Config {
-    int gemm_precision = CHAI_GEMM_FP32;     // f32 matmul arithmetic
+    int gemm_precision = CHAI_GEMM_AUTO;     // f32 matmul arithmetic (AUTO: by shape, resolve_precision)
     double rng_pi = 3.14159;                 // M_PI as the reference JIT prints it
     int rng_layout = 0;                      // 0 chai, 1 counter
     int tuner_mode = CHAI_TUNE_LEARNED;
@@ -109,6 +109,8 @@ int launch_reduce(chai_cuda_ctx* ctx, uint32_t op, uint32_t prec, const void* a,
 int launch_gemv(chai_cuda_ctx* ctx, uint32_t prec, int trans, int64_t m, int64_t n, double alpha,
                 const void* a, int64_t lda, const void* x, double beta, void* y);
 int launch_gemm(chai_cuda_ctx* ctx, const chai_gemm_desc* d);
+// arithmetic of a CHAI_GEMM_AUTO f32 product of this shape (dispatch.cpp)
+int resolve_precision(chai_cuda_ctx* ctx, int precision, long long m, long long n, long long k);
 void host_gemm_release(chai_cuda_ctx* ctx);
 int launch_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gemm_problem* p, int32_t count);
 

@@ -55,22 +55,43 @@ int Jit::resolve()
     return CHAI_OK;
 }
 
-static std::string cache_path(const std::string& dir, uint64_t h)
+static std::string cache_path(const std::string& dir, uint64_t h, uint64_t h2)
 {
-    char buf[32];
-    snprintf(buf, sizeof buf, "%016llx", (unsigned long long)h);
+    char buf[48];
+    snprintf(buf, sizeof buf, "%016llx%016llx", (unsigned long long)h, (unsigned long long)h2);
     return dir + "/chai_" + buf + ".cubin";
+}
+
+// NVRTC options of every trace kernel.  --fmad=false: every traced operation
+// rounds on its own, as the reference interpreter's scalar functors do (no
+// multiply-add contraction).
+static const char* const kNvrtcOpts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-lineinfo",
+                                         "--fmad=false"};
+static const int kNvrtcNopts = (int)(sizeof kNvrtcOpts / sizeof kNvrtcOpts[0]);
+
+// What a compiled kernel depends on besides its source: the NVRTC version and
+// the options.  It seeds the on-disk cache key, so cubins built by another
+// NVRTC or with other options are never loaded.
+static uint64_t build_identity()
+{
+    int major = 0, minor = 0;
+    nvrtcVersion(&major, &minor);
+    std::string id = "nvrtc " + std::to_string(major) + "." + std::to_string(minor);
+    for (int i = 0; i < kNvrtcNopts; i++) (id += ' ') += kNvrtcOpts[i];
+    return fnv1a64(id.data(), id.size());
 }
 
 int Jit::get(const std::string& body, const char* name, void** fn)
 {
     int st = compile_only_ ? CHAI_OK : resolve();
     if (st) return st;
-    // the prelude is fixed for the life of the library: key on the body only
-    uint64_t h = fnv1a64(body.data(), body.size());
-    h = fnv1a64(name, strlen(name), h);
+    // the prelude is fixed for the life of the library: the in-memory key is
+    // the kernel name and the whole body (compared in full, not by hash)
+    std::string key(name);
+    key += '\0';
+    key += body;
     std::lock_guard<std::mutex> g(mu_);
-    auto it = functions_.find(h);
+    auto it = functions_.find(key);
     if (it != functions_.end()) {
         *fn = it->second;
         return CHAI_OK;
@@ -84,23 +105,22 @@ int Jit::get(const std::string& body, const char* name, void** fn)
     src += kChaiTracePreludeSrc;
     src += "\n";
     src += body;
-    // on-disk cache entries are keyed by the whole source (prelude included)
-    const uint64_t hdisk = fnv1a64(name, strlen(name), fnv1a64(src.data(), src.size()));
+    // on-disk cache entries are keyed by the NVRTC version and options and the
+    // whole source (prelude included), under two independent 64-bit hashes
+    static const uint64_t ident = build_identity();
+    const uint64_t hdisk = fnv1a64(name, strlen(name), fnv1a64(src.data(), src.size(), ident));
+    const uint64_t hdisk2 = fnv1a64(src.data(), src.size(), fnv1a64(name, strlen(name), ident ^ 0x9E3779B97F4A7C15ull));
     std::vector<char> cubin;
     const char* dir = compile_only_ ? nullptr : ctx_->cfg.jit_cache.empty() ? getenv("CHAI_JIT_CACHE") : ctx_->cfg.jit_cache.c_str();
     if (dir && *dir) {
-        std::ifstream f(cache_path(dir, hdisk), std::ios::binary);
+        std::ifstream f(cache_path(dir, hdisk, hdisk2), std::ios::binary);
         if (f) cubin.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
     }
     if (cubin.empty()) {
         nvrtcProgram prog;
         if (nvrtcCreateProgram(&prog, src.c_str(), "chai_trace.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
             return set_error(ctx_, CHAI_ERR_JIT, "nvrtcCreateProgram failed");
-        // --fmad=false: every traced operation rounds on its own, as the
-        // reference interpreter's scalar functors do (no multiply-add contraction)
-        const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-lineinfo",
-                              "--fmad=false"};
-        nvrtcResult r = nvrtcCompileProgram(prog, 5, opts);
+        nvrtcResult r = nvrtcCompileProgram(prog, kNvrtcNopts, kNvrtcOpts);
         if (r != NVRTC_SUCCESS) {
             size_t n = 0;
             nvrtcGetProgramLogSize(prog, &n);
@@ -120,8 +140,14 @@ int Jit::get(const std::string& body, const char* name, void** fn)
             return CHAI_OK;
         }
         if (dir && *dir) {
-            std::ofstream f(cache_path(dir, hdisk), std::ios::binary);
-            if (f) f.write(cubin.data(), (std::streamsize)cubin.size());
+            // write to a private name, then rename: a reader never sees a partial file
+            const std::string final_path = cache_path(dir, hdisk, hdisk2);
+            const std::string tmp = final_path + ".tmp" + std::to_string((unsigned long long)(uintptr_t)this);
+            {
+                std::ofstream f(tmp, std::ios::binary);
+                if (f) f.write(cubin.data(), (std::streamsize)cubin.size());
+            }
+            std::rename(tmp.c_str(), final_path.c_str());
         }
     }
     CUmodule mod;
@@ -130,8 +156,8 @@ int Jit::get(const std::string& body, const char* name, void** fn)
     CUfunction f;
     cr = reinterpret_cast<PFN_getfn>(p_getfn_)(&f, mod, name);
     if (cr != CUDA_SUCCESS) return set_error(ctx_, CHAI_ERR_JIT, std::string("kernel not found: ") + name);
-    modules_[h] = mod;
-    functions_[h] = f;
+    modules_[key] = mod;
+    functions_[key] = f;
     *fn = f;
     return CHAI_OK;
 }

@@ -1,11 +1,12 @@
 // Runtime specialisation of trace kernels.  A trace's fused element kernel is
 // a hand-written template (chai_trace_prelude) instantiated with the trace's
 // expression body; it is compiled once per distinct body for sm_100a with
-// NVRTC and cached in memory (and optionally on disk) by a 64-bit hash, the
-// way the reference caches OpenCL kernels by trace hash
-// (kernel/KernelCache.cpp:21-119) -- but the hash here covers every byte of
-// the generated source, so traces that differ only in a literal never share a
-// kernel (bytecode/HashBC.cpp:44-50 truncates literals to integers).
+// NVRTC and cached in memory (keyed by the whole generated source) and
+// optionally on disk (keyed by two 64-bit hashes of the source, the NVRTC
+// version and the options), the way the reference caches OpenCL kernels by
+// trace hash (kernel/KernelCache.cpp:21-119) -- but the key covers every byte
+// of the generated source, so traces that differ only in a literal never share
+// a kernel (bytecode/HashBC.cpp:44-50 truncates literals to integers).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -36,8 +37,8 @@ public:
 private:
     chai_cuda_ctx* ctx_;
     std::mutex mu_;
-    std::map<uint64_t, void*> modules_;     // hash -> CUmodule
-    std::map<uint64_t, void*> functions_;   // hash -> CUfunction
+    std::map<std::string, void*> modules_;     // name + body -> CUmodule
+    std::map<std::string, void*> functions_;   // name + body -> CUfunction
     size_t compiles_ = 0;
     bool compile_only_ = false;
     // driver entry points resolved through the runtime (no libcuda link)

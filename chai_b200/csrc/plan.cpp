@@ -47,18 +47,24 @@ void plan_key(const chai_trace_desc* t, const chai_buffer_binding* b, size_t nb,
         key.push_back(b[i].slots);
         key.push_back(ordinal(b[i].buffer));
     }
-    // inline kernels: program text, name, arguments, NDRange
-    auto text_hash = [](const char* p) -> uint64_t {
-        uint64_t h = 1469598103934665603ull;
-        for (; p && *p; p++) { h ^= (unsigned char)*p; h *= 1099511628211ull; }
-        return h;
+    // inline kernels: program text, name, arguments, NDRange.  The texts go
+    // into the key whole (length, then 8 bytes per word), so two programs
+    // never share a plan by a hash collision.
+    auto push_text = [&](const char* p) {
+        const size_t n = p ? strlen(p) : 0;
+        key.push_back(n);
+        for (size_t i = 0; i < n; i += 8) {
+            uint64_t w = 0;
+            memcpy(&w, p + i, std::min<size_t>(8, n - i));
+            key.push_back(w);
+        }
     };
     const uint32_t nk = t->kernels ? t->n_kernels : 0;
     key.push_back(nk);
     for (uint32_t k = 0; k < nk; k++) {
         const chai_inline_kernel& kd = t->kernels[k];
-        key.push_back(text_hash(kd.source));
-        key.push_back(text_hash(kd.name));
+        push_text(kd.source);
+        push_text(kd.name);
         key.push_back(kd.n_args);
         for (uint32_t a = 0; a < kd.n_args && kd.args; a++) {
             const chai_kernel_arg& g = kd.args[a];

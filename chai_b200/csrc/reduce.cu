@@ -180,9 +180,14 @@ int launch_many_combine(chai_cuda_ctx* ctx, const long long* tab, int stride, co
 //     left in it.  Each partial is written before it is read, so nothing has
 //     to start at zero -- but two calls whose kernels overlap on the GPU (on
 //     different streams without ordering between them) race on the array;
-//   - the first call on a device looks up the array's device address (once
-//     per device, with that device current); make that first call before any
-//     stream capture begins.
+//   - the first call in a CUDA context (normally the device's primary
+//     context, which the runtime API uses) looks up the array's device address
+//     in that context; make that first call before any stream capture begins.
+//     The address is remembered per context: a caller that makes its own
+//     driver-API context current gets the array's address in that context.
+//   - a launch failure is reported from this call's own launches
+//     (cudaLaunchKernel's return value); an error left pending by unrelated
+//     earlier work is neither reported as this call's nor cleared.
 #include <mutex>
 
 #define CHAI_NOALLOC_PARTIALS 8192
@@ -190,8 +195,63 @@ int launch_many_combine(chai_cuda_ctx* ctx, const long long* tab, int stride, co
 static __device__ __align__(256) double chai_noalloc_partials[CHAI_NOALLOC_PARTIALS];
 
 namespace {
+typedef int (*PFN_ctxGetCurrent)(void**);   // cuCtxGetCurrent (CUresult, CUcontext*)
+
 std::mutex g_noalloc_mu;
-double* g_noalloc_ptr[256] = {nullptr};
+struct NoallocSlot {
+    void* cu_ctx;
+    double* ptr;
+};
+NoallocSlot g_noalloc_slots[64];
+int g_noalloc_used = 0;
+PFN_ctxGetCurrent g_ctx_get = nullptr;
+
+void* current_cu_ctx()
+{
+    void* c = nullptr;
+    if (g_ctx_get && g_ctx_get(&c) != 0) c = nullptr;
+    return c;
+}
+
+// Device address of the partials array in the calling thread's current CUDA
+// context (looked up once per context, under g_noalloc_mu).
+double* noalloc_partials_ptr()
+{
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_ctx_get) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return nullptr;
+        g_ctx_get = reinterpret_cast<PFN_ctxGetCurrent>(fn);
+    }
+    void* c = current_cu_ctx();
+    for (int i = 0; c && i < g_noalloc_used; i++)
+        if (g_noalloc_slots[i].cu_ctx == c) return g_noalloc_slots[i].ptr;
+    void* p = nullptr;
+    // binds the primary context to this thread if no context is current
+    if (cudaGetSymbolAddress(&p, chai_noalloc_partials) != cudaSuccess || !p) return nullptr;
+    c = current_cu_ctx();
+    if (c) {
+        for (int i = 0; i < g_noalloc_used; i++)
+            if (g_noalloc_slots[i].cu_ctx == c) return g_noalloc_slots[i].ptr;
+        if (g_noalloc_used < 64) g_noalloc_slots[g_noalloc_used++] = {c, static_cast<double*>(p)};
+    }
+    return static_cast<double*>(p);
+}
+
+template <class T>
+cudaError_t noalloc_partials_launch(bool dot, dim3 grid, cudaStream_t s, const void* a, const void* b,
+                                    unsigned long long n, double* partials)
+{
+    const T* pa = static_cast<const T*>(a);
+    const T* pb = static_cast<const T*>(b);
+    void* args[] = {&pa, &pb, &n, &partials};
+    const void* fn = dot ? reinterpret_cast<const void*>(&chai::chai_reduce_partials<T, true>)
+                         : reinterpret_cast<const void*>(&chai::chai_reduce_partials<T, false>);
+    return cudaLaunchKernel(fn, grid, dim3(256), args, 0, s);
+}
 }  // namespace
 
 extern "C" int chai_cuda_reduce_noalloc(uint32_t op, uint32_t prec, const void* a, const void* b, uint64_t n,
@@ -203,42 +263,41 @@ extern "C" int chai_cuda_reduce_noalloc(uint32_t op, uint32_t prec, const void* 
     if (!eb) return CHAI_ERR_INVALID;
     if (slots > CHAI_NOALLOC_PARTIALS) return CHAI_ERR_UNSUPPORTED;   // more partials than the fixed array holds
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return CHAI_ERR_NO_DEVICE;
-    double* partials = nullptr;
-    {
-        std::lock_guard<std::mutex> g(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, chai_noalloc_partials) != cudaSuccess || !p) {
-                cudaGetLastError();
-                return CHAI_ERR_NO_DEVICE;
-            }
-            g_noalloc_ptr[dev] = static_cast<double*>(p);
-        }
-        partials = g_noalloc_ptr[dev];
-    }
+    if (cudaGetDevice(&dev) != cudaSuccess) return CHAI_ERR_NO_DEVICE;
+    double* partials = noalloc_partials_ptr();
+    if (!partials) return CHAI_ERR_NO_DEVICE;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const unsigned long long nv = (n * eb + 15) / 16;
     unsigned long long gx = std::min<unsigned long long>((nv + 255) / 256, (unsigned long long)sms * 8 / slots + 1);
+    // blocks x slots partials must fit the fixed array
     gx = std::min<unsigned long long>(gx, CHAI_NOALLOC_PARTIALS / slots);
     if (gx < 1) gx = 1;
     cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
-    dim3 grid((unsigned)gx, slots);
+    const dim3 grid((unsigned)gx, slots);
     const bool dot = op == 2;
-#define RNA(T) (dot ? chai_reduce_partials<T, true><<<grid, 256, 0, s>>>((const T*)a, (const T*)b, n, partials) \
-                    : chai_reduce_partials<T, false><<<grid, 256, 0, s>>>((const T*)a, (const T*)b, n, partials))
+    const unsigned long long nn = n;
+    cudaError_t e = cudaSuccess;
     switch (prec) {
-        case CHAI_F32: RNA(float); break;
-        case CHAI_F64: RNA(double); break;
-        case CHAI_I32: RNA(int); break;
-        case CHAI_U32: RNA(unsigned); break;
+        case CHAI_F32: e = noalloc_partials_launch<float>(dot, grid, s, a, b, nn, partials); break;
+        case CHAI_F64: e = noalloc_partials_launch<double>(dot, grid, s, a, b, nn, partials); break;
+        case CHAI_I32: e = noalloc_partials_launch<int>(dot, grid, s, a, b, nn, partials); break;
+        case CHAI_U32: e = noalloc_partials_launch<unsigned>(dot, grid, s, a, b, nn, partials); break;
     }
-#undef RNA
-    CombineArgs ca;
-    ca.outs[0] = device_out;
-    ca.precs[0] = CHAI_F64;
-    ca.scales[0] = op == 1 ? 1.0 / (double)n : 1.0;
-    chai_combine_partials<<<dim3(slots, 1), 256, 0, s>>>(partials, (int)gx, (int)slots, ca);
-    return cudaGetLastError() == cudaSuccess ? CHAI_OK : CHAI_ERR_LAUNCH;
+    if (e == cudaSuccess) {
+        CombineArgs ca;
+        ca.outs[0] = device_out;
+        ca.precs[0] = CHAI_F64;
+        ca.scales[0] = op == 1 ? 1.0 / (double)n : 1.0;     // n = 0: mean is 0/0 = NaN, sum and dot are 0
+        const double* cp = partials;
+        int nb = (int)gx, ns = (int)slots;
+        void* args[] = {&cp, &nb, &ns, &ca};
+        e = cudaLaunchKernel(reinterpret_cast<const void*>(&chai_combine_partials), dim3(slots, 1), dim3(256), args,
+                             0, s);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();          // this call's own launch error: do not leave it pending
+        return CHAI_ERR_LAUNCH;
+    }
+    return CHAI_OK;
 }

@@ -66,7 +66,9 @@ typedef struct chai_cuda_ctx chai_cuda_ctx;
  * `config` is the text of a device spec (devspec.cfg keywords are accepted and
  * ignored where meaningless on CUDA); recognised keys, one per line or
  * space-separated, `Key=Value`:
- *   GemmPrecision=fp32|tf32|bf16|bf16x3|bf16x6|fp8   f32 matmul arithmetic
+ *   GemmPrecision=auto|fp32|tf32|bf16|bf16x3|bf16x6|fp8   f32 matmul arithmetic
+ *                         (auto, the default: bf16x3 on the tensor cores for
+ *                         M, N >= 32 and K >= 16, FP32 CUDA cores otherwise)
  *   RngPi=<double>        constant inside Box-Muller (default 3.14159, the
  *                         value the reference JIT prints)
  *   RngLayout=chai|counter   key/counter placement (default chai)
@@ -239,7 +241,7 @@ enum {
     CHAI_GEMM_BF16X6 = 4,   /* fp32 split hi+mid+lo bf16, 6 products */
     CHAI_GEMM_FP8 = 5,      /* e4m3 with per-128x128-tile scales */
     CHAI_GEMM_FP64 = 6,     /* f64 operands (Arrayd64), CUDA-core DFMA */
-    CHAI_GEMM_AUTO = 7      /* context default (GemmPrecision) */
+    CHAI_GEMM_AUTO = 7      /* context default (GemmPrecision; auto: by shape) */
 };
 typedef struct chai_gemm_desc {
     int32_t  precision;         /* CHAI_GEMM_* */
@@ -301,8 +303,12 @@ int chai_cuda_reduce(chai_cuda_ctx* ctx, uint32_t op, uint32_t prec, const void*
  * fixed device array of 8192 doubles that every GPU loading the library keeps
  * until exit, so at most 8192 slots are accepted (CHAI_ERR_UNSUPPORTED
  * beyond).  All calls share that array: calls whose kernels overlap on the GPU
- * race.  The first call on a device looks up the array's address; make it
- * before any stream capture. */
+ * race.  The kernels run in the calling thread's current CUDA context (the
+ * device's primary context unless the caller made its own driver-API context
+ * current); the first call in a context looks up the array's address there,
+ * so make that first call before any stream capture.  n = 0 gives 0 for sum
+ * and dot_product and NaN (0/0) for mean.  CHAI_ERR_LAUNCH reports a failure
+ * of this call's own launches only. */
 int chai_cuda_reduce_noalloc(uint32_t op, uint32_t prec, const void* a, const void* b, uint64_t n,
                              uint32_t slots, double* device_out, void* cuda_stream);
 

@@ -29,7 +29,16 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF = Path(os.environ.get("CHAI_REFERENCE", "/root/reference"))
+# The reference checkout: the CHAI_REFERENCE environment variable or
+# set_reference() (the command line's --reference).  There is no built-in
+# default; without one, only the oracle's own restatement is built.
+_ref_env = os.environ.get("CHAI_REFERENCE")
+REF = Path(_ref_env) if _ref_env else None
+
+
+def set_reference(path) -> None:
+    global REF
+    REF = Path(path) if path else None
 
 # Directory order of the reference's top-level Makefile `all` target
 # (Makefile:3-24), minus tools_ (CLI programs) and with vendor built from
@@ -58,7 +67,7 @@ def _run(cmd: list[str]) -> None:
 
 
 def available() -> bool:
-    return (REF / "api" / "chai.h").exists()
+    return REF is not None and (REF / "api" / "chai.h").exists()
 
 
 def build(force: bool = False) -> Path:
@@ -281,6 +290,8 @@ def build_oracle() -> Path:
 
 
 if __name__ == "__main__":
+    if "--reference" in sys.argv:
+        set_reference(sys.argv[sys.argv.index("--reference") + 1])
     build_oracle()
     build(force="--force" in sys.argv)
     build_r123_pins(force="--force" in sys.argv)

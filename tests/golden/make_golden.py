@@ -1,9 +1,11 @@
 """Generate the golden fixtures in this directory from the reference itself.
 
-Run in a checkout that has the reference sources (the oracle recipe
-oracle/build_ref.py compiles them into oracle/_ref/):
+Run with the reference checkout named (the oracle recipe oracle/build_ref.py
+compiles its sources into oracle/_ref/):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference <reference checkout>
+
+(or CHAI_REFERENCE=<reference checkout> in the environment).
 
 Fixtures (numpy .npz, a few hundred KB in all):
   r123_bijections.npz  Philox2x32/4x32/2x64 and Threefry2x32/4x32/2x64 outputs
@@ -164,6 +166,10 @@ def _interp(rng):
 
 
 def main():
+    if "--reference" in sys.argv:
+        build_ref.set_reference(sys.argv[sys.argv.index("--reference") + 1])
+    if not build_ref.available():
+        raise SystemExit("name the reference checkout: --reference PATH or CHAI_REFERENCE")
     build_ref.build_all()
     rng = np.random.default_rng(20240613)
     np.savez_compressed(HERE / "r123_bijections.npz", **_bijections(rng))

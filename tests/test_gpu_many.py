@@ -1,11 +1,17 @@
 """Many uneven traces in one persistent launch under a CUDA graph
-(chai_cuda_evaluate_many) against the same traces evaluated one at a time.
+(chai_cuda_evaluate_many) against the oracle (the same payoff computed on the
+oracle's normals, Random123/R123Philox.cpp restated in oracle/r123.c) and
+against the same traces evaluated one at a time.
 
-Tolerance: results are the reductions rounded to f32 (as read_scalar returns
-them); the two paths add FP64 partials in different orders, so they may
-differ by one f32 ulp."""
+Tolerances: against the oracle 1e-5 relative (f32 exp on the device against
+numpy's, averaged over each trace; an infinite payoff, from a u = 0 draw,
+must be infinite on both sides); against the single-trace path two f32 ulps
+(results are the reductions rounded to f32, as read_scalar returns them, and
+the two paths add FP64 partials in different orders)."""
 import numpy as np
 import pytest
+
+import oracle
 
 pytestmark = pytest.mark.gpu
 f32 = np.float32
@@ -28,13 +34,23 @@ def lengths(n, seed=7):
     return [int(4 * round(2.0 ** u / 4)) for u in rng.uniform(12, 22, n)]
 
 
-def test_many_uneven_mc_traces_match_single(chai_dev):
+def oracle_payoff(seed, W):
+    z = oracle.rng_fill(W, dist=1, seed=seed).astype(np.float32)
+    with np.errstate(over="ignore", invalid="ignore"):
+        s = f32(100) * np.exp(f32(0.03) + f32(0.2) * z)
+        return float(np.float32(np.maximum(s - f32(100), f32(0)).astype(np.float64).mean()))
+
+
+def test_many_uneven_mc_traces_match_oracle_and_single(chai_dev):
     import chai_b200.api as ch
     Ls = lengths(64)
     traces = [ch.record(lambda L=L, s=s: mc(ch, 1000 + s, L))[0] for s, L in enumerate(Ls)]
     got = ch.evaluate_many(traces)
     again = ch.evaluate_many(traces)          # graph replay
     assert np.array_equal(got, again)
+    for s, L in enumerate(Ls):
+        want = oracle_payoff(1000 + s, L)
+        assert got[s] == want or abs(got[s] - want) <= 1e-5 * abs(want), (s, L, got[s], want)
     for s, L in enumerate(Ls[:8] + Ls[-4:]):
         idx = Ls.index(L)
         want = float(mc(ch, 1000 + idx, L).read_scalar())
