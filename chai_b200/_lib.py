@@ -55,6 +55,11 @@ class chai_buffer_binding(C.Structure):
                 ("slots", C.c_uint32), ("reserved", C.c_uint32), ("buffer", C.c_uint64)]
 
 
+class chai_value_shape(C.Structure):
+    _fields_ = [("variable", C.c_uint32), ("version", C.c_uint32), ("prec", C.c_uint32), ("slots", C.c_uint32),
+                ("width", C.c_uint64), ("height", C.c_uint64)]
+
+
 class chai_rng_desc(C.Structure):
     _fields_ = [("variant", C.c_uint32), ("prec", C.c_uint32), ("dist", C.c_uint32), ("vec_len", C.c_uint32),
                 ("seed", C.c_uint64), ("width", C.c_uint64), ("height", C.c_uint64), ("slots", C.c_uint32),
@@ -102,9 +107,12 @@ SIGNATURES = {
     "chai_cuda_upload": (C.c_int, [P, C.c_uint64, P, C.c_size_t]),
     "chai_cuda_readback": (C.c_int, [P, C.c_uint64, P, C.c_size_t]),
     "chai_cuda_release": (C.c_int, [P, C.c_uint64]),
+    "chai_cuda_buffer_copy": (C.c_int, [P, C.c_uint64, C.c_uint64, C.c_size_t]),
     "chai_cuda_evaluate": (C.c_int, [P, C.POINTER(chai_trace_desc), C.POINTER(chai_buffer_binding), C.c_size_t]),
     "chai_cuda_trace_source": (C.c_int, [C.POINTER(chai_trace_desc), C.POINTER(chai_buffer_binding), C.c_size_t,
                                          C.c_char_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "chai_cuda_trace_shapes": (C.c_int, [C.POINTER(chai_trace_desc), C.POINTER(chai_buffer_binding), C.c_size_t,
+                                         C.POINTER(chai_value_shape), C.c_size_t, C.POINTER(C.c_size_t)]),
     "chai_cuda_evaluate_many": (C.c_int, [P, C.POINTER(C.POINTER(chai_trace_desc)), C.c_size_t,
                                           C.POINTER(C.c_double)]),
     "chai_cuda_rng_fill": (C.c_int, [P, C.POINTER(chai_rng_desc), P]),

@@ -357,6 +357,7 @@ int chai_cuda_buffer_info(chai_cuda_ctx* ctx, uint64_t id, void** device_ptr, si
 int chai_cuda_upload(chai_cuda_ctx* ctx, uint64_t id, const void* host, size_t bytes)
 {
     if (!ctx || (!host && bytes)) return CHAI_ERR_INVALID;
+    cudaSetDevice(ctx->device);
     int st = alloc_buffer(ctx, id, bytes);
     if (st) return st;
     Buffer* b = find_buffer(ctx, id);
@@ -370,11 +371,27 @@ int chai_cuda_upload(chai_cuda_ctx* ctx, uint64_t id, const void* host, size_t b
 int chai_cuda_readback(chai_cuda_ctx* ctx, uint64_t id, void* host, size_t bytes)
 {
     if (!ctx || (!host && bytes)) return CHAI_ERR_INVALID;
+    cudaSetDevice(ctx->device);         // client threads read back too
     Buffer* b = find_buffer(ctx, id);
     if (!b) return set_error(ctx, CHAI_ERR_NOT_FOUND, "readback: unknown id");
     if (bytes > b->bytes) return set_error(ctx, CHAI_ERR_INVALID, "readback larger than buffer");
     CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(host, b->ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     CHAI_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return CHAI_OK;
+}
+
+int chai_cuda_buffer_copy(chai_cuda_ctx* ctx, uint64_t dst, uint64_t src, size_t bytes)
+{
+    if (!ctx) return CHAI_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    Buffer* s = find_buffer(ctx, src);
+    if (!s) return set_error(ctx, CHAI_ERR_NOT_FOUND, "buffer_copy: unknown source id");
+    if (bytes > s->bytes) return set_error(ctx, CHAI_ERR_INVALID, "buffer_copy larger than the source");
+    void* sp = s->ptr;
+    int st = alloc_buffer(ctx, dst, bytes);
+    if (st) return st;
+    Buffer* d = find_buffer(ctx, dst);
+    if (bytes) CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(d->ptr, sp, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     return CHAI_OK;
 }
 
@@ -384,6 +401,7 @@ int chai_cuda_release(chai_cuda_ctx* ctx, uint64_t id)
     std::lock_guard<std::mutex> g(ctx->mem_mutex);
     auto it = ctx->buffers.find(id);
     if (it == ctx->buffers.end()) return set_error(ctx, CHAI_ERR_NOT_FOUND, "release: unknown id");
+    cudaSetDevice(ctx->device);         // client threads release too
     if (it->second.owned) cudaFreeAsync(it->second.ptr, ctx->stream);
     ctx->buffers.erase(it);
     return CHAI_OK;

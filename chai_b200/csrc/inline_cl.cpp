@@ -63,6 +63,10 @@ template <class T> __device__ __forceinline__ T mix(T x, T y, T a) { return x + 
 #define half_log log
 #define half_sqrt sqrt
 #define powr pow
+__device__ __forceinline__ double pown(double x, int n) { return pow(x, (double)n); }
+__device__ __forceinline__ float pown(float x, int n) { return powf(x, (float)n); }
+__device__ __forceinline__ double rootn(double x, int n) { return pow(x, 1.0 / n); }
+__device__ __forceinline__ float rootn(float x, int n) { return powf(x, 1.0f / n); }
 // ---- program text
 )cl";
 

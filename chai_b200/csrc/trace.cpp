@@ -407,14 +407,15 @@ int Translator::read_result(double* out)
     return CHAI_OK;
 }
 
-int Translator::run(const chai_trace_desc* t, const chai_buffer_binding* binds, size_t nb)
+// Steps 1-2 of a run: parse every statement into the node DAG, with the
+// bindings (input shapes) and inline kernels of the trace.
+int Translator::parse_all(const chai_trace_desc* t, const chai_buffer_binding* binds, size_t nb)
 {
     for (size_t i = 0; i < nb; i++) bindings_[binds[i].variable] = binds[i];
     slots_ = t->num_traces ? t->num_traces : 1;
     kernels_ = t->kernels;
     n_kernels_ = t->kernels ? t->n_kernels : 0;
-    int first_inline = -1;      // statement index of the first inline kernel
-    // 1-2: parse all statements
+    first_inline_ = -1;
     for (uint32_t i = 0; i < t->n_stmts; i++) {
         const chai_stmt& s = t->stmts[i];
         if (!s.cells || s.n_cells == 0) return fail(CHAI_ERR_INVALID, "empty statement");
@@ -431,7 +432,7 @@ int Translator::run(const chai_trace_desc* t, const chai_buffer_binding* binds, 
         } else if (nodes_[root].kind == Node::INLINE) {
             // the kernel updates its array arguments in place: later statements
             // reading (variable, version) see the values after the kernel
-            if (first_inline < 0) first_inline = (int)stmt_roots_.size();
+            if (first_inline_ < 0) first_inline_ = (int)stmt_roots_.size();
             stmt_roots_.push_back(std::make_pair(s.lhs_variable, root));
             const chai_inline_kernel& kd = kernels_[nodes_[root].buffer];
             size_t m = 0;
@@ -453,8 +454,18 @@ int Translator::run(const chai_trace_desc* t, const chai_buffer_binding* binds, 
             assigned_[std::make_pair(s.lhs_variable, s.lhs_version)] = root;
             latest_[s.lhs_variable] = root;
             stmt_roots_.push_back(std::make_pair(s.lhs_variable, root));
+            stmt_values_.push_back({s.lhs_variable, s.lhs_version, (uint32_t)nodes_[root].prec,
+                                    nodes_[root].slots, nodes_[root].W, nodes_[root].H});
         }
     }
+    return CHAI_OK;
+}
+
+int Translator::run(const chai_trace_desc* t, const chai_buffer_binding* binds, size_t nb)
+{
+    int pst = parse_all(t, binds, nb);
+    if (pst) return pst;
+    const int first_inline = first_inline_;      // statement index of the first inline kernel
     // 3: materialisation
     materialize_.assign(nodes_.size(), false);
     for (size_t i = 0; i < nodes_.size(); i++) {
@@ -575,11 +586,16 @@ int Translator::assign_storage(int i)
         note_buffer(n.buffer, node_bytes(n), false);
         return CHAI_OK;
     }
-    // the node is the final value of a bound variable -> its buffer
+    // the node is the final value of a bound variable -> its buffer.  Not when
+    // that variable is also an input of this trace: its buffer then holds the
+    // input, which a GEMM, a gather or a later kernel of this trace may still
+    // read, so the value goes to a temporary and is copied into the buffer
+    // after the last kernel (run(), bound outputs that alias another node).
     for (auto& kv : latest_) {
         if (kv.second != i) continue;
         auto b = bindings_.find(kv.first);
         if (b == bindings_.end()) continue;
+        if (inputs_.count(kv.first)) break;
         int st = alloc_buffer(ctx_, b->second.buffer, node_bytes(n));
         if (st) return st;
         note_buffer(b->second.buffer, node_bytes(n), true);

@@ -50,6 +50,10 @@ public:
     explicit Translator(chai_cuda_ctx* ctx, bool dry = false) : ctx_(ctx), dry_(dry) {}
     ~Translator();
     int run(const chai_trace_desc* t, const chai_buffer_binding* b, size_t nb);
+    // steps 1-2 of run(): parse the statements with the bindings' input shapes
+    int parse_all(const chai_trace_desc* t, const chai_buffer_binding* b, size_t nb);
+    // after parse_all(): the value each assignment statement produces, in order
+    const std::vector<chai_value_shape>& statement_values() const { return stmt_values_; }
     // parse the statements only (no bindings, storage or launches)
     int parse_only(const chai_trace_desc* t);
     // root node of the last assignment when it is a reduction, else -1
@@ -80,6 +84,8 @@ private:
     std::map<uint32_t, int> inputs_;
     std::map<std::string, int> cse_;
     std::vector<std::pair<uint32_t, int>> stmt_roots_;
+    std::vector<chai_value_shape> stmt_values_;
+    int first_inline_ = -1;
     std::vector<int> reads_;
     std::vector<bool> materialize_;
     std::vector<void*> temps_;

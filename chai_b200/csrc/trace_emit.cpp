@@ -846,3 +846,18 @@ extern "C" int chai_cuda_trace_source(const chai_trace_desc* t, const chai_buffe
     }
     return st;
 }
+
+extern "C" int chai_cuda_trace_shapes(const chai_trace_desc* t, const chai_buffer_binding* b, size_t nb,
+                                      chai_value_shape* out, size_t cap, size_t* count)
+{
+    if (!t || (!t->stmts && t->n_stmts) || (!b && nb) || (!out && cap)) return CHAI_ERR_INVALID;
+    chai_cuda_ctx ctx;
+    ctx.device = -1;
+    Translator tr(&ctx, true);
+    int st = tr.parse_all(t, b, nb);
+    if (st) return st;
+    const std::vector<chai_value_shape>& v = tr.statement_values();
+    if (count) *count = v.size();
+    for (size_t i = 0; i < v.size() && i < cap; i++) out[i] = v[i];
+    return CHAI_OK;
+}

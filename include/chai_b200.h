@@ -118,6 +118,11 @@ int chai_cuda_upload(chai_cuda_ctx* ctx, uint64_t id, const void* host, size_t b
 /* Device -> host copy; waits for all work on the context that writes `id`. */
 int chai_cuda_readback(chai_cuda_ctx* ctx, uint64_t id, void* host, size_t bytes);
 int chai_cuda_release(chai_cuda_ctx* ctx, uint64_t id);
+/* Device -> device copy of `bytes` from buffer `src` into buffer `dst`
+ * (allocated when missing), ordered on the context stream: the copy the
+ * reference's memory manager makes when a value must survive an in-place
+ * update (memmgr/MemTrans.hpp:31-235). */
+int chai_cuda_buffer_copy(chai_cuda_ctx* ctx, uint64_t dst, uint64_t src, size_t bytes);
 
 /* ----------------------------------------------------------------- trace */
 
@@ -205,6 +210,22 @@ int chai_cuda_evaluate(chai_cuda_ctx* ctx, const chai_trace_desc* trace,
  * (NUL-terminated, truncated to `cap`); `needed` receives its full size. */
 int chai_cuda_trace_source(const chai_trace_desc* trace, const chai_buffer_binding* bindings,
                            size_t n_bindings, const char* config, char* out, size_t cap, size_t* needed);
+
+/* The value each assignment statement of a trace produces: its left-hand side
+ * and the precision, shape and slots of the right-hand side, in statement order
+ * (read-back statements and inline kernels produce none).  Input shapes come
+ * from `bindings`.  Parses only: needs no device, allocates and launches
+ * nothing.  A device adapter uses it to size the host memory of the variables
+ * a trace leaves live, as the reference's memory manager sizes the BackMem of
+ * a live variable (memmgr/MemTransPrivate.cpp:45-140).  `*count` receives the
+ * number of values; at most `cap` are written. */
+typedef struct chai_value_shape {
+    uint32_t variable, version;     /* the statement's left-hand side */
+    uint32_t prec, slots;
+    uint64_t width, height;
+} chai_value_shape;
+int chai_cuda_trace_shapes(const chai_trace_desc* trace, const chai_buffer_binding* bindings, size_t n_bindings,
+                           chai_value_shape* out, size_t cap, size_t* count);
 
 /* Many traces of uneven length in one persistent launch captured in a CUDA
  * graph.  All traces share one bytecode program (same hash, different W/H);

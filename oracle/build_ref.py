@@ -66,6 +66,16 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError("command failed: %s\n%s" % (" ".join(cmd), r.stderr[-4000:]))
 
 
+# Files compiled without optimisation and without unreachable traps:
+# ArrayBase::assignOther and ArrayBase::assignExp (api/ArrayBase.cpp:122-143)
+# return ArrayBase& but end without a return statement.  GCC 13 treats the end
+# of such a function as unreachable (a trap instruction at -O0, anything at
+# -O1 and above), so every `array = expression` assignment of a sample program
+# crashes.  At -O0 with -fno-unreachable-traps the function simply returns;
+# its callers (api/ArrayFP.cpp:42,49) ignore the value.
+O0_FILES = {("api", "ArrayBase.cpp")}
+
+
 def available() -> bool:
     return REF is not None and (REF / "api" / "chai.h").exists()
 
@@ -77,7 +87,8 @@ def build(force: bool = False) -> Path:
     lib = OUT / "libchai_ref.so"
     drv = OUT / "ref_driver"
     drv_src = HERE / "ref_driver.cpp"
-    if not force and lib.exists() and drv.exists() and drv.stat().st_mtime >= drv_src.stat().st_mtime:
+    if not force and lib.exists() and drv.exists() and drv.stat().st_mtime >= drv_src.stat().st_mtime and \
+            lib.stat().st_mtime >= HERE.joinpath("build_ref.py").stat().st_mtime:
         return OUT
     objdir = OUT / "obj"
     objdir.mkdir(parents=True, exist_ok=True)
@@ -96,10 +107,11 @@ def build(force: bool = False) -> Path:
     for d in DIRS:
         for src in _objects(REF / d):
             obj = objdir / (d + "__" + src.replace(".cpp", ".o"))
-            if force or not obj.exists():
-                jobs.append(["g++", "-c", *flags, *incs, str(REF / d / src), "-o", str(obj)])
-            else:
-                pass
+            if force or not obj.exists() or (d, src) in O0_FILES and obj.stat().st_mtime < HERE.joinpath(
+                    "build_ref.py").stat().st_mtime:
+                fl = [("-O0" if f == "-O2" else f) for f in flags] + ["-fno-unreachable-traps"] \
+                    if (d, src) in O0_FILES else flags
+                jobs.append(["g++", "-c", *fl, *incs, str(REF / d / src), "-o", str(obj)])
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         list(ex.map(_run, jobs))
     stub = objdir / "clstub.o"
@@ -267,6 +279,73 @@ def build_r123_wrapper_pins(force: bool = False) -> Path:
     return so
 
 
+# Reference sample programs run unchanged on the B200 through the reference's
+# own front end and chai_b200's CudaDevice (source file -> macros it needs).
+SAMPLES = {
+    "matmul_uni": "sample/matmul_uni.cpp", "matmul_vec": "sample/matmul_vec.cpp",
+    "matmul_pth": "sample/matmul_pth.cpp", "matmul64_uni": "sample/matmul64_uni.cpp",
+    "sum_uni": "sample/sum_uni.cpp", "sum_vec": "sample/sum_vec.cpp", "sum_pth": "sample/sum_pth.cpp",
+    "loopsum_uni": "sample/loopsum_uni.cpp", "loopsum_vec": "sample/loopsum_vec.cpp",
+    "cg": "sample/cg.cpp", "cg64": "sample/cg64.cpp", "index": "sample/index.cpp", "md5": "sample/md5.cpp",
+    "mingle": "sample/mingle.cpp", "filter": "sample/filter.cpp", "kirch": "sample/kirch.cpp",
+    "pi": "sample/pi.cpp", "inline_cl": "sample/inline_cl.cpp",
+    "american_option": "sample/finance/american_option.cpp",
+    "american_option_batch": "sample/finance/american_option_batch.cpp",
+    "bitonic": "sample/sorting/bitonic.cpp",
+}
+CUDA_OUT = OUT / "cuda"
+LIBCHAI_B200 = HERE.parent / "chai_b200" / "libchai_b200.so"
+
+
+def build_cuda_frontend(force: bool = False) -> Path:
+    """The reference's front end linked with chai_b200 through the CudaDevice
+    adapter (chai_b200/refdevice/): every reference object except
+    runtime/DeviceMap.cpp, whose place the adapter's DeviceMap.cpp takes, into
+    oracle/_ref/cuda/libchai_ref_cuda.so; then the reference's sample programs,
+    unchanged, linked against it (oracle/_ref/cuda/<sample>).  A sample runs on
+    the reference interpreter as usual, and on the B200 when CHAI_CUDA is set.
+    Needs the reference objects from build() and libchai_b200.so."""
+    build()
+    CUDA_OUT.mkdir(parents=True, exist_ok=True)
+    objdir = OUT / "obj"
+    inc = CUDA_OUT / "include" / "chai"
+    inc.mkdir(parents=True, exist_ok=True)
+    for name, d in dict(PUBLIC_HEADERS, **{"ParseArgs.hpp": "applib"}).items():
+        link = inc / name
+        if link.is_symlink() or link.exists():
+            link.unlink()
+        link.symlink_to(REF / d / name)
+    adapter = HERE.parent / "chai_b200" / "refdevice"
+    incs = ["-I" + str(adapter), "-I" + str(HERE.parent / "include"), "-I" + str(HERE / "clshim"),
+            "-I" + str(OUT / "include")] + ["-I" + str(REF / d) for d in DIRS]
+    flags = ["-O2", "-fPIC", "-fopenmp", "-w", "-std=gnu++98", "-include", "cstddef",
+             "-D_VENDOR_IS_NVIDIA_", "-D__STDC_LIMIT_MACROS"]
+    lib = CUDA_OUT / "libchai_ref_cuda.so"
+    srcs = [adapter / "CudaDevice.cpp", adapter / "DeviceMap.cpp"]
+    newest = max([x.stat().st_mtime for x in srcs + [adapter / "CudaDevice.hpp", HERE.parent / "include" /
+                                                      "chai_b200.h"]])
+    if force or not lib.exists() or lib.stat().st_mtime < newest:
+        objs = []
+        for src in srcs:
+            o = CUDA_OUT / (src.stem + ".o")
+            _run(["g++", "-c", *flags, *incs, str(src), "-o", str(o)])
+            objs.append(str(o))
+        ref_objs = sorted(str(x) for x in objdir.glob("*.o") if x.name != "runtime__DeviceMap.o")
+        rpath = "-Wl,-rpath,$ORIGIN/../../../chai_b200"
+        _run(["g++", "-shared", "-fopenmp", "-o", str(lib), *ref_objs, *objs, "-L" + str(LIBCHAI_B200.parent),
+              "-lchai_b200", rpath, "-lpthread"])
+    for name, rel in SAMPLES.items():
+        exe = CUDA_OUT / name
+        src = REF / rel
+        if not force and exe.exists() and exe.stat().st_mtime >= lib.stat().st_mtime:
+            continue
+        _run(["g++", "-O2", "-fopenmp", "-w", "-std=gnu++98", "-include", "cstddef", "-I" + str(CUDA_OUT / "include"),
+              "-I" + str(src.parent), str(src), "-o", str(exe), "-L" + str(CUDA_OUT), "-lchai_ref_cuda",
+              "-L" + str(LIBCHAI_B200.parent), "-lchai_b200", "-Wl,-rpath,$ORIGIN",
+              "-Wl,-rpath,$ORIGIN/../../../chai_b200", "-lpthread"])
+    return CUDA_OUT
+
+
 def build_all() -> None:
     """Everything the oracle pins need that this host can build."""
     build_oracle()
@@ -274,6 +353,8 @@ def build_all() -> None:
         build()
         build_r123_pins()
         build_r123_wrapper_pins()
+        if LIBCHAI_B200.exists():
+            build_cuda_frontend()
 
 
 def build_oracle() -> Path:

@@ -77,3 +77,39 @@ def test_null_arguments_are_invalid():
     assert lib.chai_cuda_evaluate(None, None, None, 0) == -1
     assert lib.chai_cuda_shutdown(None) == -1
     assert lib.chai_cuda_readback(None, 1, None, 0) == -1
+
+
+def test_c_consumer_struct_layout_matches_ctypes(tmp_path):
+    """tests/abi_layout.c, compiled as C99 against include/chai_b200.h, prints
+    every structure's size and field offsets; the ctypes binding must agree."""
+    from chai_b200 import _lib
+    exe = tmp_path / "abi_layout"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I" + str(ROOT / "include"),
+                    str(ROOT / "tests" / "abi_layout.c"), "-o", str(exe)], check=True)
+    lines = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    checked = 0
+    for ln in filter(None, lines):
+        name, val = ln.split()
+        if "." in name:
+            struct, field = name.split(".")
+            assert getattr(getattr(_lib, struct), field).offset == int(val), name
+        else:
+            assert C.sizeof(getattr(_lib, name)) == int(val), name
+        checked += 1
+    assert checked > 60
+
+
+def test_trace_shapes_without_a_device():
+    """chai_cuda_trace_shapes parses a trace and reports each assignment's
+    value (needs no GPU): make2 of a 3 x 5 f32 box, then s = sum(A * A)."""
+    from chai_b200 import _lib as L
+    import chai_b200.api as ch
+    cells_a = [ch._bc(L.BC_MEMORY, buffer=1), ch._sc(1), ch._sc(3), ch._sc(5), ch._op(66)]   # make2_f32
+    cells_s = [ch._bc(L.BC_VARIABLE, 7, 0), ch._bc(L.BC_VARIABLE, 7, 0), ch._op(13), ch._op(132), ch._op(3)]   # sum(a * a) -> f32
+    desc, keep = ch.build_desc([(7, 0, cells_a), (8, 0, cells_s)])
+    out = (L.chai_value_shape * 4)()
+    n = C.c_size_t(0)
+    st = L.lib().chai_cuda_trace_shapes(C.byref(desc), None, 0, out, 4, C.byref(n))
+    assert st == 0 and n.value == 2
+    assert (out[0].variable, out[0].prec, out[0].width, out[0].height, out[0].slots) == (7, L.F32, 5, 3, 1)
+    assert (out[1].variable, out[1].prec, out[1].width, out[1].height) == (8, L.F32, 1, 1)
