@@ -159,6 +159,8 @@ void parse_config(chai::Config& c, const char* text)
             c.stencil_rows = atoi(v.c_str());
         } else if (k == "StencilMinBlocks") {
             c.stencil_min_blocks = std::max(0, std::min(8, atoi(v.c_str())));
+        } else if (k == "GemmPair") {
+            c.gemm_pair = v != "0" && v != "off";
         } else if (k == "GroupedSplit") {
             c.grouped_fused = v != "prepass";
         } else if (k == "PackF32") {

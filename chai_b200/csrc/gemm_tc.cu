@@ -539,6 +539,364 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
     }
 }
 
+// ------------------------------------------------------- CTA-pair GEMM kernel
+//
+// chai_gemm_pair: tcgen05.mma.cta_group::2 over a cluster of two CTAs on two
+// SMs.  A pair tile is 256 x 256: each CTA stages its own 128 rows of A and its
+// own 128 rows (N) of B -- half of B per SM instead of all of it, so a stage is
+// 32 KiB per CTA and each SM's shared-memory reads per MMA fall by a third
+// against the one-CTA 128 x 256 tile.  The even CTA of the pair (the leader)
+// issues the MMAs; both CTAs' TMA copies complete on the leader's barrier
+// (.cta_group::2 copies, no multicast), and the MMA commits arrive on both
+// CTAs' barriers (tcgen05.commit multicast).  Each CTA holds its 128 rows of
+// the accumulator in its own TMEM and stores them.
+//
+// Split precisions (bf16x3 / bf16x6) keep a0*b0 and the correction products
+// in separate accumulators, and, unlike the one-CTA kernel, promote the a0*b0
+// accumulator into FP32 registers every SEG K chunks: the tensor core adds
+// each 16-deep product into the TMEM accumulator with its own rounding, whose
+// error builds up coherently over a long K; restarting the TMEM sum every
+// SEG chunks and adding the segment sums in the epilogue warps' registers
+// (round to nearest) keeps the result at FP32-FFMA accuracy.  Eight epilogue
+// warps per CTA (two per TMEM lane quarter, 128 columns each) hold the
+// running sums; they drain a segment while the MMA issues the correction
+// products of the same chunk, into the other accumulator.
+//
+// Barriers (per CTA; the leader's are the ones the MMA and the copies use):
+//   full[s]    leader: expect_tx of both CTAs' bytes + both CTAs' copies
+//   empty[s]   each CTA: the MMA commit of the stage (multicast)
+//   tfull[b]   each CTA: accumulator (or drain segment) ready (multicast commit)
+//   tempty[b]  leader: 16 epilogue warps (8 per CTA) done with it
+//   drain      leader: every MMA complete before TMEM is freed
+constexpr int PAIR_THREADS = 320;           // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+constexpr int PAIR_B_STAGE = 128 * KB_BYTES;
+constexpr int PAIR_SEG = 4;                 // K chunks per promotion segment (split precisions)
+
+template <int ST>
+struct PairShape {
+    static constexpr int SMEM_BYTES = ST * (A_STAGE + PAIR_B_STAGE) + 1024 + 256;
+};
+
+__device__ __forceinline__ unsigned cta_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ unsigned cluster_index()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ unsigned cluster_count()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+    return r;
+}
+
+// shared::cluster address of this CTA's shared address `a` in CTA `rank`
+__device__ __forceinline__ unsigned map_to_rank(unsigned a, unsigned rank)
+{
+    unsigned r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_cluster(unsigned cluster_addr)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
+// 3-D TMA copy into this CTA's shared memory, completing on the barrier at a
+// shared::cluster address (the pair leader's)
+__device__ __forceinline__ void tma_load_3d_pair(unsigned dst, const CUtensorMap* map, unsigned bar_cluster, int x,
+                                                 int y, int z)
+{
+    asm volatile("cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+                 "[%0], [%1, {%3, %4, %5}], [%2];"
+                 ::"r"(dst), "l"(map), "r"(bar_cluster), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
+template <int KIND>
+__device__ __forceinline__ void mma_pair(unsigned tmem, unsigned long long a, unsigned long long b, unsigned idesc,
+                                         unsigned accumulate)
+{
+    if (KIND == KIND_TF32)
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+                     ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+    else
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                     ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+// arrive (once the MMAs issued so far complete) on the barrier at this
+// shared offset in both CTAs of the pair
+__device__ __forceinline__ void mma_commit_pair(unsigned bar)
+{
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
+                 ::"r"(bar), "h"((unsigned short)3)
+                 : "memory");
+}
+
+// spin for `ns` nanoseconds (abort path: lets copies already in flight land)
+__device__ __forceinline__ void spin_ns(unsigned long long ns)
+{
+    const unsigned long long t0 = global_ns();
+    while (global_ns() - t0 < ns) { }
+}
+
+template <int KIND, int S, int ST>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
+chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b, int kchunks,
+               TileGrid tg, EpiArgs ep, int* status)
+{
+    constexpr bool SPLIT = S > 1;
+    constexpr int BN = 256;                                    // pair tile columns
+    constexpr unsigned TMEM_COLS = 512;                        // split: main + corr; plain: two accumulators
+    constexpr int NB = SPLIT ? 1 : 2;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* sa = smem;
+    unsigned char* sb = smem + ST * A_STAGE;
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(sb + ST * PAIR_B_STAGE);
+    unsigned long long* full = bars;
+    unsigned long long* empty = bars + ST;
+    unsigned long long* tfull = bars + 2 * ST;
+    unsigned long long* tempty = bars + 2 * ST + 2;
+    unsigned long long* drain = bars + 2 * ST + 4;
+    unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * ST + 5);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned rank = cta_rank();
+    const bool leader = rank == 0;
+    const int pair = (int)cluster_index(), npairs = (int)cluster_count();
+    const int ntiles = tg.tiles_m * tg.tiles_n * tg.batch;
+    // K blocks per tile: S product blocks per 64-element chunk
+    const int kblocks = kchunks * S;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ST; s++) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&tfull[b]), 1);
+            mbar_init(smem_u32(&tempty[b]), 16);
+        }
+        mbar_init(smem_u32(drain), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    // both CTAs' barriers initialised before either signals the other's
+    cluster_sync_all();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            long long it = 0, issued = 0;
+            const int kx_mul = KB_BYTES / (KIND == KIND_TF32 ? 4 : 2);
+            const unsigned full0 = map_to_rank(smem_u32(&full[0]), 0);     // the leader's full[0]
+            for (int t = pair; t < ntiles && !*abort_flag; t += npairs) {
+                int tm, tn, tb;
+                tile_coords(tg, t, tm, tn, tb);
+                const int arow = tm * 256 + (int)rank * 128, brow = tn * BN + (int)rank * 128;
+                for (int kb = 0; kb < kblocks; kb++, it++) {
+                    const int s = (int)(it % ST);
+                    const long long r = it / ST;
+                    if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (unsigned)((r - 1) & 1), status, 121)) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    if (leader) mbar_expect_tx(smem_u32(&full[s]), 2 * (A_STAGE + PAIR_B_STAGE));
+                    int xa = kb * kx_mul, xb = xa;
+                    if (SPLIT) {
+                        const int blk = kb % S, chunk = kb / S;
+                        const int sel = S == 3 ? 1 : 2;
+                        xa = kSelA[sel][blk] * tg.plane_k + chunk * kx_mul;
+                        xb = kSelB[sel][blk] * tg.plane_k + chunk * kx_mul;
+                    }
+                    const unsigned fb = full0 + (unsigned)(s * 8);
+                    tma_load_3d_pair(smem_u32(sa + s * A_STAGE), &map_a, fb, xa, arow, tb);
+                    tma_load_3d_pair(smem_u32(sb + s * PAIR_B_STAGE), &map_b, fb, xb, brow, tb);
+                    issued = it + 1;
+                }
+            }
+            if (leader) {
+                // every copy of both CTAs has landed once the last ST phases completed
+                for (long long j = issued - ST < 0 ? 0 : issued - ST; j < issued; j++)
+                    mbar_wait(smem_u32(&full[j % ST]), (unsigned)((j / ST) & 1), status, 122);
+            }
+            if (*abort_flag) spin_ns(1000000);   // abort: let the peer's copies in flight land
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------------------- MMA
+        if (leader && lane == 0) {
+            const unsigned idesc = instr_desc<KIND, BN>() & ~(31u << 24) | (16u << 24);   // M = 256
+            long long it = 0;
+            int lt = 0;
+            long long seg_no = 0;                       // promotion segments issued (split)
+            for (int t = pair; t < ntiles && !*abort_flag; t += npairs, lt++) {
+                const int ab = NB == 2 ? (lt & 1) : 0;
+                const unsigned acc_main = tmem + (unsigned)ab * BN;
+                const unsigned acc_corr = tmem + BN;
+                bool ok = true;
+                for (int c = 0; c < kchunks && ok; c++) {
+                    // the accumulator (split: the a0*b0 segment sum) is reused
+                    // once the epilogue warps of both CTAs have drained it
+                    const bool seg_start = SPLIT ? (c % PAIR_SEG == 0) : (c == 0);
+                    if (seg_start) {
+                        // split: drain number seg_no - 1; plain: use lt / 2 - 1 of buffer ab
+                        const long long prev = SPLIT ? seg_no - 1 : (long long)(lt >> 1) - 1;
+                        if (prev >= 0 && !mbar_wait(smem_u32(&tempty[SPLIT ? 0 : ab]), (unsigned)(prev & 1), status, 125)) {
+                            ok = false;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    }
+                    for (int blk = 0; blk < S; blk++, it++) {
+                        const int s = (int)(it % ST);
+                        if (!mbar_wait(smem_u32(&full[s]), (unsigned)((it / ST) & 1), status, 123)) {
+                            ok = false;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        const unsigned a0 = smem_u32(sa + s * A_STAGE), b0 = smem_u32(sb + s * PAIR_B_STAGE);
+                        const unsigned acc = blk == 0 ? acc_main : acc_corr;
+                        const bool first = blk == 0 ? seg_start : (c == 0 && blk == 1);
+#pragma unroll
+                        for (int k = 0; k < KB_BYTES / 32; k++)
+                            mma_pair<KIND>(acc, smem_desc(a0 + 32 * k), smem_desc(b0 + 32 * k), idesc,
+                                           !(first && k == 0));
+                        mma_commit_pair(smem_u32(&empty[s]));        // stage free in both CTAs
+                        if (SPLIT && blk == 0 && (c % PAIR_SEG == PAIR_SEG - 1) && c != kchunks - 1) {
+                            mma_commit_pair(smem_u32(&tfull[0]));    // segment sum ready to drain
+                            seg_no++;
+                        }
+                    }
+                }
+                if (!ok) {
+                    *abort_flag = 1;
+                    break;
+                }
+                mma_commit_pair(smem_u32(&tfull[ab]));               // tile complete (last segment + corrections)
+                if (SPLIT) seg_no++;
+            }
+            // every MMA complete before TMEM is freed
+            mma_commit_pair(smem_u32(drain));
+            mbar_wait(smem_u32(drain), 0, status, 126);
+        }
+    } else {
+        // ----------------------------------------------------------- epilogue
+        const int ew = warp - 2;                        // 0..7
+        const int quarter = warp & 3;                   // TMEM lanes 32 * quarter .. +31
+        const int half = ew >> 2;                       // columns 128 * half .. +127 of the tile
+        const unsigned tempty0 = map_to_rank(smem_u32(&tempty[0]), 0);
+        float run[SPLIT ? 128 : 1];
+        int lt = 0;
+        long long seg_no = 0;
+        for (int t = pair; t < ntiles; t += npairs, lt++) {
+            int tm, tn, tb;
+            tile_coords(tg, t, tm, tn, tb);
+            const int ab = NB == 2 ? (lt & 1) : 0;
+            const int row = tm * 256 + (int)rank * 128 + quarter * 32 + lane;
+            float* crow = ep.c + (long long)tb * ep.stride_c + (long long)row * ep.ldc;
+            const unsigned tbase = tmem + ((unsigned)(quarter * 32) << 16);
+            const int nseg = SPLIT ? (kchunks + PAIR_SEG - 1) / PAIR_SEG : 1;
+            bool ok = true;
+            for (int g = 0; g < nseg; g++) {
+                const long long wait_no = SPLIT ? seg_no : (long long)(lt >> 1);
+                ok = mbar_wait(smem_u32(&tfull[ab]), (unsigned)(wait_no & 1), status, 124);
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const bool last = g == nseg - 1;
+                const bool do_store = ok && !*abort_flag && last;
+#pragma unroll
+                for (int c0 = 0; c0 < 128; c0 += 32) {
+                    // warp-wide TMEM loads, always executed (lane checks come later)
+                    unsigned r0[32];
+                    tmem_ld32_nowait(tbase + (unsigned)(ab * BN + half * 128 + c0), r0);
+                    tmem_wait();
+                    if (SPLIT) {
+#pragma unroll
+                        for (int i = 0; i < 32; i++)
+                            run[c0 + i] = g == 0 ? __uint_as_float(r0[i]) : run[c0 + i] + __uint_as_float(r0[i]);
+                        if (!last) continue;
+                    }
+                    float v[32];
+                    if (SPLIT) {
+                        unsigned q0[32];
+                        tmem_ld32_nowait(tbase + (unsigned)(BN + half * 128 + c0), q0);
+                        tmem_wait();
+#pragma unroll
+                        for (int i = 0; i < 32; i++) v[i] = run[c0 + i] + __uint_as_float(q0[i]);
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r0[i]);
+                    }
+                    if (!do_store) continue;
+                    const int col = tn * BN + half * 128 + c0;
+                    if (row >= ep.m || col >= ep.n) continue;
+#pragma unroll
+                    for (int i = 0; i < 32; i++) v[i] *= ep.alpha;
+                    if (ep.vec_ok && col + 32 <= ep.n) {
+                        float4* p = reinterpret_cast<float4*>(crow + col);
+#pragma unroll
+                        for (int q = 0; q < 8; q++) {
+                            float4 o = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                            if (ep.beta != 0.0f) {
+                                const float4 old = p[q];
+                                o.x += ep.beta * old.x; o.y += ep.beta * old.y;
+                                o.z += ep.beta * old.z; o.w += ep.beta * old.w;
+                            }
+                            p[q] = o;
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 32; i++)
+                            if (col + i < ep.n) crow[col + i] = ep.beta != 0.0f ? v[i] + ep.beta * crow[col + i] : v[i];
+                    }
+                }
+                // drained: the leader's MMA may overwrite this accumulator
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive_cluster(tempty0 + (unsigned)(ab * 8));
+                if (SPLIT) seg_no++;
+                if (!ok || *abort_flag) break;
+            }
+            if (!ok || *abort_flag) break;
+        }
+        if (*abort_flag) spin_ns(1000000);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncwarp();
+    // neither CTA frees TMEM or exits while the other still signals it
+    cluster_sync_all();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
 // ------------------------------------------------------------------ prepass
 
 __device__ __forceinline__ void split3(float a, __nv_bfloat16 (&p)[3])
@@ -1353,6 +1711,27 @@ static int launch_variant(chai_cuda_ctx* ctx, const TcCfg& c, unsigned grid, con
     return CHAI_OK;
 }
 
+// Launch the CTA-pair kernel: 2 x min(pair tiles, SMs / 2) CTAs in clusters of two.
+template <int KIND, int S>
+static int launch_pair(chai_cuda_ctx* ctx, const TcCfg& c, const CUtensorMap& ma, const CUtensorMap& mb,
+                       int kchunks, const tc::TileGrid& tg, const tc::EpiArgs& ep)
+{
+    using namespace tc;
+    const long long ntiles = (long long)tg.tiles_m * tg.tiles_n * tg.batch;
+    const unsigned grid = 2u * (unsigned)std::min<long long>(ntiles, std::max(1, ctx->sm_count / 2));
+#define CHAI_PAIR_V(STV)                                                                                    \
+    do {                                                                                                    \
+        auto k = chai_gemm_pair<KIND, S, STV>;                                                              \
+        const int sm = PairShape<STV>::SMEM_BYTES;                                                          \
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                          \
+        k<<<grid, PAIR_THREADS, sm, ctx->stream>>>(ma, mb, kchunks, tg, ep, ctx->status_word);              \
+    } while (0)
+    if (c.stages >= 6) CHAI_PAIR_V(6); else CHAI_PAIR_V(4);
+#undef CHAI_PAIR_V
+    CHAI_CUDA_TRY(ctx, cudaGetLastError());
+    return CHAI_OK;
+}
+
 // rows x kelems (row-major, per batch `batch_stride` elements), box kbox x rbox
 static int make_map(chai_cuda_ctx* ctx, CUtensorMap* map, const void* base, CUtensorMapDataType dt, int esize,
                     long long kelems, long long rows, long long batch, long long batch_stride, int kbox, int rbox)
@@ -1536,7 +1915,11 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     // only the instantiated tile widths exist; the raster group needs >= 1 row
     if (cfg.bn != 128) cfg.bn = 256;
     cfg.group_m = std::max(1, std::min(cfg.group_m, 1 << 16));
-    st = make_map(ctx, &mb, Bp, dt, (int)esz, kp, N, batch, N * kp, kblk, cfg.bn);
+    // 256-row pair tiles on two SMs (cta_group::2) unless configured off; fp8
+    // and tiles whose whole M fits one 128-row CTA keep the one-CTA kernel
+    const bool pair = cfg.bm == 256 && ctx->cfg.gemm_pair && !fp8 && M > 128;
+    if (pair) cfg.bn = 256;
+    st = make_map(ctx, &mb, Bp, dt, (int)esz, kp, N, batch, N * kp, kblk, pair ? 128 : cfg.bn);
     if (st) return st;
     EpiArgs ep;
     ep.c = static_cast<float*>(d->c);
@@ -1552,6 +1935,25 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     ep.nb128 = (int)nb128;
     const int kblocks = (int)(S * kpad / kblk);            // product blocks the MMA walks
     TileGrid tg;
+    if (pair) {
+        tg.tiles_m = (int)((M + 255) / 256);
+        tg.tiles_n = (int)((N + 255) / 256);
+        tg.batch = (int)batch;
+        tg.group_m = cfg.group_m;
+        tg.plane_k = (int)kpad;
+        if ((long long)tg.tiles_m * tg.tiles_n * tg.batch > (1ll << 30))
+            return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: too many tiles");
+        const int kchunks = (int)(kpad / kblk);
+        cudaEvent_t ev[2];
+        ktime_begin(ctx, "gemm_tc", ev);
+        if (tf32) st = launch_pair<KIND_TF32, 1>(ctx, cfg, ma, mb, kchunks, tg, ep);
+        else if (S == 1) st = launch_pair<KIND_BF16, 1>(ctx, cfg, ma, mb, kchunks, tg, ep);
+        else if (S == 3) st = launch_pair<KIND_BF16, 3>(ctx, cfg, ma, mb, kchunks, tg, ep);
+        else st = launch_pair<KIND_BF16, 6>(ctx, cfg, ma, mb, kchunks, tg, ep);
+        if (st) return st;
+        ktime_end(ctx, "gemm_tc", ev);
+        return CHAI_OK;
+    }
     tg.tiles_m = (int)((M + BM - 1) / BM);
     tg.tiles_n = (int)((N + cfg.bn - 1) / cfg.bn);
     tg.batch = (int)batch;

@@ -33,6 +33,7 @@ struct Config {
     int stencil_rows = 32;                   // output rows per stencil tile (multiple of 8, <= 64)
     int stencil_min_blocks = 0;              // __launch_bounds__ minimum blocks per SM for stencil kernels (0: none)
     bool grouped_fused = true;               // grouped GEMM splits f32 operands inside the kernel (else prepass planes)
+    bool gemm_pair = true;                   // 256-row GEMM tiles on CTA pairs (cta_group::2) where configured
     bool pack_f32 = true;                    // element kernels issue f32 add / sub as packed f32x2 pairs
     std::string jit_cache;
 };

@@ -210,6 +210,7 @@ int Tuner::time_cfg(const chai_gemm_key& key, chai_gemm_cfg& c, int reps, bool w
         d.beta = 0.0;
         d.batch = 1;
         TcCfg t;
+        t.bm = c.block_m == 256 ? 256 : 128;
         t.bn = c.block_n;
         t.stages = c.stages;
         t.group_m = c.group_m;
@@ -395,6 +396,7 @@ bool tuned_tc_cfg(chai_cuda_ctx* ctx, long long m, long long n, long long k, int
         hit = ctx->tuner->lookup(&key, &c);
     }
     if (!hit) return false;
+    out->bm = c.block_m == 256 ? 256 : 128;
     out->bn = c.block_n;
     out->stages = c.stages;
     out->group_m = c.group_m;

@@ -14,10 +14,11 @@ struct chai_cuda_ctx;
 
 namespace chai {
 
-// tcgen05 GEMM tile configuration (gemm_tc.cu): N-tile width, pipeline
-// stages, tile-raster group height.
+// tcgen05 GEMM tile configuration (gemm_tc.cu): M-tile height (128: one CTA
+// per tile; 256: a CTA pair on two SMs, cta_group::2), N-tile width (one-CTA
+// tiles), pipeline stages, tile-raster group height.
 struct TcCfg {
-    int bn = 256, stages = 4, group_m = 16;
+    int bm = 256, bn = 256, stages = 4, group_m = 16;
 };
 inline TcCfg default_tc_cfg() { return TcCfg(); }
 bool tuned_tc_cfg(chai_cuda_ctx* ctx, long long m, long long n, long long k, int precision, TcCfg* out);

@@ -120,10 +120,15 @@ double oracle_sum_f32(int64_t n, const float* a)
     return acc;
 }
 
+/* dot_product of two f32 arrays as interp/InterpDotprod.cpp:14-60 computes
+ * it: each product in f32 (float * float), accumulated in double */
 double oracle_dot_f32(int64_t n, const float* a, const float* b)
 {
     double acc = 0.0;
-    for (int64_t i = 0; i < n; i++) acc += (double)a[i] * (double)b[i];
+    for (int64_t i = 0; i < n; i++) {
+        const float p = a[i] * b[i];
+        acc += (double)p;
+    }
     return acc;
 }
 
