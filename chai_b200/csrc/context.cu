@@ -161,6 +161,10 @@ void parse_config(chai::Config& c, const char* text)
             c.stencil_min_blocks = std::max(0, std::min(8, atoi(v.c_str())));
         } else if (k == "GemmPair") {
             c.gemm_pair = v != "0" && v != "off";
+        } else if (k == "GemmPairSeg") {
+            c.gemm_pair_seg = std::max(1, atoi(v.c_str()));
+        } else if (k == "GemmStages") {
+            c.gemm_stages = std::max(0, atoi(v.c_str()));
         } else if (k == "GroupedSplit") {
             c.grouped_fused = v != "prepass";
         } else if (k == "PackF32") {

@@ -570,7 +570,7 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
 //   drain      leader: every MMA complete before TMEM is freed
 constexpr int PAIR_THREADS = 320;           // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 constexpr int PAIR_B_STAGE = 128 * KB_BYTES;
-constexpr int PAIR_SEG = 4;                 // K chunks per promotion segment (split precisions)
+constexpr int PAIR_SEG = 4;                 // default K chunks per promotion segment (split precisions)
 
 template <int ST>
 struct PairShape {
@@ -660,7 +660,7 @@ __device__ __forceinline__ void spin_ns(unsigned long long ns)
 template <int KIND, int S, int ST>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
 chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b, int kchunks,
-               TileGrid tg, EpiArgs ep, int* status)
+               int seg, TileGrid tg, EpiArgs ep, int* status)
 {
     constexpr bool SPLIT = S > 1;
     constexpr int BN = 256;                                    // pair tile columns
@@ -764,7 +764,7 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
                 for (int c = 0; c < kchunks && ok; c++) {
                     // the accumulator (split: the a0*b0 segment sum) is reused
                     // once the epilogue warps of both CTAs have drained it
-                    const bool seg_start = SPLIT ? (c % PAIR_SEG == 0) : (c == 0);
+                    const bool seg_start = SPLIT ? (c % seg == 0) : (c == 0);
                     if (seg_start) {
                         // split: drain number seg_no - 1; plain: use lt / 2 - 1 of buffer ab
                         const long long prev = SPLIT ? seg_no - 1 : (long long)(lt >> 1) - 1;
@@ -789,7 +789,7 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
                             mma_pair<KIND>(acc, smem_desc(a0 + 32 * k), smem_desc(b0 + 32 * k), idesc,
                                            !(first && k == 0));
                         mma_commit_pair(smem_u32(&empty[s]));        // stage free in both CTAs
-                        if (SPLIT && blk == 0 && (c % PAIR_SEG == PAIR_SEG - 1) && c != kchunks - 1) {
+                        if (SPLIT && blk == 0 && (c % seg == seg - 1) && c != kchunks - 1) {
                             mma_commit_pair(smem_u32(&tfull[0]));    // segment sum ready to drain
                             seg_no++;
                         }
@@ -822,7 +822,7 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
             const int row = tm * 256 + (int)rank * 128 + quarter * 32 + lane;
             float* crow = ep.c + (long long)tb * ep.stride_c + (long long)row * ep.ldc;
             const unsigned tbase = tmem + ((unsigned)(quarter * 32) << 16);
-            const int nseg = SPLIT ? (kchunks + PAIR_SEG - 1) / PAIR_SEG : 1;
+            const int nseg = SPLIT ? (kchunks + seg - 1) / seg : 1;
             bool ok = true;
             for (int g = 0; g < nseg; g++) {
                 const long long wait_no = SPLIT ? seg_no : (long long)(lt >> 1);
@@ -1719,12 +1719,13 @@ static int launch_pair(chai_cuda_ctx* ctx, const TcCfg& c, const CUtensorMap& ma
     using namespace tc;
     const long long ntiles = (long long)tg.tiles_m * tg.tiles_n * tg.batch;
     const unsigned grid = 2u * (unsigned)std::min<long long>(ntiles, std::max(1, ctx->sm_count / 2));
+    const int seg = std::max(1, ctx->cfg.gemm_pair_seg);
 #define CHAI_PAIR_V(STV)                                                                                    \
     do {                                                                                                    \
         auto k = chai_gemm_pair<KIND, S, STV>;                                                              \
         const int sm = PairShape<STV>::SMEM_BYTES;                                                          \
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                          \
-        k<<<grid, PAIR_THREADS, sm, ctx->stream>>>(ma, mb, kchunks, tg, ep, ctx->status_word);              \
+        k<<<grid, PAIR_THREADS, sm, ctx->stream>>>(ma, mb, kchunks, seg, tg, ep, ctx->status_word);         \
     } while (0)
     if (c.stages >= 6) CHAI_PAIR_V(6); else CHAI_PAIR_V(4);
 #undef CHAI_PAIR_V
@@ -1912,6 +1913,7 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     TcCfg cfg = default_tc_cfg();
     if (cfg_in) cfg = *cfg_in;
     else tuned_tc_cfg(ctx, M, N, K, precision, &cfg);
+    if (ctx->cfg.gemm_stages > 0) cfg.stages = ctx->cfg.gemm_stages;
     // only the instantiated tile widths exist; the raster group needs >= 1 row
     if (cfg.bn != 128) cfg.bn = 256;
     cfg.group_m = std::max(1, std::min(cfg.group_m, 1 << 16));

@@ -34,6 +34,8 @@ struct Config {
     int stencil_min_blocks = 0;              // __launch_bounds__ minimum blocks per SM for stencil kernels (0: none)
     bool grouped_fused = true;               // grouped GEMM splits f32 operands inside the kernel (else prepass planes)
     bool gemm_pair = true;                   // 256-row GEMM tiles on CTA pairs (cta_group::2) where configured
+    int gemm_pair_seg = 4;                   // pair kernel, split precisions: K chunks per promotion segment
+    int gemm_stages = 0;                     // GEMM pipeline stages (0: tuned or default)
     bool pack_f32 = true;                    // element kernels issue f32 add / sub as packed f32x2 pairs
     std::string jit_cache;
 };

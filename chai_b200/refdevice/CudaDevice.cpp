@@ -26,6 +26,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #include <set>
 #include <utility>
@@ -203,7 +204,7 @@ public:
             if (written.count(variable))
             {
                 b.buffer = dev.newId();
-                if (chai_cuda_buffer_copy(ctx, b.buffer, r.id, bytes)) error = chai_cuda_last_error(ctx);
+                if (ctx && chai_cuda_buffer_copy(ctx, b.buffer, r.id, bytes)) error = chai_cuda_last_error(ctx);
                 scratch.push_back(b.buffer);
             }
             else
@@ -219,7 +220,7 @@ public:
             vector< char > dense;
             packBoxes(fm, slots, prec, W, H, dense);
             b.buffer = dev.newId();
-            if (chai_cuda_upload(ctx, b.buffer, dense.empty() ? NULL : &dense[0], dense.size()))
+            if (ctx && chai_cuda_upload(ctx, b.buffer, dense.empty() ? NULL : &dense[0], dense.size()))
                 error = chai_cuda_last_error(ctx);
             scratch.push_back(b.buffer);
         }
@@ -259,7 +260,7 @@ public:
             // make1 / make2: the box data (memalloc copied it into padded rows)
             vector< char > dense;
             packBoxes(boxes, slots, proto->prec(), proto->W(), proto->H(), dense);
-            if (chai_cuda_upload(ctx, id, dense.empty() ? NULL : &dense[0], dense.size()))
+            if (ctx && chai_cuda_upload(ctx, id, dense.empty() ? NULL : &dense[0], dense.size()))
                 error = chai_cuda_last_error(ctx);
         }
         else
@@ -384,12 +385,47 @@ bool Flattener::laterVersion(const uint32_t variable, uint32_t& version)
     return false;
 }
 
+// CHAI_CUDA_TRACE=1: each trace as the back end receives it, on stderr (the
+// counterpart of the reference's logged kernel source, kernel/KernelCache.cpp:82-89)
+void dumpTrace(const chai_trace_desc& d, const vector< chai_buffer_binding >& binds,
+               const vector< chai_value_shape >& shapes, size_t nshapes)
+{
+    fprintf(stderr, "trace %llx: %u statements, %u traces\n", (unsigned long long)d.hash, d.n_stmts, d.num_traces);
+    for (uint32_t i = 0; i < d.n_stmts; i++)
+    {
+        const chai_stmt& st = d.stmts[i];
+        fprintf(stderr, "  (%u,%u) =", st.lhs_variable, st.lhs_version);
+        for (uint32_t c = 0; c < st.n_cells; c++)
+        {
+            const chai_bc& b = st.cells[c];
+            switch (b.kind)
+            {
+                case CHAI_BC_OPCODE : fprintf(stderr, " op%u", b.code); break;
+                case CHAI_BC_VARIABLE : fprintf(stderr, " v%u.%u", b.code, b.version); break;
+                case CHAI_BC_SCALAR : fprintf(stderr, " %g", b.scalar); break;
+                case CHAI_BC_MEMORY : fprintf(stderr, " mem#%llu", (unsigned long long)b.buffer); break;
+                default : fprintf(stderr, " kernel#%llu", (unsigned long long)b.buffer); break;
+            }
+        }
+        fprintf(stderr, "\n");
+    }
+    for (size_t i = 0; i < binds.size(); i++)
+        fprintf(stderr, "  bind v%u prec %u %llux%llu x%u -> #%llu\n", binds[i].variable, binds[i].prec,
+                (unsigned long long)binds[i].width, (unsigned long long)binds[i].height, binds[i].slots,
+                (unsigned long long)binds[i].buffer);
+    for (size_t i = 0; i < nshapes && i < shapes.size(); i++)
+        fprintf(stderr, "  value v%u.%u prec %u %llux%llu x%u\n", shapes[i].variable, shapes[i].version,
+                shapes[i].prec, (unsigned long long)shapes[i].width, (unsigned long long)shapes[i].height,
+                shapes[i].slots);
+}
+
 } // namespace
 
 CudaDevice::CudaDevice(const int deviceNum, const string& config)
     : DeviceBase(deviceNum),
       _ctx(NULL),
-      _nextId(1ull << 40)
+      _nextId(1ull << 40),
+      _failures(0)
 {
     pthread_mutex_init(&_mtx, NULL);
     const int st = chai_cuda_init(deviceNum < 0 ? 0 : deviceNum, config.c_str(), &_ctx);
@@ -479,12 +515,19 @@ BackMem* CudaDevice::residentValue(const chai_value_shape& v, const uint64_t id,
 
 bool CudaDevice::sub_evaluate(VectorTrace& vt)
 {
-    if (!_ctx) return false;
+    const char* traceEnv = getenv("CHAI_CUDA_TRACE");
+    const bool dump = traceEnv && *traceEnv && traceEnv[0] != '0';
+    if (!_ctx && !dump) return fail("no CUDA context");
     const size_t n = vt.traceLength();
     const size_t slots = vt.numTraces() ? vt.numTraces() : 1;
 
+    // constructor and destructor records of the client trace are statements
+    // with no bytecode (ClientTrace constructor / destructor); the
+    // interpreter skips them (runtime/Interpreter.cpp:340-356) and so does
+    // this device
     set< uint32_t > written;
-    for (size_t i = 0; i < n; i++) written.insert(vt.getVariable(i));
+    for (size_t i = 0; i < n; i++)
+        if (vt.getRHS(i).size()) written.insert(vt.getVariable(i));
 
     vector< vector< chai_bc > >          cells(n);
     vector< chai_stmt >                  stmts(n);
@@ -501,6 +544,7 @@ bool CudaDevice::sub_evaluate(VectorTrace& vt)
                  kernelText);
     for (size_t i = 0; i < n && fl.error.empty(); i++)
     {
+        if (!vt.getRHS(i).size()) continue;
         fl.current = i;
         fl.cells = &cells[i];
         vt.getRHS(i).ascend(fl);
@@ -508,13 +552,16 @@ bool CudaDevice::sub_evaluate(VectorTrace& vt)
         latest[vt.getVariable(i)] = vt.getVersion(i);
     }
     bool good = fl.error.empty();
+    size_t ns = 0;
     for (size_t i = 0; i < n; i++)
     {
-        memset(&stmts[i], 0, sizeof stmts[i]);
-        stmts[i].lhs_variable = vt.getVariable(i);
-        stmts[i].lhs_version = vt.getVersion(i);
-        stmts[i].n_cells = (uint32_t)cells[i].size();
-        stmts[i].cells = cells[i].empty() ? NULL : &cells[i][0];
+        if (cells[i].empty()) continue;
+        memset(&stmts[ns], 0, sizeof stmts[ns]);
+        stmts[ns].lhs_variable = vt.getVariable(i);
+        stmts[ns].lhs_version = vt.getVersion(i);
+        stmts[ns].n_cells = (uint32_t)cells[i].size();
+        stmts[ns].cells = &cells[i][0];
+        ns++;
     }
     for (size_t k = 0; k < kernels.size(); k++)
     {
@@ -525,7 +572,7 @@ bool CudaDevice::sub_evaluate(VectorTrace& vt)
     chai_trace_desc desc;
     memset(&desc, 0, sizeof desc);
     desc.num_traces = (uint32_t)slots;
-    desc.n_stmts = (uint32_t)n;
+    desc.n_stmts = (uint32_t)ns;
     desc.stmts = stmts.empty() ? NULL : &stmts[0];
     desc.hash = vt.hashCode();
     desc.kernels = kernels.empty() ? NULL : &kernels[0];
@@ -535,7 +582,7 @@ bool CudaDevice::sub_evaluate(VectorTrace& vt)
     vector< chai_buffer_binding > binds;
     for (map< uint32_t, chai_buffer_binding >::const_iterator it = inputs.begin(); it != inputs.end(); it++)
         binds.push_back(it->second);
-    vector< chai_value_shape > shapes(n + 1);
+    vector< chai_value_shape > shapes(ns + 1);
     size_t nshapes = 0;
     if (good && chai_cuda_trace_shapes(&desc, binds.empty() ? NULL : &binds[0], binds.size(), &shapes[0],
                                        shapes.size(), &nshapes))
@@ -572,6 +619,12 @@ bool CudaDevice::sub_evaluate(VectorTrace& vt)
         binds.push_back(b);
     }
 
+    if (dump) dumpTrace(desc, binds, shapes, nshapes);
+    if (!_ctx)
+    {
+        fl.error = "no CUDA context";
+        good = false;
+    }
     if (good && chai_cuda_evaluate(_ctx, &desc, binds.empty() ? NULL : &binds[0], binds.size()))
     {
         fl.error = chai_cuda_last_error(_ctx);
@@ -607,15 +660,32 @@ bool CudaDevice::sub_evaluate(VectorTrace& vt)
         }
         unpackBoxes(dense, slots, rb.prec, rb.W, rb.H, rb.boxes);
     }
-    for (size_t k = 0; k < scratch.size(); k++)
-        if (scratch[k]) chai_cuda_release(_ctx, scratch[k]);
+    if (_ctx)
+        for (size_t k = 0; k < scratch.size(); k++)
+            if (scratch[k]) chai_cuda_release(_ctx, scratch[k]);
     if (!good)
     {
-        for (map< uint32_t, uint64_t >::const_iterator it = outId.begin(); it != outId.end(); it++)
-            chai_cuda_release(_ctx, it->second);
-        fprintf(stderr, "CudaDevice: trace %llx failed: %s\n", (unsigned long long)vt.hashCode(), fl.error.c_str());
+        if (_ctx)
+            for (map< uint32_t, uint64_t >::const_iterator it = outId.begin(); it != outId.end(); it++)
+                chai_cuda_release(_ctx, it->second);
+        return fail(fl.error);
     }
-    return good;
+    _failures = 0;
+    return true;
+}
+
+// A failed trace goes back to the scheduler's queue marked as failing on this
+// device (DEVICE_FAILURE, runtime/Scheduler.cpp:221-252, 300-378), which
+// never offers it to this device again.  With the CUDA device alone in the
+// table nothing else would take it and the client would wait for ever, so
+// the program stops with the reason.
+bool CudaDevice::fail(const string& why)
+{
+    fprintf(stderr, "CudaDevice: trace failed: %s\n", why.c_str());
+    ++_failures;
+    fflush(stderr);
+    _exit(70);          // no static destructors: the scheduler's threads are still running
+    return false;
 }
 
 void CudaDevice::swizzle(BackMem* m)

@@ -58,7 +58,9 @@ private:
     uint64_t                       _nextId;
     pthread_mutex_t                _mtx;        // _nextId, _resident (client threads swizzle / release)
     std::map< BackMem*, Resident > _resident;
+    int                            _failures;   // failed traces in a row
 
+    bool fail(const std::string& why);
     BackMem* residentValue(const chai_value_shape&, const uint64_t id, std::vector< FrontMem* >& fronts);
 };
 

@@ -36,7 +36,7 @@ def available() -> bool:
         (SAMPLE_DIR / s).exists() for s in INTERP_SAMPLES + CL_SAMPLES + ["pi"])
 
 
-def run(sample: str, cuda: bool, timeout: int = 120) -> str:
+def run(sample: str, cuda: bool, timeout: int = 60) -> str:
     spec = SAMPLE_DIR / "interp.spec"
     if not spec.exists():
         spec.write_text("EnableInterpreter\n")
