@@ -70,7 +70,7 @@ void ktime_begin(chai_cuda_ctx* ctx, const char* name, cudaEvent_t* ev)
 {
     (void)name;
     ev[0] = ev[1] = nullptr;
-    if (!ctx->kernel_timing) return;
+    if (!ctx->kernel_timing || ctx->capturing) return;
     for (int k = 0; k < 2; k++) {
         if (!ctx->event_pool.empty()) {
             ev[k] = ctx->event_pool.back();
@@ -121,6 +121,8 @@ int alloc_buffer(chai_cuda_ctx* ctx, uint64_t id, size_t bytes)
 int ensure_scratch(chai_cuda_ctx* ctx, size_t bytes)
 {
     if (ctx->scratch_bytes >= bytes) return CHAI_OK;
+    // a graph must not own the context scratch: growing it ends the capture
+    if (ctx->capturing) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "scratch growth during graph capture");
     const size_t want = bytes < (64u << 20) ? (64u << 20) : (bytes + (bytes >> 2));
     if (ctx->scratch) CHAI_CUDA_TRY(ctx, cudaFreeAsync(ctx->scratch, ctx->stream));
     ctx->scratch = nullptr;
@@ -171,6 +173,8 @@ void parse_config(chai::Config& c, const char* text)
             c.pack_f32 = v != "0" && v != "off";
         } else if (k == "PlanCache") {
             c.plan_cache = v != "0" && v != "off";
+        } else if (k == "PlanGraph") {
+            c.plan_graph = (v == "auto") ? -1 : (v != "0" && v != "off") ? 1 : 0;
         } else if (k == "TuneJournal") {
             c.tune_journal = v;
         } else if (k == "TuneDB") {
@@ -248,6 +252,9 @@ int chai_cuda_shutdown(chai_cuda_ctx* ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     many_release(ctx);
     host_gemm_release(ctx);
+    for (auto& kv : ctx->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    ctx->graphs.clear();
     ctx->tuner.reset();
     ctx->jit.reset();
     for (auto& kv : ctx->kstats)
@@ -275,6 +282,12 @@ int chai_cuda_kernel_stats(chai_cuda_ctx* ctx, const char* name, double* total_m
         if (total_ms) *total_ms = 0;
         if (launches) *launches = ctx->plan_hits;
         if (reset) ctx->plan_hits = 0;
+        return CHAI_OK;
+    }
+    if (std::string(name) == "plan_graph") {       // replays launched from a captured CUDA graph
+        if (total_ms) *total_ms = 0;
+        if (launches) *launches = ctx->graph_launches;
+        if (reset) ctx->graph_launches = 0;
         return CHAI_OK;
     }
     if (std::string(name) == "grouped_fused") {    // grouped GEMMs split inside the GEMM kernel
@@ -337,6 +350,7 @@ int chai_cuda_set_stream(chai_cuda_ctx* ctx, void* stream)
 int chai_cuda_buffer_alloc(chai_cuda_ctx* ctx, uint64_t id, size_t bytes)
 {
     if (!ctx) return CHAI_ERR_INVALID;
+    std::lock_guard<std::mutex> cap(ctx->capture_mutex);      // not inside another thread's capture
     return alloc_buffer(ctx, id, bytes);
 }
 
@@ -363,6 +377,7 @@ int chai_cuda_buffer_info(chai_cuda_ctx* ctx, uint64_t id, void** device_ptr, si
 int chai_cuda_upload(chai_cuda_ctx* ctx, uint64_t id, const void* host, size_t bytes)
 {
     if (!ctx || (!host && bytes)) return CHAI_ERR_INVALID;
+    std::lock_guard<std::mutex> cap(ctx->capture_mutex);      // not inside another thread's capture
     cudaSetDevice(ctx->device);
     int st = alloc_buffer(ctx, id, bytes);
     if (st) return st;
@@ -377,6 +392,7 @@ int chai_cuda_upload(chai_cuda_ctx* ctx, uint64_t id, const void* host, size_t b
 int chai_cuda_readback(chai_cuda_ctx* ctx, uint64_t id, void* host, size_t bytes)
 {
     if (!ctx || (!host && bytes)) return CHAI_ERR_INVALID;
+    std::lock_guard<std::mutex> cap(ctx->capture_mutex);      // not inside another thread's capture
     cudaSetDevice(ctx->device);         // client threads read back too
     Buffer* b = find_buffer(ctx, id);
     if (!b) return set_error(ctx, CHAI_ERR_NOT_FOUND, "readback: unknown id");
@@ -389,6 +405,7 @@ int chai_cuda_readback(chai_cuda_ctx* ctx, uint64_t id, void* host, size_t bytes
 int chai_cuda_buffer_copy(chai_cuda_ctx* ctx, uint64_t dst, uint64_t src, size_t bytes)
 {
     if (!ctx) return CHAI_ERR_INVALID;
+    std::lock_guard<std::mutex> cap(ctx->capture_mutex);      // not inside another thread's capture
     cudaSetDevice(ctx->device);
     Buffer* s = find_buffer(ctx, src);
     if (!s) return set_error(ctx, CHAI_ERR_NOT_FOUND, "buffer_copy: unknown source id");
@@ -404,6 +421,7 @@ int chai_cuda_buffer_copy(chai_cuda_ctx* ctx, uint64_t dst, uint64_t src, size_t
 int chai_cuda_release(chai_cuda_ctx* ctx, uint64_t id)
 {
     if (!ctx) return CHAI_ERR_INVALID;
+    std::lock_guard<std::mutex> cap(ctx->capture_mutex);      // not inside another thread's capture
     std::lock_guard<std::mutex> g(ctx->mem_mutex);
     auto it = ctx->buffers.find(id);
     if (it == ctx->buffers.end()) return set_error(ctx, CHAI_ERR_NOT_FOUND, "release: unknown id");

@@ -569,12 +569,14 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
 //   tempty[b]  leader: 16 epilogue warps (8 per CTA) done with it
 //   drain      leader: every MMA complete before TMEM is freed
 constexpr int PAIR_THREADS = 320;           // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
-constexpr int PAIR_B_STAGE = 128 * KB_BYTES;
 constexpr int PAIR_SEG = 4;                 // default K chunks per promotion segment (split precisions)
 
-template <int ST>
+// a pair tile is 256 x BN (BN = 128 or 256): each CTA stages 128 rows of A
+// and BN / 2 rows of B per K block
+template <int ST, int BN>
 struct PairShape {
-    static constexpr int SMEM_BYTES = ST * (A_STAGE + PAIR_B_STAGE) + 1024 + 256;
+    static constexpr int B_STAGE = (BN / 2) * KB_BYTES;
+    static constexpr int SMEM_BYTES = ST * (A_STAGE + B_STAGE) + 1024 + 256;
 };
 
 __device__ __forceinline__ unsigned cta_rank()
@@ -657,14 +659,16 @@ __device__ __forceinline__ void spin_ns(unsigned long long ns)
     while (global_ns() - t0 < ns) { }
 }
 
-template <int KIND, int S, int ST>
+template <int KIND, int S, int ST, int BNT>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 1)
 chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b, int kchunks,
                int seg, TileGrid tg, EpiArgs ep, int* status)
 {
     constexpr bool SPLIT = S > 1;
-    constexpr int BN = 256;                                    // pair tile columns
-    constexpr unsigned TMEM_COLS = 512;                        // split: main + corr; plain: two accumulators
+    constexpr int BN = BNT;                                    // pair tile columns
+    constexpr int HB = BN / 2;                                 // B rows per CTA; accumulator columns per epilogue warp
+    constexpr int PAIR_B_STAGE = PairShape<ST, BN>::B_STAGE;
+    constexpr unsigned TMEM_COLS = 2 * BN;                     // split: main + corr; plain: two accumulators
     constexpr int NB = SPLIT ? 1 : 2;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -720,7 +724,7 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
             for (int t = pair; t < ntiles && !*abort_flag; t += npairs) {
                 int tm, tn, tb;
                 tile_coords(tg, t, tm, tn, tb);
-                const int arow = tm * 256 + (int)rank * 128, brow = tn * BN + (int)rank * 128;
+                const int arow = tm * 256 + (int)rank * 128, brow = tn * BN + (int)rank * HB;
                 for (int kb = 0; kb < kblocks; kb++, it++) {
                     const int s = (int)(it % ST);
                     const long long r = it / ST;
@@ -810,9 +814,9 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
         // ----------------------------------------------------------- epilogue
         const int ew = warp - 2;                        // 0..7
         const int quarter = warp & 3;                   // TMEM lanes 32 * quarter .. +31
-        const int half = ew >> 2;                       // columns 128 * half .. +127 of the tile
+        const int half = ew >> 2;                       // columns HB * half .. +HB-1 of the tile
         const unsigned tempty0 = map_to_rank(smem_u32(&tempty[0]), 0);
-        float run[SPLIT ? 128 : 1];
+        float run[SPLIT ? HB : 1];
         int lt = 0;
         long long seg_no = 0;
         for (int t = pair; t < ntiles; t += npairs, lt++) {
@@ -831,10 +835,10 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
                 const bool last = g == nseg - 1;
                 const bool do_store = ok && !*abort_flag && last;
 #pragma unroll
-                for (int c0 = 0; c0 < 128; c0 += 32) {
+                for (int c0 = 0; c0 < HB; c0 += 32) {
                     // warp-wide TMEM loads, always executed (lane checks come later)
                     unsigned r0[32];
-                    tmem_ld32_nowait(tbase + (unsigned)(ab * BN + half * 128 + c0), r0);
+                    tmem_ld32_nowait(tbase + (unsigned)(ab * BN + half * HB + c0), r0);
                     tmem_wait();
                     if (SPLIT) {
 #pragma unroll
@@ -845,7 +849,7 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
                     float v[32];
                     if (SPLIT) {
                         unsigned q0[32];
-                        tmem_ld32_nowait(tbase + (unsigned)(BN + half * 128 + c0), q0);
+                        tmem_ld32_nowait(tbase + (unsigned)(BN + half * HB + c0), q0);
                         tmem_wait();
 #pragma unroll
                         for (int i = 0; i < 32; i++) v[i] = run[c0 + i] + __uint_as_float(q0[i]);
@@ -854,7 +858,7 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
                         for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r0[i]);
                     }
                     if (!do_store) continue;
-                    const int col = tn * BN + half * 128 + c0;
+                    const int col = tn * BN + half * HB + c0;
                     if (row >= ep.m || col >= ep.n) continue;
 #pragma unroll
                     for (int i = 0; i < 32; i++) v[i] *= ep.alpha;
@@ -1701,6 +1705,13 @@ static int launch_variant(chai_cuda_ctx* ctx, const TcCfg& c, unsigned grid, con
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                          \
         k<<<grid, THREADS, sm, ctx->stream>>>(ma, mb, kblocks, S, tg, ep, ctx->status_word, g, ng);         \
     } while (0)
+    if constexpr (!GROUPED) {
+        if (c.bn == 64) {
+            if (c.stages >= 8) CHAI_TC_V(64, 8); else if (c.stages >= 6) CHAI_TC_V(64, 6); else CHAI_TC_V(64, 4);
+            CHAI_CUDA_TRY(ctx, cudaGetLastError());
+            return CHAI_OK;
+        }
+    }
     if (c.bn == 128) {
         if (c.stages >= 6) CHAI_TC_V(128, 6); else CHAI_TC_V(128, 4);
     } else {
@@ -1720,14 +1731,18 @@ static int launch_pair(chai_cuda_ctx* ctx, const TcCfg& c, const CUtensorMap& ma
     const long long ntiles = (long long)tg.tiles_m * tg.tiles_n * tg.batch;
     const unsigned grid = 2u * (unsigned)std::min<long long>(ntiles, std::max(1, ctx->sm_count / 2));
     const int seg = std::max(1, ctx->cfg.gemm_pair_seg);
-#define CHAI_PAIR_V(STV)                                                                                    \
+#define CHAI_PAIR_V(STV, BNV)                                                                               \
     do {                                                                                                    \
-        auto k = chai_gemm_pair<KIND, S, STV>;                                                              \
-        const int sm = PairShape<STV>::SMEM_BYTES;                                                          \
+        auto k = chai_gemm_pair<KIND, S, STV, BNV>;                                                         \
+        const int sm = PairShape<STV, BNV>::SMEM_BYTES;                                                     \
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                          \
         k<<<grid, PAIR_THREADS, sm, ctx->stream>>>(ma, mb, kchunks, seg, tg, ep, ctx->status_word);         \
     } while (0)
-    if (c.stages >= 6) CHAI_PAIR_V(6); else CHAI_PAIR_V(4);
+    if (c.bn == 128) {
+        if (c.stages >= 8) CHAI_PAIR_V(8, 128); else if (c.stages >= 6) CHAI_PAIR_V(6, 128); else CHAI_PAIR_V(4, 128);
+    } else {
+        if (c.stages >= 6) CHAI_PAIR_V(6, 256); else if (c.stages >= 4) CHAI_PAIR_V(4, 256); else CHAI_PAIR_V(3, 256);
+    }
 #undef CHAI_PAIR_V
     CHAI_CUDA_TRY(ctx, cudaGetLastError());
     return CHAI_OK;
@@ -1759,6 +1774,21 @@ static void preload_variants()
     cudaFuncGetAttributes(&a, tc::chai_gemm_tc_kernel<KIND, SPLIT, false, 256, 4>);
     cudaFuncGetAttributes(&a, tc::chai_gemm_tc_kernel<KIND, SPLIT, false, 128, 4>);
     cudaFuncGetAttributes(&a, tc::chai_gemm_tc_kernel<KIND, SPLIT, false, 128, 6>);
+    cudaFuncGetAttributes(&a, tc::chai_gemm_tc_kernel<KIND, SPLIT, false, 64, 4>);
+    cudaFuncGetAttributes(&a, tc::chai_gemm_tc_kernel<KIND, SPLIT, false, 64, 6>);
+    cudaFuncGetAttributes(&a, tc::chai_gemm_tc_kernel<KIND, SPLIT, false, 64, 8>);
+}
+
+template <int KIND, int S>
+static void preload_pair()
+{
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, tc::chai_gemm_pair<KIND, S, 3, 256>);
+    cudaFuncGetAttributes(&a, tc::chai_gemm_pair<KIND, S, 4, 256>);
+    cudaFuncGetAttributes(&a, tc::chai_gemm_pair<KIND, S, 6, 256>);
+    cudaFuncGetAttributes(&a, tc::chai_gemm_pair<KIND, S, 4, 128>);
+    cudaFuncGetAttributes(&a, tc::chai_gemm_pair<KIND, S, 6, 128>);
+    cudaFuncGetAttributes(&a, tc::chai_gemm_pair<KIND, S, 8, 128>);
 }
 
 void preload_gemm_kernels()
@@ -1768,6 +1798,10 @@ void preload_gemm_kernels()
     preload_variants<KIND_BF16, false>();
     preload_variants<KIND_BF16, true>();
     preload_variants<KIND_FP8, false>();
+    preload_pair<KIND_TF32, 1>();
+    preload_pair<KIND_BF16, 1>();
+    preload_pair<KIND_BF16, 3>();
+    preload_pair<KIND_BF16, 6>();
     cudaFuncAttributes a;
     cudaFuncGetAttributes(&a, split_rows_bf16<1>);
     cudaFuncGetAttributes(&a, split_rows_bf16<3>);
@@ -1915,13 +1949,13 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     else tuned_tc_cfg(ctx, M, N, K, precision, &cfg);
     if (ctx->cfg.gemm_stages > 0) cfg.stages = ctx->cfg.gemm_stages;
     // only the instantiated tile widths exist; the raster group needs >= 1 row
-    if (cfg.bn != 128) cfg.bn = 256;
+    if (cfg.bn != 128 && cfg.bn != 64) cfg.bn = 256;
+    if (cfg.bm == 256 && cfg.bn == 64) cfg.bn = 128;
     cfg.group_m = std::max(1, std::min(cfg.group_m, 1 << 16));
     // 256-row pair tiles on two SMs (cta_group::2) unless configured off; fp8
     // and tiles whose whole M fits one 128-row CTA keep the one-CTA kernel
     const bool pair = cfg.bm == 256 && ctx->cfg.gemm_pair && !fp8 && M > 128;
-    if (pair) cfg.bn = 256;
-    st = make_map(ctx, &mb, Bp, dt, (int)esz, kp, N, batch, N * kp, kblk, pair ? 128 : cfg.bn);
+    st = make_map(ctx, &mb, Bp, dt, (int)esz, kp, N, batch, N * kp, kblk, pair ? cfg.bn / 2 : cfg.bn);
     if (st) return st;
     EpiArgs ep;
     ep.c = static_cast<float*>(d->c);
@@ -1939,7 +1973,7 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     TileGrid tg;
     if (pair) {
         tg.tiles_m = (int)((M + 255) / 256);
-        tg.tiles_n = (int)((N + 255) / 256);
+        tg.tiles_n = (int)((N + cfg.bn - 1) / cfg.bn);
         tg.batch = (int)batch;
         tg.group_m = cfg.group_m;
         tg.plane_k = (int)kpad;

@@ -281,11 +281,18 @@ static int gemv_t(chai_cuda_ctx* ctx, int trans, int64_t m, int64_t n, double al
 #define CHAI_GV(W, U)                                                                                       \
     chai_gemv_n<T, W, U><<<(unsigned)((m + W - 1) / W), W * 32, 0, ctx->stream>>>((const T*)a, lda, (const T*)x, \
                                                                                  (T*)y, m, n, (T)alpha, (T)beta)
+#define CHAI_GVU(W)                                                                                         \
+    do {                                                                                                    \
+        if (cfg.unroll >= 8) CHAI_GV(W, 8); else if (cfg.unroll >= 4) CHAI_GV(W, 4);                        \
+        else if (cfg.unroll >= 2) CHAI_GV(W, 2); else CHAI_GV(W, 1);                                        \
+    } while (0)
         if (m > 0) {
-            if (cfg.warps <= 4) { if (cfg.unroll >= 4) CHAI_GV(4, 4); else CHAI_GV(4, 1); }
-            else if (cfg.warps <= 8) { if (cfg.unroll >= 4) CHAI_GV(8, 4); else CHAI_GV(8, 1); }
-            else { if (cfg.unroll >= 4) CHAI_GV(16, 4); else CHAI_GV(16, 1); }
+            if (cfg.warps <= 2) CHAI_GVU(2);
+            else if (cfg.warps <= 4) CHAI_GVU(4);
+            else if (cfg.warps <= 8) CHAI_GVU(8);
+            else CHAI_GVU(16);
         }
+#undef CHAI_GVU
 #undef CHAI_GV
         ktime_end(ctx, "gemv", ev);
         CHAI_CUDA_TRY(ctx, cudaGetLastError());
@@ -323,12 +330,16 @@ template <class T>
 static void preload_gemv_t()
 {
     cudaFuncAttributes a;
-    cudaFuncGetAttributes(&a, chai_gemv_n<T, 4, 1>);
-    cudaFuncGetAttributes(&a, chai_gemv_n<T, 4, 4>);
-    cudaFuncGetAttributes(&a, chai_gemv_n<T, 8, 1>);
-    cudaFuncGetAttributes(&a, chai_gemv_n<T, 8, 4>);
-    cudaFuncGetAttributes(&a, chai_gemv_n<T, 16, 1>);
-    cudaFuncGetAttributes(&a, chai_gemv_n<T, 16, 4>);
+#define CHAI_GVP(W)                                                                                         \
+    cudaFuncGetAttributes(&a, chai_gemv_n<T, W, 1>);                                                        \
+    cudaFuncGetAttributes(&a, chai_gemv_n<T, W, 2>);                                                        \
+    cudaFuncGetAttributes(&a, chai_gemv_n<T, W, 4>);                                                        \
+    cudaFuncGetAttributes(&a, chai_gemv_n<T, W, 8>)
+    CHAI_GVP(2);
+    CHAI_GVP(4);
+    CHAI_GVP(8);
+    CHAI_GVP(16);
+#undef CHAI_GVP
 }
 
 // Load every GEMV variant now (see preload_gemm_kernels).

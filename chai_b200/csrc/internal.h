@@ -30,6 +30,7 @@ struct Config {
     std::string tune_db;
     std::string tune_journal;                // crash-safe TRY / OK markers of every timing
     bool plan_cache = true;                  // replay recorded plans of repeated traces
+    int plan_graph = -1;                     // replay plans from captured CUDA graphs: 1 on, 0 off, -1 unless kernel timing
     int stencil_rows = 32;                   // output rows per stencil tile (multiple of 8, <= 64)
     int stencil_min_blocks = 0;              // __launch_bounds__ minimum blocks per SM for stencil kernels (0: none)
     bool grouped_fused = true;               // grouped GEMM splits f32 operands inside the kernel (else prepass planes)
@@ -75,6 +76,13 @@ struct chai_cuda_ctx {
     std::vector<cudaEvent_t> event_pool;
     std::unordered_map<uint64_t, std::shared_ptr<chai::Plan>> plans;   // plan cache, by key hash
     uint64_t plan_hits = 0;
+    // captured CUDA graphs of replayed plans: plan key hash -> the device
+    // pointers the graph was captured with, and the executable graph
+    struct PlanGraph { std::vector<void*> sig; cudaGraphExec_t exec = nullptr; };
+    std::unordered_map<uint64_t, PlanGraph> graphs;
+    uint64_t graph_launches = 0;
+    bool capturing = false;                                 // a plan replay is being captured
+    std::mutex capture_mutex;                               // no client-thread stream work during a capture
     // grouped GEMM with the in-kernel split: the device tile records of the
     // last call, reused while the problem array repeats
     struct GroupedPlan {

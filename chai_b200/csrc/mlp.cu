@@ -1,4 +1,4 @@
-// The tuner's cost model: a 12 -> 128 -> 128 -> 128 -> 1 ReLU MLP mapping
+// The tuner's cost model: a 14 -> 128 -> 128 -> 128 -> 1 ReLU MLP mapping
 // GEMM/GEMV shape and tile-configuration features to log(runtime).  Trained
 // and served on the GPU by the kernels in this file: a shared-memory tiled
 // FP32 matmul with optional transposes (forward and the three backward

@@ -779,6 +779,69 @@ int Translator::do_read(int i)
 
 using namespace chai;
 
+// Replay of a recorded plan from a captured CUDA graph (the reference keys
+// repeated work by trace hash, runtime/Scheduler.cpp:48-89, and re-runs its
+// statement pipeline each time).  The plan's buffers are allocated first; the
+// graph is captured once for a set of device pointers (the trace's buffers,
+// the context scratch and status word) and launched whenever the same
+// pointers come back -- one launch for the whole trace, temporaries allocated
+// and freed inside the graph.  Returns 0 when the graph ran, > 0 when the
+// plain replay should run instead (the plan does not fit, or the capture was
+// not possible), < 0 on error.
+static int graph_replay(chai_cuda_ctx* ctx, uint64_t h, const Plan& p, const std::vector<uint64_t>& ids)
+{
+    if (ids.size() != p.buf_alloc.size()) return 1;
+    std::vector<void*> sig;
+    for (size_t k = 0; k < ids.size(); k++) {
+        if (p.buf_alloc[k]) {
+            int st = alloc_buffer(ctx, ids[k], p.buf_alloc[k]);
+            if (st) return st;
+        }
+        Buffer* b = find_buffer(ctx, ids[k]);
+        if (p.buf_need[k] && (!b || b->bytes < p.buf_need[k])) return 1;
+        sig.push_back(b ? b->ptr : nullptr);
+    }
+    sig.push_back(ctx->scratch);
+    sig.push_back(ctx->status_word);
+    sig.push_back(ctx->stream);
+    chai_cuda_ctx::PlanGraph& g = ctx->graphs[h];
+    if (!g.exec || g.sig != sig) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+        g.sig.clear();
+        cudaGraph_t graph = nullptr;
+        std::lock_guard<std::mutex> cap(ctx->capture_mutex);
+        if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            return 1;
+        }
+        ctx->capturing = true;
+        int st;
+        {
+            Translator tr(ctx);
+            st = tr.replay(p, ids);
+        }   // temporaries freed inside the capture
+        ctx->capturing = false;
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        if (st != 0 || e != cudaSuccess || !graph) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return 1;                                  // run the plain replay instead
+        }
+        e = cudaGraphInstantiateWithFlags(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            g.exec = nullptr;
+            cudaGetLastError();
+            return 1;
+        }
+        g.sig = sig;
+    }
+    CHAI_CUDA_TRY(ctx, cudaGraphLaunch(g.exec, ctx->stream));
+    ctx->graph_launches++;
+    return 0;
+}
+
 extern "C" int chai_cuda_evaluate(chai_cuda_ctx* ctx, const chai_trace_desc* t, const chai_buffer_binding* b,
                                   size_t nb)
 {
@@ -793,6 +856,15 @@ extern "C" int chai_cuda_evaluate(chai_cuda_ctx* ctx, const chai_trace_desc* t, 
         for (uint64_t w : key) { h ^= w; h *= 1099511628211ull; }
         auto it = ctx->plans.find(h);
         if (it != ctx->plans.end() && it->second->key == key) {
+            const bool graphs = ctx->cfg.plan_graph == 1 || (ctx->cfg.plan_graph < 0 && !ctx->kernel_timing);
+            if (graphs) {
+                int gst = graph_replay(ctx, h, *it->second, ids);
+                if (gst < 0) return gst;
+                if (gst == 0) {
+                    ctx->plan_hits++;
+                    return CHAI_OK;
+                }
+            }
             Translator tr(ctx);
             int st = tr.replay(*it->second, ids);
             if (st < 0) return st;
@@ -813,7 +885,17 @@ extern "C" int chai_cuda_evaluate(chai_cuda_ctx* ctx, const chai_trace_desc* t, 
     if (ctx->cfg.plan_cache) {
         std::unique_ptr<Plan> p = tr.take_plan();
         if (p) {
-            if (ctx->plans.size() >= 1024) ctx->plans.clear();
+            if (ctx->plans.size() >= 1024) {
+                ctx->plans.clear();
+                for (auto& kv : ctx->graphs)
+                    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+                ctx->graphs.clear();
+            }
+            auto g = ctx->graphs.find(h);          // a graph of an earlier plan with this hash
+            if (g != ctx->graphs.end()) {
+                if (g->second.exec) cudaGraphExecDestroy(g->second.exec);
+                ctx->graphs.erase(g);
+            }
             p->key = std::move(key);
             ctx->plans[h] = std::shared_ptr<Plan>(std::move(p));
         }

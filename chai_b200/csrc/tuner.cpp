@@ -62,8 +62,8 @@ std::vector<chai_gemm_cfg> Tuner::space(const chai_gemm_key& key)
         bulk.vec_width = 1;
         bulk.cluster_m = bulk.cluster_n = 1;
         v.push_back(bulk);
-        for (int w : {4, 8, 16})
-            for (int u : {1, 4}) {
+        for (int w : {2, 4, 8, 16})
+            for (int u : {1, 2, 4, 8}) {
                 chai_gemm_cfg c{};
                 c.block_m = w;
                 c.vec_width = u;
@@ -72,27 +72,32 @@ std::vector<chai_gemm_cfg> Tuner::space(const chai_gemm_key& key)
             }
         return v;
     }
-    for (int bn : {128, 256}) {
-        const int st[2] = {bn == 256 ? 3 : 4, bn == 256 ? 4 : 6};
-        for (int s : st)
-            for (int g : {1, 16, 64}) {
-                chai_gemm_cfg c{};
-                c.block_m = 128;
-                c.block_n = bn;
-                c.block_k = 128;
-                c.stages = s;
-                c.vec_width = 4;
-                c.cluster_m = c.cluster_n = 1;
-                c.group_m = g;
-                v.push_back(c);
-            }
-    }
+    // one-CTA tiles (block_m 128): N tile 64 / 128 / 256 with their stage
+    // counts; CTA-pair tiles (block_m 256, cluster 2 x 1): N tile 128 / 256;
+    // each over eight tile-raster group heights
+    struct Tile { int bm, bn, stages; };
+    static const Tile tiles[] = {{128, 64, 4}, {128, 64, 6}, {128, 64, 8}, {128, 128, 4}, {128, 128, 6},
+                                 {128, 256, 3}, {128, 256, 4}, {256, 128, 4}, {256, 128, 6}, {256, 128, 8},
+                                 {256, 256, 3}, {256, 256, 4}, {256, 256, 6}};
+    for (const Tile& t : tiles)
+        for (int g : {1, 2, 4, 8, 16, 32, 64, 128}) {
+            chai_gemm_cfg c{};
+            c.block_m = t.bm;
+            c.block_n = t.bn;
+            c.block_k = 128;
+            c.stages = t.stages;
+            c.vec_width = 4;
+            c.cluster_m = t.bm == 256 ? 2 : 1;
+            c.cluster_n = 1;
+            c.group_m = g;
+            v.push_back(c);
+        }
     return v;
 }
 
-// Fraction of the last wave of CTAs that has work: GEMM tiles of 128 x block_n
-// over a persistent grid of 148 CTAs; GEMV blocks of `warps` rows with
-// 64 / warps blocks resident per SM.
+// Fraction of the last wave of work units that has work: GEMM tiles of
+// block_m x block_n over a persistent grid (148 one-CTA tiles or 74 CTA pairs
+// at a time); GEMV blocks of `warps` rows with 64 / warps blocks per SM.
 static double wave_efficiency(const chai_gemm_key& key, const chai_gemm_cfg& c)
 {
     const double sms = 148.0;
@@ -102,12 +107,21 @@ static double wave_efficiency(const chai_gemm_key& key, const chai_gemm_cfg& c)
         units = std::ceil((double)std::max<long long>(1, key.m) / w);
         per_wave = sms * std::max(1, std::min(32, 64 / w));
     } else {
-        const int bn = std::max(1, c.block_n);
-        units = std::ceil((double)std::max<long long>(1, key.m) / 128.0) *
+        const int bm = c.block_m == 256 ? 256 : 128, bn = std::max(1, c.block_n);
+        units = std::ceil((double)std::max<long long>(1, key.m) / bm) *
                 std::ceil((double)std::max<long long>(1, key.n) / bn);
-        per_wave = sms;
+        per_wave = bm == 256 ? sms / 2 : sms;
     }
     return units / (std::ceil(units / per_wave) * per_wave);
+}
+
+// Fraction of the tiles' area inside the product (tile quantisation)
+static double tile_fill(const chai_gemm_key& key, const chai_gemm_cfg& c)
+{
+    if (key.is_gemv) return 0.0;
+    const double m = std::max<long long>(1, key.m), n = std::max<long long>(1, key.n);
+    const double bm = c.block_m == 256 ? 256 : 128, bn = std::max(1, c.block_n);
+    return (m * n) / (std::ceil(m / bm) * bm * std::ceil(n / bn) * bn);
 }
 
 void Tuner::features(const chai_gemm_key& key, const chai_gemm_cfg& c, float* f)
@@ -122,12 +136,14 @@ void Tuner::features(const chai_gemm_key& key, const chai_gemm_cfg& c, float* f)
     f[3] = !key.is_gemv && split ? 1.0f : 0.0f;
     f[4] = !key.is_gemv && !split ? 1.0f : 0.0f;
     f[5] = key.is_gemv ? 1.0f : 0.0f;
-    f[6] = (float)c.block_n / 256.0f;
-    f[7] = (float)c.stages / 6.0f;
-    f[8] = c.group_m > 0 ? (float)(std::log2((double)c.group_m) / 6.0) : 0.0f;
-    f[9] = key.is_gemv ? (float)c.block_m / 16.0f : 0.0f;
-    f[10] = key.is_gemv ? (float)c.vec_width / 4.0f : 0.0f;
-    f[11] = (float)wave_efficiency(key, c);
+    f[6] = !key.is_gemv && c.block_m == 256 ? 1.0f : 0.0f;
+    f[7] = (float)c.block_n / 256.0f;
+    f[8] = (float)c.stages / 8.0f;
+    f[9] = c.group_m > 0 ? (float)(std::log2((double)c.group_m) / 7.0) : 0.0f;
+    f[10] = key.is_gemv ? (float)c.block_m / 16.0f : 0.0f;
+    f[11] = key.is_gemv ? (float)c.vec_width / 8.0f : 0.0f;
+    f[12] = (float)wave_efficiency(key, c);
+    f[13] = (float)tile_fill(key, c);
 }
 
 int Tuner::ensure_operands(const chai_gemm_key& key)
@@ -458,10 +474,10 @@ int chai_cuda_tune_sweep(chai_cuda_ctx* ctx, const chai_gemm_key* key, chai_gemm
     return ctx->tuner->sweep(key, out, cap, n);
 }
 
-int chai_cuda_tune_features(const chai_gemm_key* key, const chai_gemm_cfg* cfg, float* out12)
+int chai_cuda_tune_features(const chai_gemm_key* key, const chai_gemm_cfg* cfg, float* out)
 {
-    if (!key || !cfg || !out12) return CHAI_ERR_INVALID;
-    Tuner::features(*key, *cfg, out12);
+    if (!key || !cfg || !out) return CHAI_ERR_INVALID;
+    Tuner::features(*key, *cfg, out);
     return CHAI_OK;
 }
 

@@ -45,7 +45,7 @@ void preload_gemm_kernels();
 void preload_gemv_kernels();
 
 // The cost model: features (tuner.cpp) -> 3 x 128 ReLU -> log runtime (mlp.cu).
-constexpr int MLP_IN = 12, MLP_H = 128;
+constexpr int MLP_IN = 14, MLP_H = 128;
 class Mlp;
 
 class Tuner {

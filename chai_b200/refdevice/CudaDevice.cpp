@@ -143,13 +143,14 @@ public:
     vector< string >&                      kernelText;
     string                                 error;
     size_t                                 current;      // statement being flattened
+    bool                                   makeSlots;    // the next scalar is a make statement's slot count
 
     Flattener(VectorTrace& v, CudaDevice& d, chai_cuda_ctx* c, size_t s, set< pair< uint32_t, uint32_t > >& a,
               map< uint32_t, uint32_t >& l, const set< uint32_t >& w, map< uint32_t, chai_buffer_binding >& in,
               vector< uint64_t >& sc, vector< ReadBox >& rd, vector< chai_inline_kernel >& k,
               vector< vector< chai_kernel_arg > >& ka, vector< string >& kt)
         : vt(v), dev(d), ctx(c), slots(s), cells(NULL), assigned(a), latest(l), written(w), inputs(in),
-          scratch(sc), reads(rd), kernels(k), kernelArgs(ka), kernelText(kt), current(0) { }
+          scratch(sc), reads(rd), kernels(k), kernelArgs(ka), kernelText(kt), current(0), makeSlots(false) { }
 
     void push(const uint32_t kind, const uint32_t code, const uint32_t version, const double scalar,
               const uint64_t buffer)
@@ -236,7 +237,15 @@ public:
 
     void visit(const uint32_t opCode) { push(CHAI_BC_OPCODE, opCode, 0, 0, 0); }
 
-    void visit(const double scalar) { push(CHAI_BC_SCALAR, 0, 0, scalar, 0); }
+    void visit(const double scalar)
+    {
+        // a make statement of a vector trace that gathers single traces
+        // (Scheduler batching, runtime/Scheduler.cpp:48-89) holds one box per
+        // trace: its slot count is the number of traces
+        const double v = makeSlots ? (scalar > (double)slots ? scalar : (double)slots) : scalar;
+        makeSlots = false;
+        push(CHAI_BC_SCALAR, 0, 0, v, 0);
+    }
 
     void visit(void* ptr)
     {
@@ -257,7 +266,9 @@ public:
         scratch.push_back(id);
         if (proto->dataPtr())
         {
-            // make1 / make2: the box data (memalloc copied it into padded rows)
+            // make1 / make2: the box data (memalloc copied it into padded rows);
+            // the next cell is the statement's slot count
+            makeSlots = slots > 1;
             vector< char > dense;
             packBoxes(boxes, slots, proto->prec(), proto->W(), proto->H(), dense);
             if (ctx && chai_cuda_upload(ctx, id, dense.empty() ? NULL : &dense[0], dense.size()))

@@ -17,9 +17,9 @@ import numpy as np
 
 from . import _lib as L
 
-N_FEATURES = 12
-GEMM_SPACE = 12
-GEMV_SPACE = 7
+N_FEATURES = 14
+GEMM_SPACE = 104
+GEMV_SPACE = 17
 
 
 def key(m, n, k=1, precision=L.GEMM_BF16X3, is_gemv=False) -> L.chai_gemm_key:
@@ -47,9 +47,9 @@ def shapes(count: int, seed: int = 13, lo: int = 64, hi: int = 16384, gemv_frac:
 
 def sweep(ctx, k: L.chai_gemm_key):
     """Time every configuration of the search space for `k` (list of cfgs)."""
-    buf = (L.chai_gemm_cfg * 32)()
+    buf = (L.chai_gemm_cfg * 256)()
     n = C.c_int(0)
-    L.check(L.lib().chai_cuda_tune_sweep(ctx, C.byref(k), buf, 32, C.byref(n)), ctx)
+    L.check(L.lib().chai_cuda_tune_sweep(ctx, C.byref(k), buf, 256, C.byref(n)), ctx)
     return [L.chai_gemm_cfg.from_buffer_copy(buf[i]) for i in range(n.value)]
 
 
@@ -129,6 +129,11 @@ def collect(ctx, keys, log=None):
     return out, time.perf_counter() - t0
 
 
+# the configurations a call uses without a tuned entry (TcCfg / GemvCfg defaults)
+DEFAULT_GEMM = (256, 256, 128, 4, 4, 16)
+DEFAULT_GEMV = (0, 0, 0, 0, 1, 0)
+
+
 def cfg_id(c: L.chai_gemm_cfg):
     return (c.block_m, c.block_n, c.block_k, c.stages, c.vec_width, c.group_m)
 
@@ -155,7 +160,7 @@ def evaluate(ctx, held_out, default_ids=None):
         t0 = time.perf_counter()
         sweep(ctx, k)
         t_exh = time.perf_counter() - t0
-        dflt = (0, 0, 0, 0, 1, 0) if k.is_gemv else (128, 256, 128, 4, 4, 16)
+        dflt = DEFAULT_GEMV if k.is_gemv else DEFAULT_GEMM
         rows.append(dict(m=k.m, n=k.n, k=k.k, precision=k.precision, gemv=k.is_gemv, best_us=best,
                          pick_us=by_id.get(cfg_id(pick), float("nan")),
                          default_us=by_id.get(dflt, float("nan")), learned_s=t_learned, exhaustive_s=t_exh))

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define CHAI_B200_ABI_VERSION 1
+#define CHAI_B200_ABI_VERSION 2
 
 typedef enum chai_status {
     CHAI_OK = 0,
@@ -311,7 +311,7 @@ int chai_cuda_gemm_grouped(chai_cuda_ctx* ctx, int32_t precision, const chai_gem
 /* sum / mean / dot_product over `slots` arrays of n elements each
  * (enqueue/EnqueueReduce.cpp:21-222; interp/InterpAccum.cpp:13-70).
  * op: 0 sum, 1 mean, 2 dot_product (b used).  Results (one per slot) are
- * written as doubles to host memory `out`. */
+ * written as doubles to host memory `out`; at most 4096 slots per call. */
 int chai_cuda_reduce(chai_cuda_ctx* ctx, uint32_t op, uint32_t prec, const void* a, const void* b,
                      uint64_t n, uint32_t slots, double* out);
 
@@ -342,11 +342,12 @@ typedef struct chai_gemm_key {
     int32_t precision;          /* CHAI_GEMM_* */
     int32_t is_gemv;
 } chai_gemm_key;
-/* GEMM: block_m 128, block_n 128|256 (tcgen05 N tile), block_k 128 bytes,
- * stages 3..6 (shared-memory pipeline), group_m (tile-raster strip height),
- * cluster 1x1.  GEMV: block_m = warps (rows) per block, vec_width = 16-byte
- * loads in flight per lane; block_m = 0 is the bulk-copy kernel (A streamed
- * through shared memory, 16-byte aligned operands). */
+/* GEMM: block_m 128 (one CTA per tile, block_n 64|128|256) or 256 (a CTA pair
+ * on two SMs, tcgen05 cta_group::2, cluster 2 x 1, block_n 128|256), block_k
+ * 128 bytes, stages (shared-memory pipeline depth), group_m (tile-raster strip
+ * height).  GEMV: block_m = warps (rows) per block, vec_width = 16-byte loads
+ * in flight per lane; block_m = 0 is the bulk-copy kernel (A streamed through
+ * shared memory, 16-byte aligned operands). */
 typedef struct chai_gemm_cfg {
     int32_t block_m, block_n, block_k, stages;
     int32_t vec_width, cluster_m, cluster_n, group_m;
@@ -361,13 +362,14 @@ int chai_cuda_tune(chai_cuda_ctx* ctx, const chai_gemm_key* key, int mode, chai_
 /* Time every configuration of the search space for `key` (the exhaustive
  * sweep that generates the cost model's training data). */
 int chai_cuda_tune_sweep(chai_cuda_ctx* ctx, const chai_gemm_key* key, chai_gemm_cfg* out, int cap, int* n);
-/* The 12 cost-model input features of (key, cfg). */
-int chai_cuda_tune_features(const chai_gemm_key* key, const chai_gemm_cfg* cfg, float* out12);
+/* The 14 cost-model input features of (key, cfg) into out[0..13]. */
+#define CHAI_TUNE_FEATURES 14
+int chai_cuda_tune_features(const chai_gemm_key* key, const chai_gemm_cfg* cfg, float* out);
 /* Tuning DB / journal: best configuration per key, plus the MLP weights. */
 int chai_cuda_tune_db_load(chai_cuda_ctx* ctx, const char* path);
 int chai_cuda_tune_db_save(chai_cuda_ctx* ctx, const char* path);
 
-/* MLP cost model (MLP_IN=12 -> 128 -> 128 -> 128 -> 1, ReLU), trained on the
+/* MLP cost model (14 features -> 128 -> 128 -> 128 -> 1, ReLU), trained on the
  * GPU by this library's forward / backward / Adam kernels on measured
  * (key, cfg, measured_us) samples; the target is log(measured_us). */
 int chai_cuda_mlp_train(chai_cuda_ctx* ctx, const chai_gemm_key* keys, const chai_gemm_cfg* cfgs, size_t n,

@@ -11,11 +11,12 @@ autotune/AutoTuneBench.cpp:17-251).  What this file restates is therefore this
 library's own definition of the model, which the tuner uses to rank the
 candidates of that search before timing the top k:
 
-  features (12): log2 M/14, log2 N/14, log2 K/14 (K = 1 for GEMV), split
+  features (14): log2 M/14, log2 N/14, log2 K/14 (K = 1 for GEMV), split
     precision (fp32 via bf16x3) flag, single-pass tensor-core flag, GEMV flag,
-    block_n/256, stages/6, log2(group_m)/6, GEMV warps/16, GEMV unroll/4,
-    wave efficiency (fraction of the last wave of CTAs with work)
-  network: 12 -> 128 -> 128 -> 128 -> 1, ReLU on the hidden layers,
+    CTA-pair flag (block_m 256), block_n/256, stages/8, log2(group_m)/7, GEMV
+    warps/16, GEMV unroll/8, wave efficiency (fraction of the last wave of
+    work units with work), tile fill (fraction of the tiles' area inside M x N)
+  network: 14 -> 128 -> 128 -> 128 -> 1, ReLU on the hidden layers,
     y = x W + b with W stored row-major (in x out)
   target: (log(measured_us) - mean) / scale, loss = mean squared error
   parameter order: W1 b1 W2 b2 W3 b3 W4 b4, then mean and scale
@@ -24,25 +25,27 @@ from __future__ import annotations
 
 import numpy as np
 
-IN, H = 12, 128
+IN, H = 14, 128
 DIMS = [IN, H, H, H, 1]
 GEMM_FP32, GEMM_TF32, GEMM_BF16, GEMM_BF16X3, GEMM_BF16X6, GEMM_FP8, GEMM_FP64 = range(7)
+
+
+TILES = [(128, 64, 4), (128, 64, 6), (128, 64, 8), (128, 128, 4), (128, 128, 6), (128, 256, 3), (128, 256, 4),
+         (256, 128, 4), (256, 128, 6), (256, 128, 8), (256, 256, 3), (256, 256, 4), (256, 256, 6)]
 
 
 def space(is_gemv: bool):
     """Search space as dicts of chai_gemm_cfg fields (tuner.cpp Tuner::space)."""
     if is_gemv:
-        return [dict(block_m=0, vec_width=1)] + [dict(block_m=w, vec_width=u) for w in (4, 8, 16) for u in (1, 4)]
-    out = []
-    for bn in (128, 256):
-        for s in ((3, 4) if bn == 256 else (4, 6)):
-            for g in (1, 16, 64):
-                out.append(dict(block_m=128, block_n=bn, block_k=128, stages=s, vec_width=4, group_m=g))
-    return out
+        return [dict(block_m=0, vec_width=1)] + [dict(block_m=w, vec_width=u) for w in (2, 4, 8, 16)
+                                                 for u in (1, 2, 4, 8)]
+    return [dict(block_m=bm, block_n=bn, block_k=128, stages=st, vec_width=4, group_m=g,
+                 cluster_m=2 if bm == 256 else 1, cluster_n=1)
+            for bm, bn, st in TILES for g in (1, 2, 4, 8, 16, 32, 64, 128)]
 
 
 def features(m, n, k, precision, is_gemv, cfg) -> np.ndarray:
-    """float32[12] feature vector of (key, cfg)."""
+    """float32[14] feature vector of (key, cfg)."""
     m, n = max(1, m), max(1, n)
     k = 1 if is_gemv else max(1, k)
     split = precision in (GEMM_BF16X3, GEMM_BF16X6, GEMM_FP32)
@@ -53,27 +56,40 @@ def features(m, n, k, precision, is_gemv, cfg) -> np.ndarray:
     f[3] = 1.0 if (not is_gemv and split) else 0.0
     f[4] = 1.0 if (not is_gemv and not split) else 0.0
     f[5] = 1.0 if is_gemv else 0.0
-    f[6] = cfg.get("block_n", 0) / 256.0
-    f[7] = cfg.get("stages", 0) / 6.0
+    f[6] = 1.0 if (not is_gemv and cfg.get("block_m", 0) == 256) else 0.0
+    f[7] = cfg.get("block_n", 0) / 256.0
+    f[8] = cfg.get("stages", 0) / 8.0
     g = cfg.get("group_m", 0)
-    f[8] = np.log2(g) / 6.0 if g > 0 else 0.0
-    f[9] = cfg.get("block_m", 0) / 16.0 if is_gemv else 0.0
-    f[10] = cfg.get("vec_width", 0) / 4.0 if is_gemv else 0.0
-    f[11] = wave_efficiency(m, n, is_gemv, cfg)
+    f[9] = np.log2(g) / 7.0 if g > 0 else 0.0
+    f[10] = cfg.get("block_m", 0) / 16.0 if is_gemv else 0.0
+    f[11] = cfg.get("vec_width", 0) / 8.0 if is_gemv else 0.0
+    f[12] = wave_efficiency(m, n, is_gemv, cfg)
+    f[13] = tile_fill(m, n, is_gemv, cfg)
     return f.astype(np.float32)
 
 
 def wave_efficiency(m, n, is_gemv, cfg) -> float:
-    """Fraction of the last wave with work: GEMM tiles of 128 x block_n over 148
-    persistent CTAs; GEMV blocks of `warps` rows, 64 / warps blocks per SM."""
+    """Fraction of the last wave with work: GEMM tiles of block_m x block_n over
+    148 persistent CTAs (74 CTA pairs for block_m 256); GEMV blocks of `warps`
+    rows, 64 / warps blocks per SM."""
     if is_gemv:
         w = max(1, cfg.get("block_m", 0))
         units = np.ceil(max(1, m) / w)
         per_wave = 148.0 * max(1, min(32, 64 // w))
     else:
-        units = np.ceil(max(1, m) / 128.0) * np.ceil(max(1, n) / max(1, cfg.get("block_n", 0)))
-        per_wave = 148.0
+        bm = 256 if cfg.get("block_m", 0) == 256 else 128
+        units = np.ceil(max(1, m) / bm) * np.ceil(max(1, n) / max(1, cfg.get("block_n", 0)))
+        per_wave = 74.0 if bm == 256 else 148.0
     return units / (np.ceil(units / per_wave) * per_wave)
+
+
+def tile_fill(m, n, is_gemv, cfg) -> float:
+    """Fraction of the tiles' area inside the M x N product."""
+    if is_gemv:
+        return 0.0
+    bm = 256.0 if cfg.get("block_m", 0) == 256 else 128.0
+    bn = float(max(1, cfg.get("block_n", 0)))
+    return (m * n) / (np.ceil(m / bm) * bm * np.ceil(n / bn) * bn)
 
 
 def count() -> int:

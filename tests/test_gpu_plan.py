@@ -110,3 +110,59 @@ def test_plan_cache_on_and_off_agree(ch, cache):
         assert replays(dev) == (2 if cache else 0)
     finally:
         dev.close()
+
+
+def graph_launches(dev):
+    n = C.c_uint64()
+    L.check(L.lib().chai_cuda_kernel_stats(dev.ctx, b"plan_graph", None, C.byref(n), 0), dev.ctx)
+    return n.value
+
+
+def _c1_on(ch, dev, seed, out_id):
+    """The C1 trace (Philox fills, 512^3 matmul on the tensor cores, sum(C*C))
+    evaluated on `dev` into buffer out_id: RNG kernels, the split prepass, the
+    GEMM (context scratch), a fused reduction and its combine (temporaries)."""
+    import bench
+    ch._Client.pending, saved = [], ch._Client.pending
+    try:
+        s = ch.Arrayf32(bench.c1_expr(ch, ch.RNGf32(ch.RNG_PHILOX, seed), 256))
+        stmts = [(v, ver, cells) for v, ver, cells, _ in ch._Client.pending]
+    finally:
+        ch._Client.pending = saved
+    dev.evaluate(stmts, [(s.var, 4, 1, 1, 1, 0, out_id)])
+    return float(dev.readback(out_id, 1, np.float32)[0])
+
+
+def test_graph_replay_c1_and_kirsch(ch):
+    """PlanGraph=1: the third and later evaluations of a repeated trace run as
+    one captured CUDA graph (plan_graph counter); results equal the plain
+    replay's (PlanGraph=0) bit for bit, and the graph is captured again when
+    the trace's buffers move (new buffer ids)."""
+    g, p = ch.Device(config="PlanGraph=1"), ch.Device(config="PlanGraph=0")
+    try:
+        want = [_c1_on(ch, p, 3, 700) for _ in range(3)]
+        got = [_c1_on(ch, g, 3, 700) for _ in range(4)]
+        assert len(set(want)) == 1 and all(x == want[0] for x in got), (got, want)
+        assert graph_launches(g) >= 2 and graph_launches(p) == 0
+        n0 = graph_launches(g)
+        # Kirsch over fixed buffers 900 -> 901, new image contents each time
+        from tests.test_gpu_trace import kirsch_expr
+        H, W = 40, 64
+        ch._Client.pending, saved = [], ch._Client.pending
+        try:
+            a_var = next(ch._Client.vars)
+            A = ch._Raw([ch._bc(L.BC_VARIABLE, a_var, 0)], 4, W, H)
+            K = ch.Arrayf32(kirsch_expr(ch, A, W, H))
+            stmts = [(v, ver, cells) for v, ver, cells, _ in ch._Client.pending]
+        finally:
+            ch._Client.pending = saved
+        for seed in (9, 10, 11, 12):
+            img = oracle.rng_fill(W * H, seed=seed).reshape(H, W)
+            L.check(L.lib().chai_cuda_upload(g.ctx, 900, img.ctypes.data_as(C.c_void_p), img.nbytes), g.ctx)
+            g.evaluate(stmts, [(a_var, 4, W, H, 1, 0, 900), (K.var, 4, W, H, 1, 0, 901)])
+            out = g.readback(901, W * H, np.float32).reshape(H, W)
+            assert np.array_equal(out, oracle.kirsch(img)), seed
+        assert graph_launches(g) - n0 >= 2
+    finally:
+        g.close()
+        p.close()

@@ -33,7 +33,8 @@ def test_features_match_oracle(is_gemv):
 def test_search_space_sizes():
     assert len(OM.space(False)) == T.GEMM_SPACE
     assert len(OM.space(True)) == T.GEMV_SPACE
-    assert OM.count() == 12 * 128 + 128 + 2 * (128 * 128 + 128) + 128 + 1
+    assert OM.count() == 14 * 128 + 128 + 2 * (128 * 128 + 128) + 128 + 1
+    assert T.GEMM_SPACE >= 100
 
 
 def test_tuning_shapes_are_log_uniform_and_seeded():

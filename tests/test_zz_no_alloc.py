@@ -102,7 +102,8 @@ def test_noalloc_reduce_matches_oracle_and_regular_entry_point(chai_dev, op, pre
     want, mag = oracle_reduce(op, prec, a_h, b_h, n, slots)
     a = torch.from_numpy(a_h.view(np.int32) if prec == L.U32 else a_h).cuda()
     b = torch.from_numpy(b_h.view(np.int32) if prec == L.U32 else b_h).cuda()
-    reg = regular(chai_dev, op, prec, a, b, n, slots) if n else None
+    # chai_cuda_reduce stages results in 4096 pinned doubles: compare with it up to that many slots
+    reg = regular(chai_dev, op, prec, a, b, n, slots) if n and slots <= 4096 else None
     out = torch.empty(slots, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
     for call in range(2):
