@@ -871,7 +871,7 @@ def run_tuner(args, L, ctx, stream):
             finally:
                 dev.close()
             by_k[k] = r
-    rows = by_k[2]
+    rows = by_k[3]
     topk = {k: {"pick_vs_best_geomean": gm(np.array([x["best_us"] / x["pick_us"] for x in r])),
                 "within_5pct": float(np.mean([x["best_us"] / x["pick_us"] >= 1 / 1.05 for x in r])),
                 "cold_start_speedup": sum(x["exhaustive_s"] for x in r) / sum(x["learned_s"] for x in r)}
@@ -894,7 +894,7 @@ def run_tuner(args, L, ctx, stream):
         "metric": "tune time learned vs exhaustive", "unit": "x (cold-start speedup)", "value": es / ls,
         "ms_per_step": 1e3 * ls / len(rows), "dtype": "f32/bf16", "higher_is_better": True,
         "config": {"workload": "learned GEMM/GEMV tuner: %d train + %d held-out keys, M,N,K log-uniform "
-                               "[64,16384], seed 13" % (n_train, len(rows)), "top_k": 2,
+                               "[64,16384], seed 13" % (n_train, len(rows)), "top_k": 3,
                    "search_space": {"gemm": T.GEMM_SPACE, "gemv": T.GEMV_SPACE}},
         "tuner": {"pick_vs_best_geomean": gm(q), "within_5pct": float(np.mean(q >= 1 / 1.05)),
                   "default_vs_best_geomean": gm(qd), "learned_s_total": ls, "exhaustive_s_total": es,
@@ -912,7 +912,7 @@ def run_tuner_eval(args, L, ctx, stream):
     (chai_b200/data/tuner.db + .mlp, trained by `--workload tuner --save-db`
     on the 2000 training keys): the first TUNER_EVAL_KEYS of the 200 held-out
     keys (seed 13) are swept exhaustively, then tuned from cold by the learned
-    method (rank every configuration, time the top 2) and by the exhaustive
+    method (rank every configuration, time the top 3) and by the exhaustive
     one; quality is judged on each key's own sweep."""
     import torch
     from chai_b200 import tuner as T
@@ -923,7 +923,7 @@ def run_tuner_eval(args, L, ctx, stream):
     held_keys = T.shapes(2200, seed=13)[2000:2000 + n_eval]
     held, _ = T.collect(ctx, held_keys)
     with Clocks(torch.cuda.current_device()) as clk:
-        dev = ch.Device(config="TuneDB=%s TopK=2" % TUNER_DB)
+        dev = ch.Device(config="TuneDB=%s TopK=3" % TUNER_DB)
         try:
             rows = T.evaluate(dev.ctx, held)
         finally:
@@ -937,7 +937,7 @@ def run_tuner_eval(args, L, ctx, stream):
         "metric": "tune time learned vs exhaustive", "unit": "x (cold-start speedup)", "value": es / ls,
         "ms_per_step": 1e3 * ls / len(rows), "steps": len(rows), "dtype": "f32/bf16", "higher_is_better": True,
         "config": {"workload": "learned GEMM/GEMV tuner, committed cost model, %d of the 200 held-out keys "
-                               "(M,N,K log-uniform [64,16384], seed 13), top 2 timed" % len(rows)},
+                               "(M,N,K log-uniform [64,16384], seed 13), top 3 timed" % len(rows)},
         "tuner": {"pick_vs_best_geomean": gm(q), "within_5pct": float(np.mean(q >= 1 / 1.05)),
                   "default_vs_best_geomean": gm(qd), "learned_s_total": ls, "exhaustive_s_total": es},
         "e2e": None, "roofline": None, "clocks": clk.summary(), "gpu_launches": None,

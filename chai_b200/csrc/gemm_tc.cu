@@ -557,7 +557,11 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
 // each 16-deep product into the TMEM accumulator with its own rounding, whose
 // error builds up coherently over a long K; restarting the TMEM sum every
 // SEG chunks and adding the segment sums in the epilogue warps' registers
-// (round to nearest) keeps the result at FP32-FFMA accuracy.  Eight epilogue
+// (round to nearest) keeps the result near FP32-FFMA accuracy.  The segment
+// length is a launch argument (context config GemmPairSeg, default 32 chunks
+// = 2048 K: at 16384^3 the normalised error falls from 9.8e-7 to 1.7e-7 with
+// the kernel no slower than without promotion; shorter segments stall the MMA
+// on the drains).  Eight epilogue
 // warps per CTA (two per TMEM lane quarter, 128 columns each) hold the
 // running sums; they drain a segment while the MMA issues the correction
 // products of the same chunk, into the other accumulator.
@@ -569,7 +573,6 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
 //   tempty[b]  leader: 16 epilogue warps (8 per CTA) done with it
 //   drain      leader: every MMA complete before TMEM is freed
 constexpr int PAIR_THREADS = 320;           // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
-constexpr int PAIR_SEG = 4;                 // default K chunks per promotion segment (split precisions)
 
 // a pair tile is 256 x BN (BN = 128 or 256): each CTA stages 128 rows of A
 // and BN / 2 rows of B per K block

@@ -26,7 +26,7 @@ struct Config {
     double rng_pi = 3.14159;                 // M_PI as the reference JIT prints it
     int rng_layout = 0;                      // 0 chai, 1 counter
     int tuner_mode = CHAI_TUNE_LEARNED;
-    int top_k = 2;                           // learned tuner: configurations timed
+    int top_k = 3;                           // learned tuner: configurations timed
     std::string tune_db;
     std::string tune_journal;                // crash-safe TRY / OK markers of every timing
     bool plan_cache = true;                  // replay recorded plans of repeated traces
@@ -35,7 +35,7 @@ struct Config {
     int stencil_min_blocks = 0;              // __launch_bounds__ minimum blocks per SM for stencil kernels (0: none)
     bool grouped_fused = true;               // grouped GEMM splits f32 operands inside the kernel (else prepass planes)
     bool gemm_pair = true;                   // 256-row GEMM tiles on CTA pairs (cta_group::2) where configured
-    int gemm_pair_seg = 4;                   // pair kernel, split precisions: K chunks per promotion segment
+    int gemm_pair_seg = 32;                  // pair kernel, split precisions: K chunks per promotion segment
     int gemm_stages = 0;                     // GEMM pipeline stages (0: tuned or default)
     bool pack_f32 = true;                    // element kernels issue f32 add / sub as packed f32x2 pairs
     std::string jit_cache;

@@ -60,7 +60,7 @@ public:
     Mlp* mlp() { return mlp_; }
     static std::vector<chai_gemm_cfg> space(const chai_gemm_key& key);
     static void features(const chai_gemm_key& key, const chai_gemm_cfg& cfg, float* f);
-    int top_k = 2;
+    int top_k = 3;
 
 private:
     chai_cuda_ctx* ctx_;

@@ -357,7 +357,7 @@ enum { CHAI_TUNE_LEARNED = 0, CHAI_TUNE_EXHAUSTIVE = 1 };
 /* Choose a configuration for `key` and remember it (used by later GEMM/GEMV
  * calls of that shape).  EXHAUSTIVE times every configuration of the search
  * space (AutoTuneBench); LEARNED ranks them with the MLP cost model and times
- * only the top k (TopK in the init config, default 2). */
+ * only the top k (TopK in the init config, default 3). */
 int chai_cuda_tune(chai_cuda_ctx* ctx, const chai_gemm_key* key, int mode, chai_gemm_cfg* out);
 /* Time every configuration of the search space for `key` (the exhaustive
  * sweep that generates the cost model's training data). */
