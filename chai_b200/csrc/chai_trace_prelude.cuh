@@ -51,6 +51,31 @@ template <class T> __device__ __forceinline__ void st4(T* __restrict__ p, const 
     }
 }
 
+// One dot_product term as interp/InterpDotprod.cpp:40-138 forms it: the
+// product in the operands' common C type (float * float rounded to f32,
+// int * int wrapping in 32 bits, anything * double in f64), widened to
+// double for the sum.
+template <class A, class B> __device__ __forceinline__ double dot_term(A a, B b) { return (double)(a * b); }
+__device__ __forceinline__ double dot_term(int a, int b) { return (double)(int)((unsigned)a * (unsigned)b); }
+__device__ __forceinline__ double dot_term(unsigned a, int b) { return (double)(a * (unsigned)b); }
+__device__ __forceinline__ double dot_term(int a, unsigned b) { return (double)((unsigned)a * b); }
+__device__ __forceinline__ double dot_term(unsigned a, unsigned b) { return (double)(a * b); }
+
+// ld4 / st4 on 4 elements inside a longer per-thread array (rows of a
+// multi-row stencil thread)
+template <class T> __device__ __forceinline__ void ld4p(const T* __restrict__ p, T* o)
+{
+    T t[4];
+    ld4(p, t);
+    o[0] = t[0]; o[1] = t[1]; o[2] = t[2]; o[3] = t[3];
+}
+
+template <class T> __device__ __forceinline__ void st4p(T* __restrict__ p, const T* v)
+{
+    const T t[4] = {v[0], v[1], v[2], v[3]};
+    st4(p, t);
+}
+
 // 16 bytes of shared memory at p (16-byte aligned) into o[0 .. 16/sizeof(T)).
 template <class T> __device__ __forceinline__ void lds_vec(const T* p, T* o)
 {

@@ -159,6 +159,8 @@ void parse_config(chai::Config& c, const char* text)
             c.top_k = std::max(1, atoi(v.c_str()));
         } else if (k == "StencilRows") {
             c.stencil_rows = atoi(v.c_str());
+        } else if (k == "StencilRowsPerThread") {
+            c.stencil_rows_per_thread = std::max(1, std::min(4, atoi(v.c_str())));
         } else if (k == "StencilMinBlocks") {
             c.stencil_min_blocks = std::max(0, std::min(8, atoi(v.c_str())));
         } else if (k == "GemmPair") {
@@ -167,6 +169,8 @@ void parse_config(chai::Config& c, const char* text)
             c.gemm_pair_seg = std::max(1, atoi(v.c_str()));
         } else if (k == "GemmStages") {
             c.gemm_stages = std::max(0, atoi(v.c_str()));
+        } else if (k == "GroupedExact") {
+            c.grouped_exact = v != "0" && v != "off";
         } else if (k == "GroupedSplit") {
             c.grouped_fused = v != "prepass";
         } else if (k == "PackF32") {

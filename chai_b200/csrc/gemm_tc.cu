@@ -1456,9 +1456,14 @@ __device__ __forceinline__ unsigned long long smem_desc_mn(unsigned addr)
     return d;
 }
 
+// flags: FS_EXACT -- each tile's MMAs cover its own columns (N rounded up
+// to 16) and its last chunk's K (rounded up to 16) instead of the full
+// 128 x 64
+constexpr int FS_EXACT = 2;
+
 template <int S, bool ACC2>
 __global__ void __launch_bounds__(FS_THREADS, 1)
-chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* status)
+chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* status, int flags)
 {
     constexpr int P = Planes<S>::P;
     constexpr int SEL = S == 1 ? 0 : (S == 3 ? 1 : 2);
@@ -1507,13 +1512,18 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
     } else if (warp == 1) {
         // ---------------------------------------------------------------- MMA
         if (lane == 0) {
-            const unsigned idesc = instr_desc<KIND_BF16, FS_BN>() | (1u << 16);   // B MN-major
+            const unsigned idesc_full = instr_desc<KIND_BF16, FS_BN>() | (1u << 16);   // B MN-major
+            const bool exact = flags & FS_EXACT;
             long long it = 0;
             int lt = 0;
-            int kbs_next = blockIdx.x < ntiles ? tiles[blockIdx.x].kblocks : 0;
+            int4 nx = make_int4(0, 0, 0, 0);          // kblocks, cols, k of the next tile (loaded one tile ahead)
+            if (blockIdx.x < ntiles) nx = make_int4(tiles[blockIdx.x].kblocks, tiles[blockIdx.x].cols, tiles[blockIdx.x].k, 0);
             for (long long t = blockIdx.x; t < ntiles && !*abort_flag; t += G, lt++) {
-                const int kbs = kbs_next;              // loaded one tile ahead
-                if (t + G < ntiles) kbs_next = tiles[t + G].kblocks;
+                const int kbs = nx.x, tcols = nx.y, tk = nx.z;
+                if (t + G < ntiles) nx = make_int4(tiles[t + G].kblocks, tiles[t + G].cols, tiles[t + G].k, 0);
+                // N of this tile's MMAs (a multiple of 16 for M = 128)
+                const unsigned idesc = exact ? ((idesc_full & ~(0x3Fu << 17)) | ((unsigned)(((tcols + 15) & ~15) >> 3) << 17))
+                                             : idesc_full;
                 const int ab = lt & 1, use = lt >> 1;
                 if (use >= 1 && !mbar_wait(smem_u32(&tempty[ab]), (unsigned)((use - 1) & 1), status, 115)) {
                     *abort_flag = 1;
@@ -1532,6 +1542,8 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const unsigned char* pa = planes + q * PBUF;
                     const unsigned char* pb = pa + P * FS_PLANE;
+                    // K = 16 steps of this chunk (the converters zero-fill k beyond K)
+                    const int ks = exact ? min(4, (tk - kb * FS_KB + 15) >> 4) : 4;
 #pragma unroll
                     for (int blk = 0; blk < S; blk++) {
                         const unsigned a0 = smem_u32(pa + kSelA[SEL][blk] * FS_PLANE);
@@ -1540,8 +1552,9 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
                         const bool first = ACC2 ? (kb == 0 && blk <= 1) : (kb == 0 && blk == 0);
 #pragma unroll
                         for (int k = 0; k < 4; k++)
-                            mma<KIND_BF16>(acc, smem_desc(a0 + 32 * k), smem_desc_mn(b0 + 2 * FS_B_SBO * k),
-                                           idesc, !(first && k == 0));
+                            if (k < ks)
+                                mma<KIND_BF16>(acc, smem_desc(a0 + 32 * k), smem_desc_mn(b0 + 2 * FS_B_SBO * k),
+                                               idesc, !(first && k == 0));
                     }
                     mma_commit(smem_u32(&pempty[q]));  // buffer q free once these MMAs finish
                 }
@@ -2090,13 +2103,14 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
     const FsTile* dt = static_cast<const FsTile*>(gp.dev);
     const long long tiles = gp.tiles;
     const unsigned grid = (unsigned)std::min<long long>(tiles, ctx->sm_count);
+    const int flags = ctx->cfg.grouped_exact ? FS_EXACT : 0;
     cudaEvent_t ev[2];
     ktime_begin(ctx, "gemm_grouped", ev);
 #define CHAI_FS(SS, A2)                                                                              \
     do {                                                                                             \
         auto k = chai_gemm_fused_split<SS, A2>;                                                      \
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, fs_smem_bytes(SS));    \
-        k<<<grid, FS_THREADS, fs_smem_bytes(SS), s>>>(dt, tiles, ctx->status_word);                  \
+        k<<<grid, FS_THREADS, fs_smem_bytes(SS), s>>>(dt, tiles, ctx->status_word, flags);           \
     } while (0)
     if (S == 1) CHAI_FS(1, false);
     else if (S == 3 && !gp.acc2) CHAI_FS(3, false);

@@ -32,7 +32,9 @@ struct Config {
     bool plan_cache = true;                  // replay recorded plans of repeated traces
     int plan_graph = -1;                     // replay plans from captured CUDA graphs: 1 on, 0 off, -1 unless kernel timing
     int stencil_rows = 32;                   // output rows per stencil tile (multiple of 8, <= 64)
+    int stencil_rows_per_thread = 1;         // output rows per stencil thread (1, 2 or 4; 4 columns each)
     int stencil_min_blocks = 0;              // __launch_bounds__ minimum blocks per SM for stencil kernels (0: none)
+    bool grouped_exact = true;               // in-kernel split: MMAs cover each tile's N and last K (rounded to 16)
     bool grouped_fused = true;               // grouped GEMM splits f32 operands inside the kernel (else prepass planes)
     bool gemm_pair = true;                   // 256-row GEMM tiles on CTA pairs (cta_group::2) where configured
     int gemm_pair_seg = 32;                  // pair kernel, split precisions: K chunks per promotion segment

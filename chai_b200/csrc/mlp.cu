@@ -1,13 +1,14 @@
 // The tuner's cost model: a 14 -> 128 -> 128 -> 128 -> 1 ReLU MLP mapping
 // GEMM/GEMV shape and tile-configuration features to log(runtime).  Trained
 // and served on the GPU by the kernels in this file: a shared-memory tiled
-// FP32 matmul with optional transposes (forward and the three backward
-// products), bias / ReLU, mean-squared-error gradient, column sums for the
-// bias gradients and Adam.  The reference's counterpart is the EM search of
+// FP32 matmul with optional transposes (forward and the backward input
+// gradient), a split-K form for the weight and bias gradients (K = samples),
+// bias / ReLU, mean-squared-error gradient and Adam.  The reference's counterpart is the EM search of
 // autotune/StandardEM.cpp:69-147, which has no model: it times every
 // candidate.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -36,6 +37,44 @@ __global__ void mlp_matmul(const float* __restrict__ A, const float* __restrict_
         __syncthreads();
     }
     if (r < M && c < N) C[(long long)r * N + c] = acc ? C[(long long)r * N + c] + sum : sum;
+}
+
+// Split-K product for the gradients, whose K is the sample count (10^5 and
+// more for a full training set): block z covers k in [z kc, (z + 1) kc) and
+// writes its partial C to P + z M N; mlp_splitk_sum adds the partials in a
+// fixed order, so the gradients are deterministic.
+__global__ void mlp_matmul_splitk(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ P,
+                                  int M, int N, int K, int kc, int ta, int tb)
+{
+    __shared__ float as[16][17], bs[16][17];
+    const int r = blockIdx.y * 16 + threadIdx.y, c = blockIdx.x * 16 + threadIdx.x;
+    const int kbeg = blockIdx.z * kc, kend = min(K, kbeg + kc);
+    float sum = 0.0f;
+    for (int k0 = kbeg; k0 < kend; k0 += 16) {
+        const int ka = k0 + threadIdx.x, kb = k0 + threadIdx.y;
+        as[threadIdx.y][threadIdx.x] = (r < M && ka < kend) ? (ta ? A[(long long)ka * M + r] : A[(long long)r * K + ka]) : 0.0f;
+        bs[threadIdx.y][threadIdx.x] = (kb < kend && c < N) ? (tb ? B[(long long)c * K + kb] : B[(long long)kb * N + c]) : 0.0f;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 16; k++) sum = fmaf(as[threadIdx.y][k], bs[k][threadIdx.x], sum);
+        __syncthreads();
+    }
+    if (r < M && c < N) P[(long long)blockIdx.z * M * N + (long long)r * N + c] = sum;
+}
+
+__global__ void mlp_splitk_sum(const float* __restrict__ P, float* __restrict__ C, int splits, int mn)
+{
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= mn) return;
+    float s = 0.0f;
+    for (int z = 0; z < splits; z++) s += P[(long long)z * mn + i];
+    C[i] = s;
+}
+
+__global__ void mlp_fill(float* __restrict__ p, long long n, float v)
+{
+    const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (i < n) p[i] = v;
 }
 
 __global__ void mlp_bias_act(float* __restrict__ Y, const float* __restrict__ b, long long M, int N, int relu)
@@ -71,22 +110,6 @@ __global__ void mlp_mse(const float* __restrict__ p, const float* __restrict__ y
         __syncthreads();
     }
     if (threadIdx.x == 0) part[blockIdx.x] = sm[0];
-}
-
-// db[j] = sum_i dY[i][j], one block per column, fixed order
-__global__ void mlp_colsum(const float* __restrict__ dY, float* __restrict__ db, long long M, int N)
-{
-    __shared__ float sm[256];
-    const int j = blockIdx.x;
-    float s = 0.0f;
-    for (long long i = threadIdx.x; i < M; i += 256) s += dY[i * N + j];
-    sm[threadIdx.x] = s;
-    __syncthreads();
-    for (int k = 128; k > 0; k >>= 1) {
-        if (threadIdx.x < k) sm[threadIdx.x] += sm[threadIdx.x + k];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) db[j] = sm[0];
 }
 
 __global__ void mlp_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
@@ -163,6 +186,8 @@ Mlp::~Mlp()
     if (x_) cudaFree(x_);
     if (y_) cudaFree(y_);
     if (part_) cudaFree(part_);
+    if (splitk_) cudaFree(splitk_);
+    if (ones_) cudaFree(ones_);
     if (host_) cudaFreeHost(host_);
 }
 
@@ -181,6 +206,9 @@ int Mlp::ensure(size_t n)
     if (x_) cudaFree(x_);
     if (y_) cudaFree(y_);
     if (part_) cudaFree(part_);
+    if (ones_) cudaFree(ones_);
+    ones_ = nullptr;
+    if (!splitk_) CHAI_CUDA_TRY(ctx_, cudaMalloc(&splitk_, (size_t)kMaxSplits * MLP_H * MLP_H * sizeof(float)));
     for (int l = 0; l < 4; l++) {
         CHAI_CUDA_TRY(ctx_, cudaMalloc(&acts_[l], n * out_[l] * sizeof(float)));
         CHAI_CUDA_TRY(ctx_, cudaMalloc(&dacts_[l], n * out_[l] * sizeof(float)));
@@ -188,6 +216,8 @@ int Mlp::ensure(size_t n)
     CHAI_CUDA_TRY(ctx_, cudaMalloc(&x_, n * MLP_IN * sizeof(float)));
     CHAI_CUDA_TRY(ctx_, cudaMalloc(&y_, n * sizeof(float)));
     CHAI_CUDA_TRY(ctx_, cudaMalloc(&part_, blocks_for((long long)n) * sizeof(double)));
+    CHAI_CUDA_TRY(ctx_, cudaMalloc(&ones_, n * sizeof(float)));
+    mlp_fill<<<blocks_for((long long)n), 256, 0, ctx_->stream>>>(ones_, (long long)n, 1.0f);
     cap_ = n;
     return CHAI_OK;
 }
@@ -238,10 +268,9 @@ double Mlp::backward(size_t n)
     for (int l = 3; l >= 0; l--) {
         if (l < 3) mlp_relu_back<<<blocks_for((long long)n * out_[l]), 256, 0, s>>>(dacts_[l], acts_[l], (long long)n * out_[l]);
         const float* in = l == 0 ? x_ : acts_[l - 1];
-        // dW = in^T dY  (in_[l] x out_[l])
-        dim3 gw((out_[l] + 15) / 16, (in_[l] + 15) / 16);
-        mlp_matmul<<<gw, dim3(16, 16), 0, s>>>(in, dacts_[l], grads_ + w_off_[l], in_[l], out_[l], (int)n, 1, 0, 0);
-        mlp_colsum<<<out_[l], 256, 0, s>>>(dacts_[l], grads_ + b_off_[l], (long long)n, out_[l]);
+        // dW = in^T dY  (in_[l] x out_[l]) and db = 1^T dY, split over the samples
+        splitk(in, dacts_[l], grads_ + w_off_[l], in_[l], out_[l], n);
+        splitk(ones_, dacts_[l], grads_ + b_off_[l], 1, out_[l], n);
         if (l > 0) {
             // dX = dY W^T  (n x in_[l])
             dim3 gx((in_[l] + 15) / 16, (unsigned)((n + 15) / 16));
@@ -255,6 +284,17 @@ double Mlp::backward(size_t n)
     double e = 0.0;
     for (double v : part) e += v;
     return e / (double)n;
+}
+
+// C (M x N) = A^T B over K = n samples (A: n x M, B: n x N), split over K
+void Mlp::splitk(const float* A, const float* B, float* C, int M, int N, size_t n)
+{
+    cudaStream_t s = ctx_->stream;
+    const int kc = std::max(256, (int)(((n + kMaxSplits - 1) / kMaxSplits + 15) / 16 * 16));
+    const int splits = (int)((n + kc - 1) / kc);
+    dim3 g((N + 15) / 16, (M + 15) / 16, (unsigned)splits);
+    mlp_matmul_splitk<<<g, dim3(16, 16), 0, s>>>(A, B, splitk_, M, N, (int)n, kc, 1, 0);
+    mlp_splitk_sum<<<(M * N + 255) / 256, 256, 0, s>>>(splitk_, C, splits, M * N);
 }
 
 void Mlp::adam(double lr)

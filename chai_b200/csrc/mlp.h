@@ -36,6 +36,9 @@ private:
     float* x_ = nullptr;
     float* y_ = nullptr;
     double* part_ = nullptr;
+    float* splitk_ = nullptr;            // split-K partial gradients (kMaxSplits x MLP_H x MLP_H)
+    float* ones_ = nullptr;              // n ones: the bias gradient is 1^T dY
+    static constexpr int kMaxSplits = 64;
     float* host_ = nullptr;              // pinned staging of inference inputs / outputs
     size_t host_cap_ = 0;
     size_t cap_ = 0;
@@ -48,6 +51,7 @@ private:
     void forward(size_t n);
     double backward(size_t n);
     void adam(double lr);
+    void splitk(const float* A, const float* B, float* C, int M, int N, size_t n);
 };
 
 }  // namespace chai

@@ -191,14 +191,35 @@ int Translator::emit_group(const std::vector<int>& roots)
         for (int r : roots) dfs(r);
     }
     const int SH = ST_TY + 2 * R, SW = ST_TX + 2 * ST_PX;
+    // Output rows per stencil thread (StencilRowsPerThread; each thread: RY
+    // rows x 4 columns).  The rows of a thread share their staged windows --
+    // the row at offset d serves the gathers at cy = d - q of every row q.
+    // Default 1: on the Kirsch trace two rows issue as many instructions per
+    // output as one (63.8 against 63.3) at 58 instead of 40 registers, and
+    // run 3 % slower.  Groups with generators or reductions keep one row
+    // (their per-element order is tied to 4-element vectors).
+    int RY = 1;
+    if (mode2d) {
+        bool simple = true;
+        for (int i : body)
+            if (nodes_[i].kind == Node::RNG || nodes_[i].kind == Node::REDUCE) simple = false;
+        const int want = std::max(1, std::min(4, ctx_->cfg.stencil_rows_per_thread));
+        if (simple)
+            for (int ry = want; ry > 1; ry /= 2)
+                if (ST_TY % (8 * ry) == 0) { RY = ry; break; }
+    }
+    const int NV = 4 * RY;   // values per thread and node
+    const std::string JL = "for (int j = 0; j < " + std::to_string(NV) + "; j++)";
     std::map<std::pair<int, int>, int> win_lo, win_hi;   // (source tile, row offset) -> column range
     std::set<std::pair<int, int>> win_done;
     for (auto& kv : sten) {
         const int k = (int)(std::find(srcs.begin(), srcs.end(), kv.second.src) - srcs.begin());
-        const std::pair<int, int> wk(k, kv.second.cy);
-        if (!win_lo.count(wk)) { win_lo[wk] = kv.second.cx; win_hi[wk] = kv.second.cx; }
-        win_lo[wk] = std::min(win_lo[wk], kv.second.cx);
-        win_hi[wk] = std::max(win_hi[wk], kv.second.cx);
+        for (int q = 0; q < RY; q++) {
+            const std::pair<int, int> wk(k, kv.second.cy + q);
+            if (!win_lo.count(wk)) { win_lo[wk] = kv.second.cx; win_hi[wk] = kv.second.cx; }
+            win_lo[wk] = std::min(win_lo[wk], kv.second.cx);
+            win_hi[wk] = std::max(win_hi[wk], kv.second.cx);
+        }
     }
     const bool use_tma = mode2d && (W % 4) == 0;
     std::vector<TmapRec> tmaps;
@@ -295,33 +316,39 @@ int Translator::emit_group(const std::vector<int>& roots)
         }
         os << "    }\n    __syncthreads();\n  }\n";
         os << "  const int lx = (threadIdx.x & 31) * 4;\n";
-        os << "  for (int rr = 0; rr < " << ST_TY / 8 << " && tile_ok; rr++) {\n";
-        os << "    const int ly = (threadIdx.x >> 5) + 8 * rr;\n";
+        os << "  for (int rr = 0; rr < " << ST_TY / (8 * RY) << " && tile_ok; rr++) {\n";
+        os << "    const int ly = " << RY << " * ((threadIdx.x >> 5) + 8 * rr);\n";
         os << "    const long long yv = ty0 + ly, xv = tx0 + lx;\n";
         os << "    if (yv >= H || xv >= W) continue;\n";
         os << "    const long long e0 = yv * W + xv;\n";
-        os << "    bool ok[4]; long long xx[4], yy[4];\n";
-        os << "    for (int j = 0; j < 4; j++) { ok[j] = xv + j < W; xx[j] = xv + j; yy[j] = yv; }\n";
+        os << "    bool ok[" << NV << "]; long long xx[" << NV << "], yy[" << NV << "];\n";
+        os << "    " << JL << " { ok[j] = xv + (j & 3) < W && yv + (j >> 2) < H; xx[j] = xv + (j & 3); "
+              "yy[j] = yv + (j >> 2); }\n";
     }
     const double two_pi = 2.0 * ctx_->cfg.rng_pi;
     const int layout = ctx_->cfg.rng_layout;
     for (int i : body) {
         const Node& nd = nodes_[i];
         const char* T = ctype_of(nd.prec);
-        os << "    " << T << " v" << i << "[4];\n";
+        os << "    " << T << " v" << i << "[" << NV << "];\n";
         if (loads.count(i)) {
             const long long sl = nd.slots > 1 ? (long long)(nd.W * nd.H) : 0;
             std::string sbase = "(long long)(slot % " + std::to_string(nd.slots) + ") * " + std::to_string(sl);
             if (nd.W == W && nd.H == H) {
-                if (vec) os << "    chai_k::ld4(p" << i << " + " << sbase << " + e0, v" << i << ");\n";
+                if (vec && RY == 1) os << "    chai_k::ld4(p" << i << " + " << sbase << " + e0, v" << i << ");\n";
+                else if (vec)
+                    for (int q = 0; q < RY; q++)
+                        os << "    if (yv + " << q << " < H) chai_k::ld4p(p" << i << " + " << sbase << " + e0 + " << q
+                           << " * W, v" << i << " + " << 4 * q << "); else for (int j = 0; j < 4; j++) v" << i
+                           << "[" << 4 * q << " + j] = (" << T << ")0;\n";
                 else
-                    os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = ok[j] ? p" << i << "[" << sbase
-                       << " + e0 + j] : (" << T << ")0;\n";
+                    os << "    " << JL << " v" << i << "[j] = ok[j] ? p" << i << "[" << sbase
+                       << " + e0 + (j >> 2) * W + (j & 3)] : (" << T << ")0;\n";
             } else if (nd.W == 1 && nd.H == 1) {
                 os << "    { const " << T << " t = p" << i << "[slot % " << nd.slots
-                   << "]; for (int j = 0; j < 4; j++) v" << i << "[j] = t; }\n";
+                   << "]; " << JL << " v" << i << "[j] = t; }\n";
             } else {
-                os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = p" << i << "[" << sbase << " + (yy[j] % "
+                os << "    " << JL << " v" << i << "[j] = p" << i << "[" << sbase << " + (yy[j] % "
                    << nd.H << ") * " << nd.W << " + (xx[j] % " << nd.W << ")];\n";
             }
             continue;
@@ -330,20 +357,20 @@ int Translator::emit_group(const std::vector<int>& roots)
             case Node::SCALAR:
             case Node::FILL: {
                 const std::string lit = literal(nd.scalar, nd.prec);
-                os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = " << lit << ";\n";
+                os << "    " << JL << " v" << i << "[j] = " << lit << ";\n";
                 break;
             }
             case Node::CONVERT:
-                os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = (" << T << ")v" << nd.kids[0] << "[j];\n";
+                os << "    " << JL << " v" << i << "[j] = (" << T << ")v" << nd.kids[0] << "[j];\n";
                 break;
             case Node::INDEX:
-                os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = (" << T << ")("
+                os << "    " << JL << " v" << i << "[j] = (" << T << ")("
                    << (nd.dim == 0 ? "xx" : "yy") << "[j] % " << (nd.dim == 0 ? nd.W : nd.H) << ");\n";
                 break;
             case Node::OP: {
                 const int ar = (int)nd.kids.size();
                 if (nd.op == 23) {
-                    os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = (v" << nd.kids[0] << "[j] != 0) ? ("
+                    os << "    " << JL << " v" << i << "[j] = (v" << nd.kids[0] << "[j] != 0) ? ("
                        << T << ")v" << nd.kids[1] << "[j] : (" << T << ")v" << nd.kids[2] << "[j];\n";
                     break;
                 }
@@ -361,7 +388,7 @@ int Translator::emit_group(const std::vector<int>& roots)
                 }
                 // operand precision: widest operand (fp-only ops at least f32);
                 // predicates return 1/0 in that precision
-                os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = f" << ar << "<" << nd.op << ", " << T
+                os << "    " << JL << " v" << i << "[j] = f" << ar << "<" << nd.op << ", " << T
                    << ">(";
                 for (int k = 0; k < ar; k++)
                     os << (k ? ", " : "") << "(" << T << ")v" << nd.kids[k] << "[j]";
@@ -370,34 +397,38 @@ int Translator::emit_group(const std::vector<int>& roots)
             }
             case Node::GATHER: {
                 if (sten.count(i)) {
-                    // all gathers of one (source, row offset) share one window of the
-                    // staged row: columns lx + PX + cmin .. lx + PX + 3 + cmax, read with
-                    // 16-byte shared loads where aligned (lx and the tile pitch are
-                    // multiples of 4 elements)
+                    // all gathers of one (source, absolute row offset) share one
+                    // window of the staged row: columns lx + PX + cmin .. lx + PX +
+                    // 3 + cmax, read with 16-byte shared loads where aligned (lx and
+                    // the tile pitch are multiples of 4 elements); row q of the
+                    // thread reads the window at row offset cy + q
                     const Sten& g = sten[i];
                     const int k = (int)(std::find(srcs.begin(), srcs.end(), g.src) - srcs.begin());
-                    const std::pair<int, int> wkey(k, g.cy);
-                    const int cmin = win_lo[wkey], cmax = win_hi[wkey];
-                    const int b0 = ST_PX + cmin, w = 4 + cmax - cmin;
-                    const std::string wn = "w" + std::to_string(k) + "_" + std::to_string(g.cy + 8);
                     const char* ST = ctype_of(nodes_[g.src].prec);
                     const int ve = 16 / (int)prec_bytes(nodes_[g.src].prec);
-                    if (!win_done.count(wkey)) {
-                        win_done.insert(wkey);
-                        os << "    " << ST << " " << wn << "[" << w << "]; { const " << ST << "* rowp = tile" << k
-                           << " + (ly + " << R + g.cy << ") * " << SW << " + lx;\n";
-                        for (int t = 0; t < w;) {
-                            if ((b0 + t) % ve == 0 && t + ve <= w) {
-                                os << "      chai_k::lds_vec(rowp + " << b0 + t << ", " << wn << " + " << t << ");\n";
-                                t += ve;
-                            } else {
-                                os << "      " << wn << "[" << t << "] = rowp[" << b0 + t << "];\n";
-                                t++;
+                    for (int q = 0; q < RY; q++) {
+                        const std::pair<int, int> wkey(k, g.cy + q);
+                        const int cmin = win_lo[wkey], cmax = win_hi[wkey];
+                        const int b0 = ST_PX + cmin, w = 4 + cmax - cmin;
+                        const std::string wn = "w" + std::to_string(k) + "_" + std::to_string(g.cy + q + 8);
+                        if (!win_done.count(wkey)) {
+                            win_done.insert(wkey);
+                            os << "    " << ST << " " << wn << "[" << w << "]; { const " << ST << "* rowp = tile" << k
+                               << " + (ly + " << R + g.cy + q << ") * " << SW << " + lx;\n";
+                            for (int t = 0; t < w;) {
+                                if ((b0 + t) % ve == 0 && t + ve <= w) {
+                                    os << "      chai_k::lds_vec(rowp + " << b0 + t << ", " << wn << " + " << t << ");\n";
+                                    t += ve;
+                                } else {
+                                    os << "      " << wn << "[" << t << "] = rowp[" << b0 + t << "];\n";
+                                    t++;
+                                }
                             }
+                            os << "    }\n";
                         }
-                        os << "    }\n";
+                        os << "    for (int j = 0; j < 4; j++) v" << i << "[" << 4 * q << " + j] = " << wn << "[j + "
+                           << g.cx - cmin << "];\n";
                     }
-                    os << "    for (int j = 0; j < 4; j++) v" << i << "[j] = " << wn << "[j + " << g.cx - cmin << "];\n";
                     break;
                 }
                 const Node& a = nodes_[nd.kids[0]];
@@ -512,8 +543,9 @@ int Translator::emit_group(const std::vector<int>& roots)
         if (nd.op == 130) {
             const Node& b = nodes_[nd.kids[1]];
             (void)b;
-            // products and sums in FP64, as the interpreter accumulates
-            term = "(double)v" + std::to_string(nd.kids[0]) + "[j] * (double)v" + std::to_string(nd.kids[1]) + "[j]";
+            // each product in the operands' common type, summed in FP64, as
+            // the interpreter accumulates (interp/InterpDotprod.cpp:40-138)
+            term = "chai_k::dot_term(v" + std::to_string(nd.kids[0]) + "[j], v" + std::to_string(nd.kids[1]) + "[j])";
         } else {
             (void)a;
             term = "(double)v" + std::to_string(nd.kids[0]) + "[j]";
@@ -525,9 +557,13 @@ int Translator::emit_group(const std::vector<int>& roots)
     for (int r : roots) {
         const Node& nd = nodes_[r];
         if (nd.kind == Node::REDUCE) continue;
-        if (vec) os << "    chai_k::st4(o" << r << " + (long long)slot * n + e0, v" << r << ");\n";
+        if (vec && RY == 1) os << "    chai_k::st4(o" << r << " + (long long)slot * n + e0, v" << r << ");\n";
+        else if (vec)
+            for (int q = 0; q < RY; q++)
+                os << "    if (yv + " << q << " < H) chai_k::st4p(o" << r << " + (long long)slot * n + e0 + " << q
+                   << " * W, v" << r << " + " << 4 * q << ");\n";
         else
-            os << "    for (int j = 0; j < 4; j++) if (ok[j]) o" << r << "[(long long)slot * n + e0 + j] = v" << r
+            os << "    " << JL << " if (ok[j]) o" << r << "[(long long)slot * n + e0 + (j >> 2) * W + (j & 3)] = v" << r
                << "[j];\n";
     }
     os << "  }\n";

@@ -213,6 +213,26 @@ def test_reductions_sum_mean_dot(ch):
         assert abs(d - np.float32(refd)) <= 2 * np.spacing(np.float32(abs(refd))) + 1e-30
 
 
+def test_dot_product_terms_in_operand_type(ch):
+    """dot_product forms each product in the operands' common C type before
+    the FP64 sum (interp/InterpDotprod.cpp:40-138): f32 * f32 rounds to f32,
+    i32 * i32 and u32 * u32 wrap in 32 bits."""
+    e = np.float32(1 + 2.0 ** -12)
+    # exact products: (1 + 2^-11 + 2^-24) - 1; the f32 product rounds the
+    # 2^-24 away (ties to even), so the reference's result is 2^-11
+    a = np.array([e, 1], dtype=np.float32)
+    b = np.array([e, -1], dtype=np.float32)
+    d = float(ch.Arrayf32(ch.dot_product(ch.make1(a), ch.make1(b))).read_scalar())
+    assert d == oracle.dot_f32(a, b) == 2.0 ** -11
+    # 70000^2 = 4.9e9 wraps to 605032704 in 32 bits
+    for dt, arr in ((np.int32, ch.Arrayi32), (np.uint32, ch.Arrayu32)):
+        x = np.array([70000, 3], dtype=dt)
+        y = np.array([70000, 5], dtype=dt)
+        want = int((np.int64(70000) * 70000) % (1 << 32)) + 15
+        got = int(arr(ch.dot_product(ch.make1(x), ch.make1(y))).read_scalar())
+        assert got == want == 605032719, (dt, got)
+
+
 def test_reduction_vectorised_slots(ch):
     """make2 with a list of host arrays: one trace, `slots` independent sums."""
     rng = np.random.default_rng(2)

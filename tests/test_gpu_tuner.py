@@ -221,7 +221,8 @@ def test_learned_tuner_gain_over_defaults_and_cold_start(tmp_path):
     bf16x3, bf16, and f32 GEMV) train the cost model on the GPU; on 30
     held-out keys of the same distribution the learned method (rank the whole
     search space with the model, time the top 3) is judged on each key's own
-    exhaustive sweep.  Asserted: its pick reaches >= 0.95 of the exhaustive
+    exhaustive sweep (per-configuration median of 5 sweeps, so that the
+    exhaustive best is not the luckiest of ~100 single samples).  Asserted: its pick reaches >= 0.95 of the exhaustive
     best (geometric mean), it beats the fixed default configuration the
     library uses without tuning, and it tunes >= 10x faster than the
     exhaustive sweep (wall time of chai_cuda_tune against the sweep)."""
@@ -233,7 +234,8 @@ def test_learned_tuner_gain_over_defaults_and_cold_start(tmp_path):
         data, _ = T.collect(ctx, train)
         samples = [(k, c) for k, cs in data for c in cs if c.measured_us < 1e29]
         T.train(ctx, samples, epochs=2500, lr=1e-3, seed=1)
-        held, _ = T.collect(ctx, held_keys)
+        # held-out keys judged on the per-configuration median of 5 sweeps
+        held, _ = T.collect(ctx, held_keys, repeats=5)
         rows = T.evaluate(ctx, held)
     finally:
         dev.close()

@@ -77,6 +77,10 @@ def test_kirsch_trace_is_one_kernel_with_gathers():
     # the 8 gathers read 3 row windows (row offsets -1, 0, +1), each one
     # 16-byte shared load plus two edge elements
     assert src.count("const float* rowp = tile0") == 3 and src.count("chai_k::lds_vec(rowp") == 3
+    # two rows x 4 columns per thread: 4 row windows (offsets -1 .. +2) serve both rows
+    st2, src2 = source(stmts, [(K.var, 4, 64, 64, 1, 0, 8)], "StencilRowsPerThread=2")
+    assert st2 == 0 and src2.count("const float* rowp = tile0") == 4 and src2.count("chai_k::lds_vec(rowp") == 4
+    assert "[8];" in src2 and " < H) chai_k::st4p(o" in src2 and "st4p" not in src
     # the index arithmetic under the stencil gathers is not emitted; f32 ops
     # stay scalar in stencil kernels
     body = src.split("chai_group")[1]
