@@ -169,6 +169,8 @@ void parse_config(chai::Config& c, const char* text)
             c.gemm_pair_seg = std::max(1, atoi(v.c_str()));
         } else if (k == "GemmStages") {
             c.gemm_stages = std::max(0, atoi(v.c_str()));
+        } else if (k == "GroupedTmaB") {
+            c.grouped_tma_b = v != "0" && v != "off";
         } else if (k == "GroupedExact") {
             c.grouped_exact = v != "0" && v != "off";
         } else if (k == "GroupedSplit") {
@@ -269,6 +271,7 @@ int chai_cuda_shutdown(chai_cuda_ctx* ctx)
     ctx->buffers.clear();
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->gplan.dev) cudaFree(ctx->gplan.dev);
+    if (ctx->gplan.maps) cudaFree(ctx->gplan.maps);
     if (ctx->status_word) cudaFree(ctx->status_word);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

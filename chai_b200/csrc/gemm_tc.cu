@@ -558,10 +558,10 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
 // error builds up coherently over a long K; restarting the TMEM sum every
 // SEG chunks and adding the segment sums in the epilogue warps' registers
 // (round to nearest) keeps the result near FP32-FFMA accuracy.  The segment
-// length is a launch argument (context config GemmPairSeg, default 32 chunks
-// = 2048 K: at 16384^3 the normalised error falls from 9.8e-7 to 1.7e-7 with
-// the kernel no slower than without promotion; shorter segments stall the MMA
-// on the drains).  Eight epilogue
+// length is a launch argument (context config GemmPairSeg, default 64 chunks
+// = 4096 K: at 16384^3 the normalised error falls from 9.8e-7 to 2.3e-7 and
+// the kernel runs 2-4 % faster than without promotion; 32-chunk segments give
+// 1.7e-7 about 1 % slower, shorter ones stall the MMA on the drains).  Eight epilogue
 // warps per CTA (two per TMEM lane quarter, 128 columns each) hold the
 // running sums; they drain a segment while the MMA issues the correction
 // products of the same chunk, into the other accumulator.
@@ -1292,9 +1292,19 @@ constexpr int FS_ESTAGE = 4 * 32 * FS_EP * 4;  // four epilogue warps x 32 rows
 // plane buffers: convert one chunk while the MMAs read the other
 __host__ __device__ constexpr int fs_pbufs(int) { return 2; }
 
-__host__ __device__ constexpr int fs_smem_bytes(int S)
+// B through TMA (BT, config GroupedTmaB=1): raw f32 B chunks (64 k x 128 n,
+// 32 KiB) in FS_BST stages filled by warp 0, so the converters hold two A
+// chunks in their registers; bf16 and bf16x3 only (the bf16x6 planes leave
+// no room for the stages).  Off by default: on the 4096-problem group it runs
+// 1.82 ms against 1.48 ms for the register path -- two stages are all that fit
+// beside the plane buffers, so B is still one chunk ahead, and the raw stage
+// adds a shared-memory write and read per element.
+constexpr int FS_BST = 2;
+constexpr int FS_BRAW = FS_KB * FS_BN * 4;
+
+__host__ __device__ constexpr int fs_smem_bytes(int S, bool BT = false)
 {
-    return fs_pbufs(S) * 2 * distinct_planes(S) * FS_PLANE + FS_ESTAGE + 1024 + 256;
+    return fs_pbufs(S) * 2 * distinct_planes(S) * FS_PLANE + (BT ? FS_BST * FS_BRAW : 0) + FS_ESTAGE + 1024 + 256;
 }
 
 struct FusedEntry {
@@ -1443,6 +1453,141 @@ __device__ __forceinline__ void fs_convert(const FsA& ra, const FsB& rb, unsigne
     }
 }
 
+// A part of fs_convert (the B chunk comes from shared memory in the BT form)
+template <int P>
+__device__ __forceinline__ void fs_convert_a(const FsA& ra, unsigned char* pa, int cw, int lane)
+{
+    const int kq = lane & 15;
+#pragma unroll
+    for (int i = 0; i < BM / FS_CONV / 2; i++) {
+        const int row = cw * (BM / FS_CONV) + 2 * i + (lane >> 4);
+        unsigned h0[3], h1[3];
+        split_pair<P>(ra.v[i].x, ra.v[i].y, h0);
+        split_pair<P>(ra.v[i].z, ra.v[i].w, h1);
+        const unsigned off = sw128(row, kq >> 1) + (kq & 1) * 8;
+#pragma unroll
+        for (int p = 0; p < P; p++) *reinterpret_cast<uint2*>(pa + p * FS_PLANE + off) = make_uint2(h0[p], h1[p]);
+    }
+}
+
+// B chunk from its raw stage (row-major 64 k x 128 n f32, as the TMA box
+// lands; zeros beyond N and K from the copy's out-of-bounds fill) into the
+// MN-major planes: the same thread-to-element map as the register path, so
+// a warp reads one 512-byte k row per step.
+template <int P>
+__device__ __forceinline__ void fs_convert_b_smem(const unsigned char* braw, unsigned char* pb, int ct)
+{
+    const int n4 = ct & 31, kr = ct >> 5;
+    const int nb = n4 >> 4, ch = (n4 & 15) >> 1, half = (n4 & 1) * 8;
+#pragma unroll
+    for (int u = 0; u < FS_BV; u++) {
+        const int k = kr + 16 * u;
+        const float4 x = *reinterpret_cast<const float4*>(braw + (k * FS_BN + 4 * n4) * 4);
+        unsigned h0[3], h1[3];
+        split_pair<P>(x.x, x.y, h0);
+        split_pair<P>(x.z, x.w, h1);
+        const unsigned off = (unsigned)(nb * FS_B_LBO + (k >> 3) * FS_B_SBO) + sw128(k & 7, ch) + half;
+#pragma unroll
+        for (int p = 0; p < P; p++) *reinterpret_cast<uint2*>(pb + p * FS_PLANE + off) = make_uint2(h0[p], h1[p]);
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, unsigned bar, int x, int y)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+                 ::"r"(dst), "l"(map), "r"(bar), "r"(x), "r"(y)
+                 : "memory");
+}
+
+// The fields of a tile record the A loads need (5 registers instead of the
+// record's 16)
+struct FsATile {
+    const float* a;
+    int k, rows, kblocks;
+};
+
+__device__ __forceinline__ FsATile fs_atile(const FsTile* tiles, long long t)
+{
+    const FsTile* r = tiles + t;
+    return FsATile{r->a, r->k, r->rows, r->kblocks};
+}
+
+// The converters' cursor over the chunks of their CTA's tiles (tile t =
+// blockIdx.x, + gridDim.x, ...; chunk kb of each), with the next tile's
+// fields loaded one tile ahead.
+struct FsCursor {
+    long long t;
+    int kb;
+    FsATile ti, next;
+};
+
+__device__ __forceinline__ void fs_cursor_init(FsCursor& c, const FsTile* tiles, long long ntiles, long long G)
+{
+    c.t = blockIdx.x;
+    c.kb = 0;
+    if (c.t < ntiles) c.ti = fs_atile(tiles, c.t);
+    if (c.t + G < ntiles) c.next = fs_atile(tiles, c.t + G);
+}
+
+__device__ __forceinline__ void fs_cursor_advance(FsCursor& c, const FsTile* tiles, long long ntiles, long long G)
+{
+    if (++c.kb < c.ti.kblocks) return;
+    c.kb = 0;
+    c.t += G;
+    c.ti = c.next;
+    if (c.t + G < ntiles) c.next = fs_atile(tiles, c.t + G);
+}
+
+// fs_load_a on the compact fields
+__device__ __forceinline__ void fs_load_a2(FsA& r, const FsATile& ti, int kb, int cw, int lane)
+{
+    const int kv = min(FS_KB, ti.k - kb * FS_KB);
+    const int kq = lane & 15;
+    const bool kok = 4 * kq < kv;
+    const float* ap = ti.a + (long long)kb * FS_KB + 4 * kq;
+#pragma unroll
+    for (int i = 0; i < BM / FS_CONV / 2; i++) {
+        const int row = cw * (BM / FS_CONV) + 2 * i + (lane >> 4);
+        r.v[i] = (kok && row < ti.rows) ? __ldcg(reinterpret_cast<const float4*>(ap + (long long)row * ti.k))
+                                        : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// One chunk of the BT converters: planes q free, B stage landed, A from the
+// registers `ra` and B from shared memory into the planes, then the A of the
+// chunk two ahead into `ra` (the other register set holds the chunk between).
+template <int P, int NPB>
+__device__ __forceinline__ bool fs_bt_step(FsA& ra, bool& have, long long& it, FsCursor& cur, const FsTile* tiles,
+                                           long long ntiles, long long G, unsigned char* planes, unsigned char* braw,
+                                           unsigned long long* pfull, unsigned long long* pempty,
+                                           unsigned long long* bfull, unsigned long long* bempty, int* status, int cw,
+                                           int lane, int ct)
+{
+    constexpr int PBUF = 2 * P * FS_PLANE;
+    const int q = (int)(it % NPB);
+    if (it >= NPB && !mbar_wait(smem_u32(&pempty[q]), (unsigned)((it / NPB - 1) & 1), status, 117)) return false;
+    const int bs = (int)(it % FS_BST);
+    if (!mbar_wait(smem_u32(&bfull[bs]), (unsigned)((it / FS_BST) & 1), status, 120)) return false;
+    unsigned char* pa = planes + q * PBUF;
+    fs_convert_a<P>(ra, pa, cw, lane);
+    fs_convert_b_smem<P>(braw + bs * FS_BRAW, pa + P * FS_PLANE, ct);
+    // async proxy on both sides: the tensor core reads the planes, and the
+    // next TMA copy into the raw stage must not overtake this thread's reads
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) {
+        mbar_arrive(smem_u32(&bempty[bs]));             // the raw stage may be refilled
+        mbar_arrive(smem_u32(&pfull[q]));
+    }
+    it++;
+    have = cur.t < ntiles;
+    if (have) {
+        fs_load_a2(ra, cur.ti, cur.kb, cw, lane);
+        fs_cursor_advance(cur, tiles, ntiles, G);
+    }
+    return true;
+}
+
 // MN-major SWIZZLE_128B descriptor: LBO between 64-element n blocks, SBO
 // between 8-row k groups
 __device__ __forceinline__ unsigned long long smem_desc_mn(unsigned addr)
@@ -1461,9 +1606,10 @@ __device__ __forceinline__ unsigned long long smem_desc_mn(unsigned addr)
 // 128 x 64
 constexpr int FS_EXACT = 2;
 
-template <int S, bool ACC2>
+template <int S, bool ACC2, bool BT>
 __global__ void __launch_bounds__(FS_THREADS, 1)
-chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* status, int flags)
+chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* status, int flags,
+                      const CUtensorMap* __restrict__ bmaps)
 {
     constexpr int P = Planes<S>::P;
     constexpr int SEL = S == 1 ? 0 : (S == 3 ? 1 : 2);
@@ -1474,8 +1620,10 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char* planes = smem;                                  // NPB plane buffers
-    float* estage = reinterpret_cast<float*>(planes + NPB * PBUF);  // epilogue stages
-    unsigned long long* bars = reinterpret_cast<unsigned long long*>(planes + NPB * PBUF + FS_ESTAGE);
+    unsigned char* braw = planes + NPB * PBUF;                     // BT: FS_BST raw B stages
+    constexpr int BRAW_BYTES = BT ? FS_BST * FS_BRAW : 0;
+    float* estage = reinterpret_cast<float*>(braw + BRAW_BYTES);   // epilogue stages
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(braw + BRAW_BYTES + FS_ESTAGE);
     unsigned long long* pfull = bars;                              // [2] planes written (per converter warp)
     unsigned long long* pempty = bars + 2;                         // [2] planes consumed (tcgen05.commit)
     unsigned long long* tfull = bars + 4;                          // [2]
@@ -1483,6 +1631,9 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
     unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 8);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     unsigned long long* drain = bars + 9;                          // every MMA complete (before dealloc)
+    unsigned long long* bfull = bars + 10;                         // BT [FS_BST] raw B stage landed (tx bytes)
+    unsigned long long* bempty = bars + 10 + FS_BST;               // BT [FS_BST] raw B stage read (per converter warp)
+    static_assert(8 * (10 + 2 * FS_BST) <= 256, "barrier area");
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long G = gridDim.x;
@@ -1492,6 +1643,10 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
             mbar_init(smem_u32(&pempty[b]), 1);
             mbar_init(smem_u32(&tfull[b]), 1);
             mbar_init(smem_u32(&tempty[b]), 4);
+        }
+        for (int b = 0; b < FS_BST; b++) {
+            mbar_init(smem_u32(&bfull[b]), 1);
+            mbar_init(smem_u32(&bempty[b]), FS_CONV);
         }
         mbar_init(smem_u32(drain), 1);
         *abort_flag = 0;
@@ -1508,7 +1663,51 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
     const unsigned tmem = *tmem_slot;
 
     if (warp == 0) {
-        // idle: both operands reach shared memory through the converters
+        if (BT && lane == 0) {
+            // ------------------------------------------------- B producer (BT)
+            // one 64 k x 128 n box of the tile's problem's B per chunk (the
+            // problem's tensor map in global memory), FS_BST stages ahead
+            static_assert(FS_BST == 2, "two raw B stages");
+            long long it = 0;
+            long long last0 = -1, last1 = -1;      // the last chunk issued into stage 0 / 1
+            // the next tile's fields are loaded one tile ahead
+            int nprob = 0, ncol = 0, nkbs = 0;
+            if (blockIdx.x < ntiles) {
+                nprob = tiles[blockIdx.x].prob;
+                ncol = tiles[blockIdx.x].col0;
+                nkbs = tiles[blockIdx.x].kblocks;
+            }
+            for (long long t = blockIdx.x; t < ntiles && !*abort_flag; t += G) {
+                const int prob = nprob, col0 = ncol, kbs = nkbs;
+                if (t + G < ntiles) {
+                    nprob = tiles[t + G].prob;
+                    ncol = tiles[t + G].col0;
+                    nkbs = tiles[t + G].kblocks;
+                }
+                bool ok = true;
+                for (int kb = 0; kb < kbs; kb++, it++) {
+                    const int b = (int)(it % FS_BST);
+                    if (it >= FS_BST &&
+                        !mbar_wait(smem_u32(&bempty[b]), (unsigned)((it / FS_BST - 1) & 1), status, 118)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(smem_u32(&bfull[b]), FS_BRAW);
+                    tma_load_2d(smem_u32(braw + b * FS_BRAW), bmaps + prob, smem_u32(&bfull[b]), col0, kb * FS_KB);
+                    if (b) last1 = it;
+                    else last0 = it;
+                }
+                if (!ok) {
+                    *abort_flag = 1;
+                    break;
+                }
+            }
+            // every copy issued lands before the CTA can exit (the converters
+            // have waited for them already unless the kernel aborted)
+            if (last0 >= 0) mbar_wait(smem_u32(&bfull[0]), (unsigned)((last0 / FS_BST) & 1), status, 119);
+            if (last1 >= 0) mbar_wait(smem_u32(&bfull[1]), (unsigned)((last1 / FS_BST) & 1), status, 119);
+        }
+        // without BT: idle (both operands reach shared memory through the converters)
     } else if (warp == 1) {
         // ---------------------------------------------------------------- MMA
         if (lane == 0) {
@@ -1627,6 +1826,42 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
             if (lane == 0) mbar_arrive(smem_u32(&tempty[ab]));
             if (!ok || *abort_flag) break;
         }
+    } else if (BT) {
+        // ------------------------------------------------- converters (BT)
+        // A from global memory in two register sets (two chunks in flight),
+        // B from the producer's raw stages
+        const int cw = warp - 6;
+        const int ct = threadIdx.x - 6 * 32;
+        FsCursor cur;
+        fs_cursor_init(cur, tiles, ntiles, G);
+        FsA r0, r1;
+        bool h0 = false, h1 = false;
+        if (cur.t < ntiles) {
+            fs_load_a2(r0, cur.ti, cur.kb, cw, lane);
+            fs_cursor_advance(cur, tiles, ntiles, G);
+            h0 = true;
+        }
+        if (cur.t < ntiles) {
+            fs_load_a2(r1, cur.ti, cur.kb, cw, lane);
+            fs_cursor_advance(cur, tiles, ntiles, G);
+            h1 = true;
+        }
+        long long it = 0;
+        bool ok = true;
+        while (h0 && !*abort_flag) {
+            if (!fs_bt_step<P, NPB>(r0, h0, it, cur, tiles, ntiles, G, planes, braw, pfull, pempty, bfull, bempty,
+                                    status, cw, lane, ct)) {
+                ok = false;
+                break;
+            }
+            if (!h1 || *abort_flag) break;
+            if (!fs_bt_step<P, NPB>(r1, h1, it, cur, tiles, ntiles, G, planes, braw, pfull, pempty, bfull, bempty,
+                                    status, cw, lane, ct)) {
+                ok = false;
+                break;
+            }
+        }
+        if (!ok && lane == 0) *abort_flag = 1;
     } else {
         // --------------------------------------------------------- converters
         const int cw = warp - 6;                    // 0 .. FS_CONV-1
@@ -1828,10 +2063,13 @@ void preload_gemm_kernels()
     cudaFuncGetAttributes(&a, pad_rows_f32);
     cudaFuncGetAttributes(&a, transpose_pad_f32);
     cudaFuncGetAttributes(&a, fs_tiles);
-    cudaFuncGetAttributes(&a, chai_gemm_fused_split<1, false>);
-    cudaFuncGetAttributes(&a, chai_gemm_fused_split<3, false>);
-    cudaFuncGetAttributes(&a, chai_gemm_fused_split<3, true>);
-    cudaFuncGetAttributes(&a, chai_gemm_fused_split<6, true>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_split<1, false, false>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_split<3, false, false>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_split<3, true, false>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_split<6, true, false>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_split<1, false, true>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_split<3, false, true>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_split<3, true, true>);
 }
 
 int launch_wait_selftest(chai_cuda_ctx* ctx, double limit_ms)
@@ -2099,6 +2337,36 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
         gp.tiles = tiles;
         // the same accumulator rule as the prepass path (see launch_gemm_grouped)
         gp.acc2 = S == 6 || kmax > 2048;
+        // B through TMA: one 2-D tensor map per problem (n inner, row pitch
+        // n * 4 bytes -- N is a multiple of 4 and B 16-byte aligned, see
+        // fused_split_ok -- box 128 n x 64 k, zeros outside the matrix)
+        gp.bt = false;
+        if ((S == 1 || S == 3) && ctx->cfg.grouped_tma_b) {
+            PFN_encodeTiled enc = encode_fn(ctx);
+            if (!enc) return CHAI_ERR_NO_DEVICE;
+            std::vector<CUtensorMap> maps(count);
+            for (int i = 0; i < count; i++) {
+                const chai_gemm_problem& q = p[i];
+                const cuuint64_t dims[2] = {(cuuint64_t)q.n, (cuuint64_t)q.k};
+                const cuuint64_t strides[1] = {(cuuint64_t)q.n * 4};
+                const cuuint32_t box[2] = {(cuuint32_t)FS_BN, (cuuint32_t)FS_KB};
+                const cuuint32_t es[2] = {1, 1};
+                if (enc(&maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(q.b), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                    return set_error(ctx, CHAI_ERR_INVALID, "grouped gemm: B tensor map of problem " + std::to_string(i));
+            }
+            const size_t mb = (size_t)count * sizeof(CUtensorMap);
+            if (gp.map_bytes < mb) {
+                if (gp.maps) CHAI_CUDA_TRY(ctx, cudaFreeAsync(gp.maps, s));
+                gp.maps = nullptr;
+                gp.map_bytes = 0;
+                CHAI_CUDA_TRY(ctx, cudaMallocAsync(&gp.maps, mb, s));
+                gp.map_bytes = mb;
+            }
+            CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(gp.maps, maps.data(), mb, cudaMemcpyHostToDevice, s));
+            gp.bt = true;
+        }
     }
     const FsTile* dt = static_cast<const FsTile*>(gp.dev);
     const long long tiles = gp.tiles;
@@ -2106,16 +2374,20 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
     const int flags = ctx->cfg.grouped_exact ? FS_EXACT : 0;
     cudaEvent_t ev[2];
     ktime_begin(ctx, "gemm_grouped", ev);
-#define CHAI_FS(SS, A2)                                                                              \
+    const CUtensorMap* maps = static_cast<const CUtensorMap*>(gp.maps);
+#define CHAI_FS(SS, A2, BTV)                                                                         \
     do {                                                                                             \
-        auto k = chai_gemm_fused_split<SS, A2>;                                                      \
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, fs_smem_bytes(SS));    \
-        k<<<grid, FS_THREADS, fs_smem_bytes(SS), s>>>(dt, tiles, ctx->status_word, flags);           \
+        auto k = chai_gemm_fused_split<SS, A2, BTV>;                                                 \
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, fs_smem_bytes(SS, BTV)); \
+        k<<<grid, FS_THREADS, fs_smem_bytes(SS, BTV), s>>>(dt, tiles, ctx->status_word, flags, maps); \
     } while (0)
-    if (S == 1) CHAI_FS(1, false);
-    else if (S == 3 && !gp.acc2) CHAI_FS(3, false);
-    else if (S == 3) CHAI_FS(3, true);
-    else CHAI_FS(6, true);
+    if (S == 1 && gp.bt) CHAI_FS(1, false, true);
+    else if (S == 1) CHAI_FS(1, false, false);
+    else if (S == 3 && !gp.acc2 && gp.bt) CHAI_FS(3, false, true);
+    else if (S == 3 && !gp.acc2) CHAI_FS(3, false, false);
+    else if (S == 3 && gp.bt) CHAI_FS(3, true, true);
+    else if (S == 3) CHAI_FS(3, true, false);
+    else CHAI_FS(6, true, false);
 #undef CHAI_FS
     CHAI_CUDA_TRY(ctx, cudaGetLastError());
     ktime_end(ctx, "gemm_grouped", ev);

@@ -34,10 +34,11 @@ struct Config {
     int stencil_rows = 32;                   // output rows per stencil tile (multiple of 8, <= 64)
     int stencil_rows_per_thread = 1;         // output rows per stencil thread (1, 2 or 4; 4 columns each)
     int stencil_min_blocks = 0;              // __launch_bounds__ minimum blocks per SM for stencil kernels (0: none)
+    bool grouped_tma_b = false;              // in-kernel split: B chunks through TMA (bf16, bf16x3; slower, see gemm_tc.cu)
     bool grouped_exact = true;               // in-kernel split: MMAs cover each tile's N and last K (rounded to 16)
     bool grouped_fused = true;               // grouped GEMM splits f32 operands inside the kernel (else prepass planes)
     bool gemm_pair = true;                   // 256-row GEMM tiles on CTA pairs (cta_group::2) where configured
-    int gemm_pair_seg = 32;                  // pair kernel, split precisions: K chunks per promotion segment
+    int gemm_pair_seg = 64;                  // pair kernel, split precisions: K chunks per promotion segment
     int gemm_stages = 0;                     // GEMM pipeline stages (0: tuned or default)
     bool pack_f32 = true;                    // element kernels issue f32 add / sub as packed f32x2 pairs
     std::string jit_cache;
@@ -94,6 +95,9 @@ struct chai_cuda_ctx {
         size_t bytes = 0;
         long long tiles = 0;
         bool acc2 = false;
+        void* maps = nullptr;        // per-problem B tensor maps (B through TMA)
+        size_t map_bytes = 0;
+        bool bt = false;             // maps valid for `problems`
     } gplan;
     uint64_t fused_launches = 0;
 };

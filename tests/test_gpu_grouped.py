@@ -127,3 +127,23 @@ def test_unaligned_c_uses_scalar_stores(chai_dev, prepass_dev):
         outs.append([c.cpu().numpy() for c in tc])
     for (m, n, k), a, b in zip(shapes, outs[0], outs[1]):
         assert a[0] == -7.0 and np.array_equal(a, b), (m, n, k)
+
+
+@pytest.mark.parametrize("prec", [L.GEMM_BF16, L.GEMM_BF16X3])
+def test_tma_b_equals_register_b(chai_dev, prec):
+    """B through TMA (raw f32 boxes of 64 k x 128 n, zero-filled past N and
+    K, split from shared memory) against B loaded into the converters'
+    registers (the default): the same planes, so C is bit-identical,
+    including a K > 2048 problem (two accumulators) and N of 4."""
+    import chai_b200.api as ch
+    shapes = problems(40, seed=9) + [(136, 260, 100), (129, 132, 36), (300, 4, 2056), (68, 44, 20), (3, 128, 4)]
+    _, _, reg = run_grouped(chai_dev, shapes, prec, seed=4)
+    dev = ch.Device(config="GroupedTmaB=1")
+    try:
+        before = fused_count(dev)
+        _, _, bt = run_grouped(dev, shapes, prec, seed=4)
+        assert fused_count(dev) == before + 1
+    finally:
+        dev.close()
+    for i, (a, b) in enumerate(zip(bt, reg)):
+        assert np.array_equal(a, b), (i, shapes[i])

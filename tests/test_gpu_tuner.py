@@ -217,7 +217,7 @@ def test_unsupported_tuning_keys_are_rejected(chai_dev):
 
 def test_learned_tuner_gain_over_defaults_and_cold_start(tmp_path):
     """What the trained network gains over the method without it.  Exhaustive
-    sweeps of 300 training keys (M, N, K log-uniform in [64, 2048]; fp32 via
+    sweeps of 600 training keys (M, N, K log-uniform in [64, 2048]; fp32 via
     bf16x3, bf16, and f32 GEMV) train the cost model on the GPU; on 30
     held-out keys of the same distribution the learned method (rank the whole
     search space with the model, time the top 3) is judged on each key's own
@@ -229,8 +229,8 @@ def test_learned_tuner_gain_over_defaults_and_cold_start(tmp_path):
     dev = ch.Device(config="TopK=3")
     try:
         ctx = dev.ctx
-        keys = T.shapes(330, seed=29, lo=64, hi=2048)
-        train, held_keys = keys[:300], keys[300:]
+        keys = T.shapes(630, seed=29, lo=64, hi=2048)
+        train, held_keys = keys[:600], keys[600:]
         data, _ = T.collect(ctx, train)
         samples = [(k, c) for k, cs in data for c in cs if c.measured_us < 1e29]
         T.train(ctx, samples, epochs=2500, lr=1e-3, seed=1)
