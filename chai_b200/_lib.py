@@ -20,7 +20,7 @@ PHILOX, THREEFRY = 1230, 1231
 BC_OPCODE, BC_VARIABLE, BC_SCALAR, BC_MEMORY, BC_KERNEL = 0, 1, 2, 3, 4
 KARG_ARRAY, KARG_LOCAL, KARG_SCALAR = 0, 1, 2
 GEMM_FP32, GEMM_TF32, GEMM_BF16, GEMM_BF16X3, GEMM_BF16X6, GEMM_FP8, GEMM_FP64, GEMM_AUTO = range(8)
-TUNE_LEARNED, TUNE_EXHAUSTIVE = 0, 1
+TUNE_LEARNED, TUNE_EXHAUSTIVE, TUNE_DEFAULT = 0, 1, 2
 
 
 class chai_bc(C.Structure):

@@ -159,6 +159,8 @@ void parse_config(chai::Config& c, const char* text)
             c.top_k = std::max(1, atoi(v.c_str()));
         } else if (k == "StencilRows") {
             c.stencil_rows = atoi(v.c_str());
+        } else if (k == "ReduceAccum") {
+            c.reduce_accum_f32 = v == "f32";
         } else if (k == "StencilRowsPerThread") {
             c.stencil_rows_per_thread = std::max(1, std::min(4, atoi(v.c_str())));
         } else if (k == "StencilMinBlocks") {

@@ -2198,7 +2198,7 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
                                    : fp8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     st = make_map(ctx, &ma, Ap, dt, (int)esz, kp, M, batch, M * kp, kblk, BM);
     if (st) return st;
-    TcCfg cfg = default_tc_cfg();
+    TcCfg cfg = default_tc_cfg(M, N, ctx->sm_count);
     if (cfg_in) cfg = *cfg_in;
     else tuned_tc_cfg(ctx, M, N, K, precision, &cfg);
     if (ctx->cfg.gemm_stages > 0) cfg.stages = ctx->cfg.gemm_stages;

@@ -32,6 +32,7 @@ struct Config {
     bool plan_cache = true;                  // replay recorded plans of repeated traces
     int plan_graph = -1;                     // replay plans from captured CUDA graphs: 1 on, 0 off, -1 unless kernel timing
     int stencil_rows = 32;                   // output rows per stencil tile (multiple of 8, <= 64)
+    bool reduce_accum_f32 = false;           // f32 reductions: per-thread partials in f32 (block tree, combine FP64)
     int stencil_rows_per_thread = 1;         // output rows per stencil thread (1, 2 or 4; 4 columns each)
     int stencil_min_blocks = 0;              // __launch_bounds__ minimum blocks per SM for stencil kernels (0: none)
     bool grouped_tma_b = false;              // in-kernel split: B chunks through TMA (bf16, bf16x3; slower, see gemm_tc.cu)
@@ -81,7 +82,11 @@ struct chai_cuda_ctx {
     uint64_t plan_hits = 0;
     // captured CUDA graphs of replayed plans: plan key hash -> the device
     // pointers the graph was captured with, and the executable graph
-    struct PlanGraph { std::vector<void*> sig; cudaGraphExec_t exec = nullptr; };
+    struct PlanGraph {
+        std::vector<void*> sig;              // pointers the instantiated graph was captured with
+        cudaGraphExec_t exec = nullptr;
+        std::vector<void*> pending;          // pointers of the last plain replay (captured when seen again)
+    };
     std::unordered_map<uint64_t, PlanGraph> graphs;
     uint64_t graph_launches = 0;
     bool capturing = false;                                 // a plan replay is being captured

@@ -270,7 +270,21 @@ int Translator::emit_group(const std::vector<int>& roots)
     }
     os << ")\n{\n";
     os << "  using namespace chai_ops; using namespace chai_rng;\n";
+    // Per-thread accumulators: FP64 (the interpreter's accumulator type,
+    // interp/InterpAccum.cpp) by default; ReduceAccum=f32 keeps the
+    // per-thread partial sums of f32 reductions in f32 (block tree and the
+    // combine stay FP64) -- an option that trades accuracy for issue slots,
+    // measured against the default on the Monte Carlo trace
+    std::vector<bool> red_f32(reds.size(), false);
+    for (size_t k = 0; k < reds.size(); k++) {
+        const Node& nd = nodes_[reds[k]];
+        bool f = ctx_->cfg.reduce_accum_f32;
+        for (int kid : nd.kids) f = f && nodes_[kid].prec == CHAI_F32;
+        red_f32[k] = f;
+    }
     if (nred) os << "  double red[" << nred << "] = {0};\n";
+    if (std::find(red_f32.begin(), red_f32.end(), true) != red_f32.end())
+        os << "  float redf[" << nred << "] = {0};\n";
     if (!mode2d) {
         os << "  const int slot = blockIdx.y;\n";
         os << "  const long long nchunk = (n + 3) >> 2;\n";
@@ -540,6 +554,13 @@ int Translator::emit_group(const std::vector<int>& roots)
         const Node& nd = nodes_[reds[k]];
         const Node& a = nodes_[nd.kids[0]];
         std::string term;
+        if (red_f32[k]) {
+            term = nd.op == 130 ? "v" + std::to_string(nd.kids[0]) + "[j] * v" + std::to_string(nd.kids[1]) + "[j]"
+                                : "v" + std::to_string(nd.kids[0]) + "[j]";
+            os << "    for (int j = 0; j < 4; j++) " << (vec ? "" : "if (ok[j]) ") << "redf[" << k << "] += " << term
+               << ";\n";
+            continue;
+        }
         if (nd.op == 130) {
             const Node& b = nodes_[nd.kids[1]];
             (void)b;
@@ -568,6 +589,8 @@ int Translator::emit_group(const std::vector<int>& roots)
     }
     os << "  }\n";
     if (nred) {
+        for (int k = 0; k < nred; k++)
+            if (red_f32[k]) os << "  red[" << k << "] = (double)redf[" << k << "];\n";
         os << "  chai_k::block_sum<" << nred << ", 256>(red);\n";
         if (!mode2d)
             os << "  if (threadIdx.x == 0) for (int k = 0; k < " << nred << "; k++) partials[((long long)k * gridDim.y + "
@@ -842,6 +865,13 @@ static int graph_replay(chai_cuda_ctx* ctx, uint64_t h, const Plan& p, const std
     sig.push_back(ctx->stream);
     chai_cuda_ctx::PlanGraph& g = ctx->graphs[h];
     if (!g.exec || g.sig != sig) {
+        // capture on the second consecutive replay with these pointers: a
+        // trace whose buffers change every evaluation (fresh uploads) keeps
+        // the plain replay instead of paying a capture per call
+        if (g.pending != sig) {
+            g.pending = sig;
+            return 1;
+        }
         if (g.exec) cudaGraphExecDestroy(g.exec);
         g.exec = nullptr;
         g.sig.clear();

@@ -274,6 +274,27 @@ int Tuner::sweep(const chai_gemm_key* key, chai_gemm_cfg* out, int cap, int* n)
 
 int Tuner::tune(const chai_gemm_key* key, int mode, chai_gemm_cfg* out)
 {
+    if (mode == CHAI_TUNE_DEFAULT) {
+        // what an untuned call of this shape runs (GemvCfg / default_tc_cfg)
+        chai_gemm_cfg c{};
+        c.cluster_m = c.cluster_n = 1;
+        if (key->is_gemv) {
+            const GemvCfg g;
+            c.block_m = g.warps;
+            c.vec_width = g.unroll;
+        } else {
+            const TcCfg t = default_tc_cfg(key->m, key->n, ctx_->sm_count);
+            c.block_m = t.bm;
+            c.block_n = t.bn;
+            c.block_k = 128;
+            c.stages = t.stages;
+            c.vec_width = 4;
+            c.cluster_m = t.bm == 256 ? 2 : 1;
+            c.group_m = t.group_m;
+        }
+        if (out) *out = c;
+        return CHAI_OK;
+    }
     std::vector<chai_gemm_cfg> v = space(*key);
     std::vector<chai_gemm_cfg> timed;
     if (mode == CHAI_TUNE_LEARNED && mlp_->trained()) {

@@ -20,7 +20,19 @@ namespace chai {
 struct TcCfg {
     int bm = 256, bn = 256, stages = 4, group_m = 16;
 };
-inline TcCfg default_tc_cfg() { return TcCfg(); }
+// The configuration of an untuned shape: 256 x 256 CTA-pair tiles, unless
+// they would keep fewer than half of the `sms` SMs busy (small products, e.g.
+// 512^2: 4 pairs on 8 SMs); then one-CTA 128 x 64 tiles, 8x as many (128 x
+// 128 or 128 x 256 tiles would still leave over half of the SMs idle there).
+inline TcCfg default_tc_cfg(long long m, long long n, int sms)
+{
+    TcCfg c;
+    const long long pairs = ((m + 255) / 256) * ((n + 255) / 256);
+    if (2 * pairs >= sms / 2) return c;
+    c.bm = 128;
+    c.bn = 64;
+    return c;
+}
 bool tuned_tc_cfg(chai_cuda_ctx* ctx, long long m, long long n, long long k, int precision, TcCfg* out);
 
 // GEMV configuration (gemv.cu): warps (rows) per block, 16-byte loads in

@@ -145,11 +145,6 @@ def collect(ctx, keys, log=None, repeats=1):
     return out, time.perf_counter() - t0
 
 
-# the configurations a call uses without a tuned entry (TcCfg / GemvCfg defaults)
-DEFAULT_GEMM = (256, 256, 128, 4, 4, 16)
-DEFAULT_GEMV = (0, 0, 0, 0, 1, 0)
-
-
 def cfg_id(c: L.chai_gemm_cfg):
     return (c.block_m, c.block_n, c.block_k, c.stages, c.vec_width, c.group_m)
 
@@ -157,8 +152,9 @@ def cfg_id(c: L.chai_gemm_cfg):
 def evaluate(ctx, held_out, default_ids=None):
     """Learned top-k tuning of held-out keys judged against their exhaustive
     sweeps: per key, the best time over the sweep, the sweep's own time for the
-    learned pick and for the default configuration, and the wall time of each
-    method (learned: ranking + timing the top k; exhaustive: the sweep)."""
+    learned pick and for the default configuration (what an untuned call of
+    that shape runs, TUNE_DEFAULT), and the wall time of each method (learned:
+    ranking + timing the top k; exhaustive: the sweep)."""
     rows = []
     # size every operand / scratch buffer for the largest key first, so that
     # neither method's timing includes a first-touch allocation
@@ -176,7 +172,7 @@ def evaluate(ctx, held_out, default_ids=None):
         t0 = time.perf_counter()
         sweep(ctx, k)
         t_exh = time.perf_counter() - t0
-        dflt = DEFAULT_GEMV if k.is_gemv else DEFAULT_GEMM
+        dflt = cfg_id(tune(ctx, k, L.TUNE_DEFAULT))
         rows.append(dict(m=k.m, n=k.n, k=k.k, precision=k.precision, gemv=k.is_gemv, best_us=best,
                          pick_us=by_id.get(cfg_id(pick), float("nan")),
                          default_us=by_id.get(dflt, float("nan")), learned_s=t_learned, exhaustive_s=t_exh))

@@ -353,11 +353,13 @@ typedef struct chai_gemm_cfg {
     int32_t vec_width, cluster_m, cluster_n, group_m;
     double  measured_us;        /* timing of the configuration (0 if not timed) */
 } chai_gemm_cfg;
-enum { CHAI_TUNE_LEARNED = 0, CHAI_TUNE_EXHAUSTIVE = 1 };
+enum { CHAI_TUNE_LEARNED = 0, CHAI_TUNE_EXHAUSTIVE = 1, CHAI_TUNE_DEFAULT = 2 };
 /* Choose a configuration for `key` and remember it (used by later GEMM/GEMV
  * calls of that shape).  EXHAUSTIVE times every configuration of the search
  * space (AutoTuneBench); LEARNED ranks them with the MLP cost model and times
- * only the top k (TopK in the init config, default 3). */
+ * only the top k (TopK in the init config, default 3).  DEFAULT returns,
+ * untimed and unremembered, the configuration an untuned call of that shape
+ * uses (the method without the tuner). */
 int chai_cuda_tune(chai_cuda_ctx* ctx, const chai_gemm_key* key, int mode, chai_gemm_cfg* out);
 /* Time every configuration of the search space for `key` (the exhaustive
  * sweep that generates the cost model's training data). */

@@ -233,6 +233,27 @@ def test_dot_product_terms_in_operand_type(ch):
         assert got == want == 605032719, (dt, got)
 
 
+def test_reduce_accum_f32_stays_close(ch):
+    """ReduceAccum=f32 (per-thread f32 partials) on a 2^22-element Monte Carlo
+    mean: within 1e-6 relative of the FP64 default."""
+    f32 = np.float32
+
+    def payoff():
+        g = ch.RNGf32(ch.RNG_PHILOX, 42)
+        return float(ch.Arrayf32(ch.mean(ch.max(f32(100) * ch.exp(
+            f32(0.03) + f32(0.2) * ch.rng_normal_make(g, 2048, 2048)) - f32(100), f32(0)))).read_scalar())
+    ref = payoff()
+    saved = ch._vm
+    dev = ch.Device(config="ReduceAccum=f32")
+    try:
+        ch._vm = dev
+        got = payoff()
+    finally:
+        ch._vm = saved
+        dev.close()
+    assert got != 0.0 and abs(got - ref) <= 1e-6 * abs(ref), (got, ref)
+
+
 def test_reduction_vectorised_slots(ch):
     """make2 with a list of host arrays: one trace, `slots` independent sums."""
     rng = np.random.default_rng(2)

@@ -246,3 +246,22 @@ def test_learned_tuner_gain_over_defaults_and_cold_start(tmp_path):
     assert pick >= 0.95, (pick, dflt, speedup)
     assert pick > dflt, (pick, dflt)
     assert speedup >= 10.0, speedup
+
+
+def test_default_mode_reports_the_untuned_configuration(chai_dev):
+    """TUNE_DEFAULT: what an untuned call runs, untimed -- CTA-pair 256 x 256
+    tiles for large products, one-CTA 128-row tiles for products whose pair
+    tiles would leave most SMs idle, the bulk kernel for GEMV."""
+    ctx = chai_dev.ctx
+    big = T.tune(ctx, T.key(16384, 16384, 16384, L.GEMM_BF16X3), L.TUNE_DEFAULT)
+    assert T.cfg_id(big) == (256, 256, 128, 4, 4, 16) and big.cluster_m == 2 and big.measured_us == 0
+    small = T.tune(ctx, T.key(512, 512, 512, L.GEMM_BF16X3), L.TUNE_DEFAULT)
+    assert (small.block_m, small.block_n, small.cluster_m) == (128, 64, 1)
+    # 4 x 16 pair tiles keep 128 SMs busy: pair tiles
+    mid = T.tune(ctx, T.key(1024, 4096, 512, L.GEMM_BF16), L.TUNE_DEFAULT)
+    assert (mid.block_m, mid.block_n) == (256, 256)
+    gv = T.tune(ctx, T.key(4096, 4096, is_gemv=True, precision=L.GEMM_FP32), L.TUNE_DEFAULT)
+    assert T.cfg_id(gv) == (0, 0, 0, 0, 1, 0)
+    # the small default is a point of the search space
+    k = T.key(512, 512, 512, L.GEMM_BF16X3)
+    assert T.cfg_id(small) in {T.cfg_id(x) for x in T.sweep(ctx, k)}

@@ -52,6 +52,19 @@ def test_monte_carlo_is_one_fused_kernel():
     assert "double" not in src.split("for (long long c")[1].split("red[0] +=")[0].replace("(double)", "")
 
 
+def test_reduce_accum_f32_option():
+    """ReduceAccum=f32: per-thread partial sums of f32 reductions in f32, the
+    block tree and the combine in FP64; the default accumulates in FP64."""
+    def build():
+        a = ch.index_f32(0, 64, 4)
+        return ch.Arrayf32(ch.sum(a) + ch.dot_product(a, a))
+    stmts, p = record(build)
+    st, src = source(stmts + [read_stmt(p)])
+    assert st == 0 and "redf" not in src and "red[0] += (double)v" in src
+    st, src = source(stmts + [read_stmt(p)], config="ReduceAccum=f32")
+    assert st == 0 and "redf[0] += v" in src and "red[1] = (double)redf[1];" in src
+
+
 def test_double_literal_promotes_to_f64():
     def build():
         return ch.Arrayf32(0.2 * ch.index_f32(0, 64, 4) + 1.0)
