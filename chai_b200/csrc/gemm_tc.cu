@@ -241,6 +241,10 @@ struct EpiArgs {
 struct TileGrid {
     int tiles_m, tiles_n, batch, group_m;
     int plane_k;       // split precisions: K elements per stored plane (plane p starts at column p * plane_k)
+    // host-side failure injection (CHAI_FAULT_INJECT=gemm_stall, one-CTA
+    // kernel): CTA 0's producer posts chunk `stall`'s expected bytes but
+    // issues no copy, so the MMA's bounded wait on it runs out (-1: off)
+    int stall = -1;
 };
 
 // Split precisions store each distinct bf16 plane once per row, side by side
@@ -403,6 +407,10 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
                     }
                     const unsigned fb = smem_u32(&full[s]);
                     mbar_expect_tx(fb, A_STAGE + B_STAGE);
+                    if (it == tg.stall && blockIdx.x == 0) {   // injected: this chunk's copies never land
+                        issued = it + 1;
+                        continue;
+                    }
                     int xa = kb * kx_mul, xb = xa;
                     if (SPLIT || split_s > 1) {
                         const int blk = kb % split_s, chunk = kb / split_s;
@@ -2248,6 +2256,7 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     tg.tiles_n = (int)((N + cfg.bn - 1) / cfg.bn);
     tg.batch = (int)batch;
     tg.group_m = cfg.group_m;
+    if (kblocks >= 2 && fault_injected("gemm_stall")) tg.stall = 1;
     tg.plane_k = (int)kpad;
     const long long ntiles = (long long)tg.tiles_m * tg.tiles_n * tg.batch;
     if (ntiles > (1ll << 30)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: too many tiles");

@@ -51,3 +51,45 @@ def test_injected_failures_are_clean(ch, chai_dev, site):
         del os.environ["CHAI_FAULT_INJECT"]
     # the same work succeeds once the injection is off
     assert np.array_equal(ch.Arrayf32(ch.make1(x) * np.float32(2)).read1(), x * np.float32(2))
+
+
+def test_gemm_wait_runs_out_and_next_gemm_is_exact(ch):
+    """A bounded wait inside the tcgen05 GEMM runs out: with
+    CHAI_FAULT_INJECT=gemm_stall the one-CTA kernel's producer (CTA 0) posts
+    one chunk's expected bytes but issues no copy, so the MMA's wait gives up
+    after its limit, the kernel drains its MMAs, frees TMEM and returns; the
+    host reads CHAI_ERR_TIMEOUT from the status word, and the next GEMM on
+    the same context is bit-identical to one before the failure."""
+    import torch
+    dev = ch.Device(config="GemmPair=0")
+    try:
+        M, N, K = 512, 384, 256
+        g = torch.Generator(device="cuda").manual_seed(5)
+        A = torch.rand((M, K), device="cuda", generator=g) * 2 - 1
+        B = torch.rand((K, N), device="cuda", generator=g) * 2 - 1
+
+        def gemm():
+            Cm = torch.full((M, N), float("nan"), device="cuda")
+            d = L.chai_gemm_desc(L.GEMM_BF16X3, 0, 0, 0, M, N, K, A.data_ptr(), K, B.data_ptr(), N, Cm.data_ptr(), N,
+                                 1.0, 0.0, 1, 0, 0, 0)
+            st = L.lib().chai_cuda_gemm(dev.ctx, C.byref(d))
+            return st, Cm
+        st, before = gemm()
+        assert st == 0
+        L.check(L.lib().chai_cuda_synchronize(dev.ctx), dev.ctx)
+        os.environ["CHAI_FAULT_INJECT"] = "gemm_stall"
+        try:
+            t0 = time.perf_counter()
+            st, _ = gemm()
+            sync = L.lib().chai_cuda_synchronize(dev.ctx)
+            dt = time.perf_counter() - t0
+        finally:
+            del os.environ["CHAI_FAULT_INJECT"]
+        assert st == 0 and sync == -5, (st, sync)      # CHAI_ERR_TIMEOUT
+        assert 1.0 < dt < 30.0, dt
+        st, after = gemm()
+        assert st == 0
+        L.check(L.lib().chai_cuda_synchronize(dev.ctx), dev.ctx)
+        assert torch.equal(before, after) and torch.isfinite(after).all()
+    finally:
+        dev.close()
