@@ -780,7 +780,12 @@ def run_mc_many(args, L, ctx, stream):
                    "host_ms_per_call": wall, "l2": "no HBM inputs (RNG in registers)"},
         "e2e": {"value": total / (e_ms * 1e-3) / 1e9, "unit": "Gnormals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 8 * len(Ls)},
-        "roofline": None, "clocks": clk, "steps": steps, "gpu_launches": steps * 2,
+        # issue roofline of chai_many (warp instructions per normal from
+        # profiles/many_traces_mc_many.md); the timed region also holds the
+        # combine (about 3 us of the step)
+        "roofline": issue_roofline(kern if k_n else None, total, "trace_many_warp_inst_per_normal",
+                                   "chai_many (+ chai_many_combine in the timed graph)"),
+        "clocks": clk, "steps": steps, "gpu_launches": steps * 2,
     }
 
 
@@ -1185,11 +1190,18 @@ def aggregate_ranks(res, world, reduce_max):
     """Whole-job figures from one rank's result under weak scaling: every rank
     processes the same per-GPU workload, the job's step time is the maximum
     over ranks (reduce_max: the collective), and `value` becomes the units all
-    ranks processed divided by that time."""
+    ranks processed divided by that time.  The end-to-end figure is
+    aggregated the same way from the slowest rank's end-to-end rate."""
     local_ms = res["ms_per_step"]
     ms = reduce_max(local_ms)
     res["value"] = res["value"] * world * local_ms / ms
     res["ms_per_step"] = ms
+    # every rank takes part in the collective, with or without an e2e figure
+    e2e = res.get("e2e")
+    v = e2e["value"] if e2e and e2e.get("value") else float("inf")
+    slowest = -reduce_max(-v)                      # min over ranks (higher is better)
+    if e2e and math.isfinite(slowest):
+        res["e2e"] = dict(e2e, value=slowest * world, per_rank_min=slowest)
     return res
 
 

@@ -33,7 +33,7 @@ def _rank(rank, world, port, out):
     try:
         units = 1000.0                      # per-rank work per step
         ms = 2.0 + rank                     # rank 1 is slower
-        res = {"value": units / ms, "ms_per_step": ms}
+        res = {"value": units / ms, "ms_per_step": ms, "e2e": {"value": 10.0 - rank, "unit": "x"}}
 
         def reduce_max(x):
             t = torch.tensor([x], dtype=torch.float64)
@@ -41,7 +41,7 @@ def _rank(rank, world, port, out):
             return float(t.item())
 
         bench.aggregate_ranks(res, world, reduce_max)
-        out[rank] = (res["value"], res["ms_per_step"])
+        out[rank] = (res["value"], res["ms_per_step"], res["e2e"]["value"])
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -58,6 +58,7 @@ def test_weak_scaling_value_is_total_units_over_slowest_rank():
         p.join(120)
         assert p.exitcode == 0
     for r in range(2):
-        value, ms = out[r]
+        value, ms, e2e = out[r]
         assert ms == pytest.approx(3.0)
         assert value == pytest.approx(2 * 1000.0 / 3.0)
+        assert e2e == pytest.approx(2 * 9.0)          # the slowest rank's end-to-end rate, times the ranks
