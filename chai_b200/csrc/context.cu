@@ -159,6 +159,8 @@ void parse_config(chai::Config& c, const char* text)
             c.top_k = std::max(1, atoi(v.c_str()));
         } else if (k == "StencilRows") {
             c.stencil_rows = atoi(v.c_str());
+        } else if (k == "FuseMaxAffine") {
+            c.fuse_max_affine = v != "0" && v != "off";
         } else if (k == "ReduceAccum") {
             c.reduce_accum_f32 = v == "f32";
         } else if (k == "StencilRowsPerThread") {

@@ -340,6 +340,60 @@ def test_kirsch_trace_bit_exact(ch):
     assert np.array_equal(got, oracle.kirsch(img))
 
 
+def _kirsch_tree_numpy(img):
+    """The traced Kirsch program in numpy f32, one IEEE operation at a time:
+    periodic neighbours, 8 * ((n_k + n_k+1) + n_k+2) - 3 * total, and the max
+    tree of chai's `a < b ? b : a`."""
+    f = np.float32
+    n = [np.roll(np.roll(img, -dy, 0), -dx, 1) for dx, dy in
+         ((-1, -1), (0, -1), (1, -1), (1, 0), (1, 1), (0, 1), (-1, 1), (-1, 0))]
+    with np.errstate(all="ignore"):
+        total = n[0]
+        for k in range(1, 8):
+            total = total + n[k]
+        t3 = f(3) * total
+        r = [f(8) * ((n[k] + n[(k + 1) % 8]) + n[(k + 2) % 8]) - t3 for k in range(8)]
+    mx = lambda a, b: np.where(a < b, b, a)
+    return mx(mx(mx(r[0], r[1]), mx(r[2], r[3])), mx(mx(r[4], r[5]), mx(r[6], r[7])))
+
+
+def test_max_affine_fusion_is_exact_on_special_values(ch):
+    """The max-of-affine rewrite (c * max(s_k) - t for a max tree of
+    c * s_k - t, FuseMaxAffine) against the plain tree (FuseMaxAffine=0) and
+    a numpy restatement, on an image with signed zeros, NaNs, infinities and
+    values whose 8 * s overflows: bit-identical on the GPU, and equal to
+    numpy except for the sign of NaNs (parity exception 7)."""
+    H, W = 64, 64
+    rng = np.random.default_rng(21)
+    img = rng.uniform(0, 1, (H, W)).astype(np.float32)
+    img[8:16, 8:16] = np.where(rng.uniform(size=(8, 8)) < 0.5, np.float32(-0.0), np.float32(0.0))
+    img[10, 40] = np.nan
+    img[30, 5] = np.inf
+    img[50, 50] = -np.inf
+    img[40:43, 20:23] = np.float32(3e38)
+    img[20:22, 55:58] = np.float32(-3e38)
+    img[60, 1] = np.float32(1e-40)                 # a subnormal
+    outs = []
+    for cfg in ("", "FuseMaxAffine=0"):
+        saved = ch._vm
+        dev = ch.Device(config=cfg) if cfg else None
+        try:
+            if dev:
+                ch._vm = dev
+            outs.append(ch.Arrayf32(kirsch_expr(ch, ch.make2(img), W, H)).read2())
+        finally:
+            ch._vm = saved
+            if dev:
+                dev.close()
+    fused, plain = outs
+    assert np.array_equal(fused.view(np.uint32), plain.view(np.uint32))
+    want = _kirsch_tree_numpy(img)
+    nan = np.isnan(want)
+    assert np.array_equal(np.isnan(fused), nan)
+    assert np.array_equal(fused[~nan].view(np.uint32), want[~nan].view(np.uint32))
+    assert (fused == 0).any() and np.isinf(fused).any() and nan.any()
+
+
 @pytest.mark.parametrize("shape", [(96, 128), (130, 517), (16, 16), (300, 1024)])
 def test_stencil_tiles_bit_exact(ch, shape):
     """Constant-offset gathers run as 2-D shared-memory tiles (TMA for

@@ -90,6 +90,11 @@ def test_kirsch_trace_is_one_kernel_with_gathers():
     # the 8 gathers read 3 row windows (row offsets -1, 0, +1), each one
     # 16-byte shared load plus two edge elements
     assert src.count("const float* rowp = tile0") == 3 and src.count("chai_k::lds_vec(rowp") == 3
+    # the max tree of 8 * s_k - 3 * total runs as 8 * max(s_k) - 3 * total
+    # when 3 * total is finite (the plain tree otherwise, and with FuseMaxAffine=0)
+    assert src.count("isinf(") == 1 and src.count("f2<13, float>") == 10   # 3 * total, fast, 8 slow
+    st0, src0 = source(stmts, [(K.var, 4, 64, 64, 1, 0, 8)], "FuseMaxAffine=0")
+    assert st0 == 0 and "isinf(" not in src0
     # two rows x 4 columns per thread: 4 row windows (offsets -1 .. +2) serve both rows
     st2, src2 = source(stmts, [(K.var, 4, 64, 64, 1, 0, 8)], "StencilRowsPerThread=2")
     assert st2 == 0 and src2.count("const float* rowp = tile0") == 4 and src2.count("chai_k::lds_vec(rowp") == 4
