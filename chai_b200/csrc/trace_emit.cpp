@@ -224,13 +224,106 @@ int Translator::emit_group(const std::vector<int>& roots)
     const bool use_tma = mode2d && (W % 4) == 0;
     std::vector<TmapRec> tmaps;
 
+    // Max of monotone affine maps.  A tree of chai max ops (`a < b ? b : a`)
+    // whose leaves are all c * s_k - t, with one constant c >= 1 and one node
+    // t, equals c * m - t where m is the same tree over the s_k, bit for bit,
+    // whenever t is not infinite: s -> fl(fl(c s) - t) is monotone
+    // non-decreasing (rounding is monotone, c > 0), NaNs sit at the same
+    // leaves in both trees, two leaves with equal values have equal bits
+    // (with c >= 1, c s rounds to zero only for s = +-0, so the only
+    // signed-zero result, -0, comes from s = -0 and t = +0 and ties no larger
+    // s), and a NaN t makes every leaf the canonical NaN.  The kernel takes
+    // the short form per element and the original tree when t is infinite
+    // (inf - inf would break monotonicity).  Saves, per output of an n-leaf
+    // tree, n - 1 multiplies and n - 1 subtractions (Kirsch: 14 of ~63).
+    struct MaxAffine {
+        int t = -1, c = -1;
+        bool c_first = true;
+        std::string fast, slow;        // the tree over s_k / over c * s_k - t, element j
+    };
+    std::map<int, MaxAffine> fused;
+    std::set<int> absorbed;
+    if (ctx_->cfg.fuse_max_affine) {
+        std::map<int, int> uses;
+        for (int i : body)
+            for (int k : nodes_[i].kids) uses[k]++;
+        for (int r : roots) uses[r]++;
+        for (auto it = body.rbegin(); it != body.rend(); ++it) {
+            const int r = *it;
+            const Node& rn = nodes_[r];
+            if (absorbed.count(r) || loads.count(r) || rn.kind != Node::OP || rn.op != 302 || rn.kids.size() != 2 ||
+                (rn.prec != CHAI_F32 && rn.prec != CHAI_F64))
+                continue;
+            const int P = rn.prec;
+            const char* TT = ctype_of(P);
+            MaxAffine m;
+            std::vector<int> inner;
+            auto own = [&](int k) { return uses[k] == 1 && !root_set.count(k) && !loads.count(k); };
+            std::function<bool(int, bool, std::string&, std::string&)> walk =
+                [&](int k, bool top, std::string& fs, std::string& ss) -> bool {
+                const Node& n = nodes_[k];
+                if (n.kind == Node::OP && n.op == 302 && n.kids.size() == 2 && n.prec == P && (top || own(k))) {
+                    std::string f0, s0, f1, s1;
+                    if (!walk(n.kids[0], false, f0, s0) || !walk(n.kids[1], false, f1, s1)) return false;
+                    if (!top) inner.push_back(k);
+                    fs = std::string("f2<302, ") + TT + ">(" + f0 + ", " + f1 + ")";
+                    ss = std::string("f2<302, ") + TT + ">(" + s0 + ", " + s1 + ")";
+                    return true;
+                }
+                // leaf: sub(mul(c, s), t) (or mul(s, c)), owned by the tree
+                if (top || !own(k) || n.kind != Node::OP || n.op != 14 || n.kids.size() != 2 || n.prec != P) return false;
+                const int mk = n.kids[0], tk = n.kids[1];
+                const Node& mn = nodes_[mk];
+                if (!own(mk) || mn.kind != Node::OP || mn.op != 13 || mn.kids.size() != 2 || mn.prec != P ||
+                    nodes_[tk].prec != P)
+                    return false;
+                int ck = -1, sk = -1;
+                bool c_first = true;
+                for (int side = 0; side < 2; side++) {
+                    const Node& cn = nodes_[mn.kids[side]];
+                    if (cn.kind != Node::SCALAR) continue;
+                    const double cv = P == CHAI_F32 ? (double)(float)cn.scalar : cn.scalar;
+                    if (!(cv >= 1.0) || std::isinf(cv)) continue;
+                    ck = mn.kids[side];
+                    sk = mn.kids[1 - side];
+                    c_first = side == 0;
+                    break;
+                }
+                if (ck < 0 || nodes_[sk].prec != P) return false;
+                if (m.t < 0) {
+                    m.t = tk;
+                    m.c = ck;
+                    m.c_first = c_first;
+                } else if (m.t != tk || nodes_[m.c].scalar != nodes_[ck].scalar) {
+                    return false;
+                }
+                inner.push_back(k);
+                inner.push_back(mk);
+                const std::string vs = "v" + std::to_string(sk) + "[j]", vc = "v" + std::to_string(ck) + "[j]";
+                fs = vs;
+                ss = std::string("f2<14, ") + TT + ">(f2<13, " + TT + ">(" + (c_first ? vc + ", " + vs : vs + ", " + vc) +
+                     "), v" + std::to_string(tk) + "[j])";
+                return true;
+            };
+            std::string fs, ss;
+            if (!walk(r, true, fs, ss) || m.t < 0) continue;
+            m.fast = fs;
+            m.slow = ss;
+            fused[r] = m;
+            for (int k : inner) absorbed.insert(k);
+        }
+    }
     std::ostringstream os;
     std::vector<KArg> args;
     args.push_back({KArg::I64, nullptr, n});
     args.push_back({KArg::I64, nullptr, (long long)W});
     args.push_back({KArg::I64, nullptr, (long long)H});
     os << "extern \"C\" __global__ void __launch_bounds__(256";
-    if (mode2d && ctx_->cfg.stencil_min_blocks > 0) os << ", " << ctx_->cfg.stencil_min_blocks;
+    // stencil kernels: StencilMinBlocks CTAs per SM if set; a fused max tree
+    // keeps its sums live across the finiteness test, so those kernels ask
+    // for 5 (48 registers: 54 otherwise, 4 CTAs per SM, 4 % slower on Kirsch)
+    const int min_blocks = ctx_->cfg.stencil_min_blocks > 0 ? ctx_->cfg.stencil_min_blocks : fused.empty() ? 0 : 5;
+    if (mode2d && min_blocks > 0) os << ", " << min_blocks;
     os << ") chai_group(const long long n, const long long W, const long long H";
     bool need_xy = false;
     for (int i : body) {
@@ -341,101 +434,15 @@ int Translator::emit_group(const std::vector<int>& roots)
     }
     const double two_pi = 2.0 * ctx_->cfg.rng_pi;
     const int layout = ctx_->cfg.rng_layout;
-    // Max of monotone affine maps.  A tree of chai max ops (`a < b ? b : a`)
-    // whose leaves are all c * s_k - t, with one constant c >= 1 and one node
-    // t, equals c * m - t where m is the same tree over the s_k, bit for bit,
-    // whenever t is not infinite: s -> fl(fl(c s) - t) is monotone
-    // non-decreasing (rounding is monotone, c > 0), NaNs sit at the same
-    // leaves in both trees, two leaves with equal values have equal bits
-    // (with c >= 1, c s rounds to zero only for s = +-0, so the only
-    // signed-zero result, -0, comes from s = -0 and t = +0 and ties no larger
-    // s), and a NaN t makes every leaf the canonical NaN.  The kernel takes
-    // the short form per element and the original tree when t is infinite
-    // (inf - inf would break monotonicity).  Saves, per output of an n-leaf
-    // tree, n - 1 multiplies and n - 1 subtractions (Kirsch: 14 of ~63).
-    struct MaxAffine {
-        int t = -1, c = -1;
-        bool c_first = true;
-        std::string fast, slow;        // the tree over s_k / over c * s_k - t, element j
-    };
-    std::map<int, MaxAffine> fused;
-    std::set<int> absorbed;
-    if (ctx_->cfg.fuse_max_affine) {
-        std::map<int, int> uses;
-        for (int i : body)
-            for (int k : nodes_[i].kids) uses[k]++;
-        for (int r : roots) uses[r]++;
-        for (auto it = body.rbegin(); it != body.rend(); ++it) {
-            const int r = *it;
-            const Node& rn = nodes_[r];
-            if (absorbed.count(r) || loads.count(r) || rn.kind != Node::OP || rn.op != 302 || rn.kids.size() != 2 ||
-                (rn.prec != CHAI_F32 && rn.prec != CHAI_F64))
-                continue;
-            const int P = rn.prec;
-            const char* TT = ctype_of(P);
-            MaxAffine m;
-            std::vector<int> inner;
-            auto own = [&](int k) { return uses[k] == 1 && !root_set.count(k) && !loads.count(k); };
-            std::function<bool(int, bool, std::string&, std::string&)> walk =
-                [&](int k, bool top, std::string& fs, std::string& ss) -> bool {
-                const Node& n = nodes_[k];
-                if (n.kind == Node::OP && n.op == 302 && n.kids.size() == 2 && n.prec == P && (top || own(k))) {
-                    std::string f0, s0, f1, s1;
-                    if (!walk(n.kids[0], false, f0, s0) || !walk(n.kids[1], false, f1, s1)) return false;
-                    if (!top) inner.push_back(k);
-                    fs = std::string("f2<302, ") + TT + ">(" + f0 + ", " + f1 + ")";
-                    ss = std::string("f2<302, ") + TT + ">(" + s0 + ", " + s1 + ")";
-                    return true;
-                }
-                // leaf: sub(mul(c, s), t) (or mul(s, c)), owned by the tree
-                if (top || !own(k) || n.kind != Node::OP || n.op != 14 || n.kids.size() != 2 || n.prec != P) return false;
-                const int mk = n.kids[0], tk = n.kids[1];
-                const Node& mn = nodes_[mk];
-                if (!own(mk) || mn.kind != Node::OP || mn.op != 13 || mn.kids.size() != 2 || mn.prec != P ||
-                    nodes_[tk].prec != P)
-                    return false;
-                int ck = -1, sk = -1;
-                bool c_first = true;
-                for (int side = 0; side < 2; side++) {
-                    const Node& cn = nodes_[mn.kids[side]];
-                    if (cn.kind != Node::SCALAR) continue;
-                    const double cv = P == CHAI_F32 ? (double)(float)cn.scalar : cn.scalar;
-                    if (!(cv >= 1.0) || std::isinf(cv)) continue;
-                    ck = mn.kids[side];
-                    sk = mn.kids[1 - side];
-                    c_first = side == 0;
-                    break;
-                }
-                if (ck < 0 || nodes_[sk].prec != P) return false;
-                if (m.t < 0) {
-                    m.t = tk;
-                    m.c = ck;
-                    m.c_first = c_first;
-                } else if (m.t != tk || nodes_[m.c].scalar != nodes_[ck].scalar) {
-                    return false;
-                }
-                inner.push_back(k);
-                inner.push_back(mk);
-                const std::string vs = "v" + std::to_string(sk) + "[j]", vc = "v" + std::to_string(ck) + "[j]";
-                fs = vs;
-                ss = std::string("f2<14, ") + TT + ">(f2<13, " + TT + ">(" + (c_first ? vc + ", " + vs : vs + ", " + vc) +
-                     "), v" + std::to_string(tk) + "[j])";
-                return true;
-            };
-            std::string fs, ss;
-            if (!walk(r, true, fs, ss) || m.t < 0) continue;
-            m.fast = fs;
-            m.slow = ss;
-            fused[r] = m;
-            for (int k : inner) absorbed.insert(k);
-        }
-    }
     for (int i : body) {
         const Node& nd = nodes_[i];
         const char* T = ctype_of(nd.prec);
         if (absorbed.count(i)) continue;
         os << "    " << T << " v" << i << "[" << NV << "];\n";
         if (fused.count(i)) {
+            // the test per element (one per thread for all its elements
+            // issued fewer instructions, 53.9 against 56.1 per Kirsch output,
+            // but left less independent work: 155.4 against 148.6 us)
             const MaxAffine& m = fused[i];
             const std::string vc = "v" + std::to_string(m.c) + "[j]";
             os << "    " << JL << " { if (!isinf(v" << m.t << "[j])) { const " << T << " m = " << m.fast << "; v" << i
