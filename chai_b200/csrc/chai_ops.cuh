@@ -206,6 +206,14 @@ CHAI_F2FP(250, (decltype(a))pow(a, b))
 CHAI_F2FP(251, (decltype(a))remainder(a, b))
 CHAI_F2FP(254, (decltype(a))pow(a, (decltype(a))1 / (decltype(a))(int)b))
 CHAI_F2ALL(302, (a < b ? b : a))
+// IEEE maximum that returns NaN when either input is NaN (one instruction);
+// used by the translator's max-of-affine rewrite where NaN is tested for
+__device__ __forceinline__ float max_nan(float a, float b)
+{
+    float d;
+    asm("max.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
 CHAI_F2ALL(303, (a < b ? a : b))
 CHAI_F2FP(306, (decltype(a))(b < a ? 0 : 1))
 CHAI_F2INT(401, (decltype(a))(a < b ? b - a : a - b))

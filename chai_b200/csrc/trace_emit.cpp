@@ -236,10 +236,15 @@ int Translator::emit_group(const std::vector<int>& roots)
     // the short form per element and the original tree when t is infinite
     // (inf - inf would break monotonicity).  Saves, per output of an n-leaf
     // tree, n - 1 multiplies and n - 1 subtractions (Kirsch: 14 of ~63).
+    // f32 trees go one step further: with t finite and non-zero and no NaN
+    // among the s_k, the chai tree's pick equals the IEEE maximum in value,
+    // and a zero of either sign gives c * (+-0) - t = -t, so the tree runs as
+    // max.NaN.f32 (one instruction per node instead of compare + select),
+    // whose NaN result sends the element to the original tree.
     struct MaxAffine {
         int t = -1, c = -1;
         bool c_first = true;
-        std::string fast, slow;        // the tree over s_k / over c * s_k - t, element j
+        std::string fast, slow, nanfast;   // the tree over s_k / over c * s_k - t / over s_k by max.NaN, element j
     };
     std::map<int, MaxAffine> fused;
     std::set<int> absorbed;
@@ -259,15 +264,16 @@ int Translator::emit_group(const std::vector<int>& roots)
             MaxAffine m;
             std::vector<int> inner;
             auto own = [&](int k) { return uses[k] == 1 && !root_set.count(k) && !loads.count(k); };
-            std::function<bool(int, bool, std::string&, std::string&)> walk =
-                [&](int k, bool top, std::string& fs, std::string& ss) -> bool {
+            std::function<bool(int, bool, std::string&, std::string&, std::string&)> walk =
+                [&](int k, bool top, std::string& fs, std::string& ss, std::string& ns) -> bool {
                 const Node& n = nodes_[k];
                 if (n.kind == Node::OP && n.op == 302 && n.kids.size() == 2 && n.prec == P && (top || own(k))) {
-                    std::string f0, s0, f1, s1;
-                    if (!walk(n.kids[0], false, f0, s0) || !walk(n.kids[1], false, f1, s1)) return false;
+                    std::string f0, s0, n0, f1, s1, n1;
+                    if (!walk(n.kids[0], false, f0, s0, n0) || !walk(n.kids[1], false, f1, s1, n1)) return false;
                     if (!top) inner.push_back(k);
                     fs = std::string("f2<302, ") + TT + ">(" + f0 + ", " + f1 + ")";
                     ss = std::string("f2<302, ") + TT + ">(" + s0 + ", " + s1 + ")";
+                    ns = "max_nan(" + n0 + ", " + n1 + ")";
                     return true;
                 }
                 // leaf: sub(mul(c, s), t) (or mul(s, c)), owned by the tree
@@ -301,14 +307,16 @@ int Translator::emit_group(const std::vector<int>& roots)
                 inner.push_back(mk);
                 const std::string vs = "v" + std::to_string(sk) + "[j]", vc = "v" + std::to_string(ck) + "[j]";
                 fs = vs;
+                ns = vs;
                 ss = std::string("f2<14, ") + TT + ">(f2<13, " + TT + ">(" + (c_first ? vc + ", " + vs : vs + ", " + vc) +
                      "), v" + std::to_string(tk) + "[j])";
                 return true;
             };
-            std::string fs, ss;
-            if (!walk(r, true, fs, ss) || m.t < 0) continue;
+            std::string fs, ss, ns;
+            if (!walk(r, true, fs, ss, ns) || m.t < 0) continue;
             m.fast = fs;
             m.slow = ss;
+            if (P == CHAI_F32) m.nanfast = ns;
             fused[r] = m;
             for (int k : inner) absorbed.insert(k);
         }
@@ -445,9 +453,15 @@ int Translator::emit_group(const std::vector<int>& roots)
             // but left less independent work: 155.4 against 148.6 us)
             const MaxAffine& m = fused[i];
             const std::string vc = "v" + std::to_string(m.c) + "[j]";
-            os << "    " << JL << " { if (!isinf(v" << m.t << "[j])) { const " << T << " m = " << m.fast << "; v" << i
-               << "[j] = f2<14, " << T << ">(f2<13, " << T << ">(" << (m.c_first ? vc + ", m" : "m, " + vc) << "), v"
-               << m.t << "[j]); } else v" << i << "[j] = " << m.slow << "; }\n";
+            const std::string cm = m.c_first ? vc + ", m" : "m, " + vc;
+            if (!m.nanfast.empty())
+                os << "    " << JL << " { const " << T << " m = " << m.nanfast << "; const " << T << " t = v" << m.t
+                   << "[j]; if (!isinf(t) && t != (" << T << ")0 && !isnan(m)) v" << i << "[j] = f2<14, " << T
+                   << ">(f2<13, " << T << ">(" << cm << "), t); else v" << i << "[j] = " << m.slow << "; }\n";
+            else
+                os << "    " << JL << " { if (!isinf(v" << m.t << "[j])) { const " << T << " m = " << m.fast << "; v" << i
+                   << "[j] = f2<14, " << T << ">(f2<13, " << T << ">(" << cm << "), v" << m.t << "[j]); } else v" << i
+                   << "[j] = " << m.slow << "; }\n";
             continue;
         }
         if (loads.count(i)) {

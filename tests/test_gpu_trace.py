@@ -341,10 +341,10 @@ def test_kirsch_trace_bit_exact(ch):
 
 
 def _kirsch_tree_numpy(img):
-    """The traced Kirsch program in numpy f32, one IEEE operation at a time:
-    periodic neighbours, 8 * ((n_k + n_k+1) + n_k+2) - 3 * total, and the max
-    tree of chai's `a < b ? b : a`."""
-    f = np.float32
+    """The traced Kirsch program in numpy (the image's precision), one IEEE
+    operation at a time: periodic neighbours, 8 * ((n_k + n_k+1) + n_k+2) -
+    3 * total, and the max tree of chai's `a < b ? b : a`."""
+    f = img.dtype.type
     n = [np.roll(np.roll(img, -dy, 0), -dx, 1) for dx, dy in
          ((-1, -1), (0, -1), (1, -1), (1, 0), (1, 1), (0, 1), (-1, 1), (-1, 0))]
     with np.errstate(all="ignore"):
@@ -357,22 +357,27 @@ def _kirsch_tree_numpy(img):
     return mx(mx(mx(r[0], r[1]), mx(r[2], r[3])), mx(mx(r[4], r[5]), mx(r[6], r[7])))
 
 
-def test_max_affine_fusion_is_exact_on_special_values(ch):
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_max_affine_fusion_is_exact_on_special_values(ch, dt):
     """The max-of-affine rewrite (c * max(s_k) - t for a max tree of
-    c * s_k - t, FuseMaxAffine) against the plain tree (FuseMaxAffine=0) and
-    a numpy restatement, on an image with signed zeros, NaNs, infinities and
-    values whose 8 * s overflows: bit-identical on the GPU, and equal to
-    numpy except for the sign of NaNs (parity exception 7)."""
+    c * s_k - t, FuseMaxAffine; f32 trees through max.NaN) against the plain
+    tree (FuseMaxAffine=0) and a numpy restatement, on an image with signed
+    zeros, NaNs, infinities, subnormals and values whose 8 * s overflows:
+    bit-identical on the GPU, and equal to numpy except for the sign of NaNs
+    (parity exception 7)."""
     H, W = 64, 64
+    big = 3e38 if dt == np.float32 else 1.7e308
     rng = np.random.default_rng(21)
-    img = rng.uniform(0, 1, (H, W)).astype(np.float32)
-    img[8:16, 8:16] = np.where(rng.uniform(size=(8, 8)) < 0.5, np.float32(-0.0), np.float32(0.0))
+    img = rng.uniform(0, 1, (H, W)).astype(dt)
+    img[8:16, 8:16] = np.where(rng.uniform(size=(8, 8)) < 0.5, dt(-0.0), dt(0.0))
     img[10, 40] = np.nan
     img[30, 5] = np.inf
     img[50, 50] = -np.inf
-    img[40:43, 20:23] = np.float32(3e38)
-    img[20:22, 55:58] = np.float32(-3e38)
-    img[60, 1] = np.float32(1e-40)                 # a subnormal
+    img[40:43, 20:23] = dt(big)
+    img[20:22, 55:58] = dt(-big)
+    img[60, 1] = dt(1e-40 if dt == np.float32 else 1e-310)     # a subnormal
+    arr = ch.Arrayf32 if dt == np.float32 else ch.Arrayf64
+    ut = np.uint32 if dt == np.float32 else np.uint64
     outs = []
     for cfg in ("", "FuseMaxAffine=0"):
         saved = ch._vm
@@ -380,17 +385,18 @@ def test_max_affine_fusion_is_exact_on_special_values(ch):
         try:
             if dev:
                 ch._vm = dev
-            outs.append(ch.Arrayf32(kirsch_expr(ch, ch.make2(img), W, H)).read2())
+            outs.append(arr(kirsch_expr(ch, ch.make2(img), W, H)).read2())
         finally:
             ch._vm = saved
             if dev:
                 dev.close()
     fused, plain = outs
-    assert np.array_equal(fused.view(np.uint32), plain.view(np.uint32))
+    assert fused.dtype == dt
+    assert np.array_equal(fused.view(ut), plain.view(ut))
     want = _kirsch_tree_numpy(img)
     nan = np.isnan(want)
     assert np.array_equal(np.isnan(fused), nan)
-    assert np.array_equal(fused[~nan].view(np.uint32), want[~nan].view(np.uint32))
+    assert np.array_equal(fused[~nan].view(ut), want[~nan].view(ut))
     assert (fused == 0).any() and np.isinf(fused).any() and nan.any()
 
 
