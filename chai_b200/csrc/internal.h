@@ -31,7 +31,7 @@ struct Config {
     std::string tune_journal;                // crash-safe TRY / OK markers of every timing
     bool plan_cache = true;                  // replay recorded plans of repeated traces
     int plan_graph = -1;                     // replay plans from captured CUDA graphs: 1 on, 0 off, -1 unless kernel timing
-    int stencil_rows = 32;                   // output rows per stencil tile (multiple of 8, <= 64)
+    int stencil_rows = 0;                    // output rows per stencil tile (multiple of 8, <= 64; 0: 64 or 32 per kernel)
     bool fuse_max_affine = true;             // max of c * s_k - t leaves -> c * max(s_k) - t (exact when t is finite)
     bool reduce_accum_f32 = false;           // f32 reductions: per-thread partials in f32 (block tree, combine FP64)
     int stencil_rows_per_thread = 1;         // output rows per stencil thread (1, 2 or 4; 4 columns each)
