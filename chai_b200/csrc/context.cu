@@ -173,6 +173,8 @@ void parse_config(chai::Config& c, const char* text)
             c.gemm_pair_seg = std::max(1, atoi(v.c_str()));
         } else if (k == "GemmStages") {
             c.gemm_stages = std::max(0, atoi(v.c_str()));
+        } else if (k == "GroupedPair") {
+            c.grouped_pair = v != "0" && v != "off";
         } else if (k == "GroupedTmaB") {
             c.grouped_tma_b = v != "0" && v != "off";
         } else if (k == "GroupedExact") {

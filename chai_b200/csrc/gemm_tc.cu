@@ -124,6 +124,35 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int* st
     }
 }
 
+// The same, acquiring at cluster scope: for barriers that threads of the
+// other CTA of a pair arrive on (their writes before the arrive are visible
+// after the wait)
+__device__ __forceinline__ bool mbar_try_wait_cluster(unsigned bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(bar), "r"(parity), "r"(1000u)
+                 : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_cluster(unsigned bar, unsigned parity, int* status, int code,
+                                                  unsigned long long limit_ns = WAIT_NS)
+{
+    if (mbar_try_wait_cluster(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        if (mbar_try_wait_cluster(bar, parity)) return true;
+        if (global_ns() - t0 > limit_ns) {
+            atomicExch(status, code);
+            return false;
+        }
+    }
+}
+
 // Self-test of the bounded wait: one thread waits on an mbarrier that nothing
 // ever arrives on; the wait must give up after limit_ns and report `code`.
 __global__ void chai_wait_selftest(int* status, unsigned long long limit_ns, int code)
@@ -1338,22 +1367,25 @@ struct __align__(16) FsTile {
 
 static_assert(sizeof(FsTile) == 64, "tile record size");
 
-__global__ void __launch_bounds__(128) fs_tiles(const FusedEntry* __restrict__ groups, FsTile* __restrict__ out)
+// tile records of TM x TN output tiles (128 x 128 for the one-CTA kernel,
+// 256 x 256 for the CTA-pair kernel)
+__global__ void __launch_bounds__(128) fs_tiles(const FusedEntry* __restrict__ groups, FsTile* __restrict__ out, int TM,
+                                                int TN)
 {
     const FusedEntry g = groups[blockIdx.x];
-    const int tiles = ((g.m + BM - 1) / BM) * g.tiles_n;
+    const int tiles = ((g.m + TM - 1) / TM) * g.tiles_n;
     for (int l = threadIdx.x; l < tiles; l += blockDim.x) {
         const int tm = l / g.tiles_n, tn = l - tm * g.tiles_n;
         FsTile t;
-        t.a = g.a + (long long)tm * BM * g.k;
-        t.b = g.b + (long long)tn * FS_BN;
-        t.c = g.c + (long long)tm * BM * g.n + (long long)tn * FS_BN;
+        t.a = g.a + (long long)tm * TM * g.k;
+        t.b = g.b + (long long)tn * TN;
+        t.c = g.c + (long long)tm * TM * g.n + (long long)tn * TN;
         t.prob = blockIdx.x;
         t.n = g.n;
         t.k = g.k;
-        t.col0 = tn * FS_BN;
-        t.rows = min(BM, g.m - tm * BM);
-        t.cols = min(FS_BN, g.n - tn * FS_BN);
+        t.col0 = tn * TN;
+        t.rows = min(TM, g.m - tm * TM);
+        t.cols = min(TN, g.n - tn * TN);
         t.kblocks = g.kblocks;
         t.vec_ok = g.vec_ok;
         out[g.tile_start + l] = t;
@@ -1927,6 +1959,258 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
     }
 }
 
+// ---------------------------------------- grouped GEMM, split in-kernel, CTA pair
+//
+// chai_gemm_fused_pair: the in-kernel split of chai_gemm_fused_split on
+// 256 x 256 output tiles computed by a cluster of two CTAs with
+// tcgen05.mma.cta_group::2 (M = 256).  CTA r of the pair converts rows
+// 128 r .. 128 r + 127 of the tile's A and columns 128 r .. 128 r + 127 of
+// its B into its own plane buffers (the same per-CTA planes, layouts and
+// thread-to-element map as the one-CTA kernel), so a chunk of A and B read
+// by an SM feeds twice the output: the group's operand reads from L2 fall
+// from 6.37 to 3.77 GB (the unique bytes are 3.68 GB) and the chunk steps
+// per SM by 30 %.  The leader's MMA thread waits until the converters of
+// both CTAs have written a chunk (its plane-full barrier counts both CTAs'
+// warps), issues the S product blocks, and commits to both CTAs'
+// plane-empty and accumulator barriers (commit multicast); each CTA's four
+// epilogue warps store its 128 accumulator rows (all 256 columns) and arrive
+// on the leader's accumulator-empty barrier.  The MMA sequence per output
+// element is the one-CTA kernel's, so C is bit-identical to it.  bf16 and
+// bf16x3 with one accumulator (K <= 2048); the rest take the one-CTA kernel.
+constexpr int FP_BN = 256;                     // pair tile columns (128 per CTA)
+
+// MMA width of a pair tile with `cols` valid columns: a multiple of 32, so
+// each CTA's half is a multiple of 16
+__device__ __forceinline__ int fp_cols(int cols) { return min(FP_BN, max(32, (cols + 31) & ~31)); }
+
+template <int S>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(FS_THREADS, 1)
+chai_gemm_fused_pair(const FsTile* __restrict__ tiles, long long ntiles, int* status, int flags)
+{
+    constexpr int P = Planes<S>::P;
+    constexpr int SEL = S == 1 ? 0 : (S == 3 ? 1 : 2);
+    constexpr int NPB = fs_pbufs(S);
+    constexpr int PBUF = 2 * P * FS_PLANE;
+    constexpr unsigned TMEM_COLS = 2 * FP_BN;                      // double-buffered 256-column accumulators
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* planes = smem;
+    float* estage = reinterpret_cast<float*>(planes + NPB * PBUF);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(planes + NPB * PBUF + FS_ESTAGE);
+    unsigned long long* pfull = bars;          // [2] leader: converter warps of both CTAs
+    unsigned long long* pempty = bars + 2;     // [2] each CTA: MMA commit (multicast)
+    unsigned long long* tfull = bars + 4;      // [2] each CTA: MMA commit (multicast)
+    unsigned long long* tempty = bars + 6;     // [2] leader: epilogue warps of both CTAs
+    unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 8);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    unsigned long long* drain = bars + 9;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned rank = cta_rank();
+    const bool leader = rank == 0;
+    const long long pair = cluster_index(), npairs = cluster_count();
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&pfull[b]), 2 * FS_CONV);
+            mbar_init(smem_u32(&pempty[b]), 1);
+            mbar_init(smem_u32(&tfull[b]), 1);
+            mbar_init(smem_u32(&tempty[b]), 8);
+        }
+        mbar_init(smem_u32(drain), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    // both CTAs' barriers initialised before either signals the other's
+    cluster_sync_all();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // idle: both operands reach shared memory through the converters
+    } else if (warp == 1) {
+        // ---------------------------------------------------------------- MMA
+        if (leader && lane == 0) {
+            // M = 256 (cta_group::2), N = 256, B MN-major
+            const unsigned idesc_full = (instr_desc<KIND_BF16, FP_BN>() & ~(31u << 24)) | (16u << 24) | (1u << 16);
+            const bool exact = flags & FS_EXACT;
+            long long it = 0;
+            int lt = 0;
+            int4 nx = make_int4(0, 0, 0, 0);           // kblocks, k, cols of the next tile (loaded one tile ahead)
+            if (pair < ntiles) nx = make_int4(tiles[pair].kblocks, tiles[pair].k, tiles[pair].cols, 0);
+            for (long long t = pair; t < ntiles && !*abort_flag; t += npairs, lt++) {
+                const int kbs = nx.x, tk = nx.y, tcols = nx.z;
+                if (t + npairs < ntiles)
+                    nx = make_int4(tiles[t + npairs].kblocks, tiles[t + npairs].k, tiles[t + npairs].cols, 0);
+                // exact: N = the tile's columns rounded up to 32 (each CTA
+                // supplies N / 2 columns of B, a multiple of 16)
+                const unsigned idesc = exact ? ((idesc_full & ~(0x3Fu << 17)) | ((unsigned)(fp_cols(tcols) >> 3) << 17))
+                                             : idesc_full;
+                const int ab = lt & 1, use = lt >> 1;
+                if (use >= 1 && !mbar_wait_cluster(smem_u32(&tempty[ab]), (unsigned)((use - 1) & 1), status, 135)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const unsigned acc = tmem + (unsigned)ab * FP_BN;
+                bool ok = true;
+                for (int kb = 0; kb < kbs; kb++, it++) {
+                    const int q = (int)(it % NPB);
+                    if (!mbar_wait_cluster(smem_u32(&pfull[q]), (unsigned)((it / NPB) & 1), status, 133)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const unsigned char* pa = planes + q * PBUF;
+                    const unsigned char* pb = pa + P * FS_PLANE;
+                    const int ks = exact ? min(4, (tk - kb * FS_KB + 15) >> 4) : 4;
+#pragma unroll
+                    for (int blk = 0; blk < S; blk++) {
+                        const unsigned a0 = smem_u32(pa + kSelA[SEL][blk] * FS_PLANE);
+                        const unsigned b0 = smem_u32(pb + kSelB[SEL][blk] * FS_PLANE);
+                        const bool first = kb == 0 && blk == 0;
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                            if (k < ks)
+                                mma_pair<KIND_BF16>(acc, smem_desc(a0 + 32 * k), smem_desc_mn(b0 + 2 * FS_B_SBO * k),
+                                                    idesc, !(first && k == 0));
+                    }
+                    mma_commit_pair(smem_u32(&pempty[q]));     // both CTAs' buffer q free once these MMAs finish
+                }
+                if (!ok) {
+                    *abort_flag = 1;
+                    break;
+                }
+                mma_commit_pair(smem_u32(&tfull[ab]));         // accumulator ab complete in both CTAs
+            }
+            mma_commit_pair(smem_u32(drain));
+            mbar_wait(smem_u32(drain), 0, status, 136);
+        }
+    } else if (warp < 6) {
+        // ----------------------------------------------------------- epilogue
+        // this CTA's 128 accumulator rows, all 256 columns, through the stage
+        const int quarter = warp & 3;
+        const int r = quarter * 32 + lane;
+        float* es = estage + quarter * (32 * FS_EP);
+        const unsigned tempty0 = map_to_rank(smem_u32(&tempty[0]), 0);
+        int lt = 0;
+        for (long long t = pair; t < ntiles; t += npairs, lt++) {
+            const FsTile ti = tiles[t];
+            const int ab = lt & 1;
+            const bool ok = mbar_wait(smem_u32(&tfull[ab]), (unsigned)((lt >> 1) & 1), status, 134);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int rows = max(0, min(BM, ti.rows - (int)rank * BM));
+            float* cbase = ti.c + (long long)rank * BM * ti.n;
+            const bool do_store = ok && !*abort_flag && r < rows;
+            const unsigned tbase = tmem + ((unsigned)(quarter * 32) << 16) + (unsigned)ab * FP_BN;
+#pragma unroll 1
+            for (int c0 = 0; c0 < FP_BN; c0 += 32) {
+                unsigned r0[32];
+                tmem_ld32_nowait(tbase + (unsigned)c0, r0);              // warp-wide, always executed
+                tmem_wait();
+                if (c0 >= ti.cols) continue;               // uniform across the warp
+                if (ti.vec_ok) {
+                    __syncwarp();
+                    float4* er = reinterpret_cast<float4*>(es + lane * FS_EP);
+#pragma unroll
+                    for (int q = 0; q < 8; q++)
+                        er[q] = make_float4(__uint_as_float(r0[4 * q]), __uint_as_float(r0[4 * q + 1]),
+                                            __uint_as_float(r0[4 * q + 2]), __uint_as_float(r0[4 * q + 3]));
+                    __syncwarp();
+                    const bool go = ok && !*abort_flag;
+                    const int col = c0 + 4 * (lane & 7);
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const int row = 4 * i + (lane >> 3);
+                        const float4 x = *reinterpret_cast<const float4*>(es + row * FS_EP + 4 * (lane & 7));
+                        if (go && quarter * 32 + row < rows && col < ti.cols)
+                            *reinterpret_cast<float4*>(cbase + (long long)(quarter * 32 + row) * ti.n + col) = x;
+                    }
+                } else {
+                    if (!do_store) continue;
+                    float* crow = cbase + (long long)r * ti.n;
+#pragma unroll
+                    for (int i = 0; i < 32; i++)
+                        if (c0 + i < ti.cols) crow[c0 + i] = __uint_as_float(r0[i]);
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(tempty0 + (unsigned)(ab * 8));
+            if (!ok || *abort_flag) break;
+        }
+    } else {
+        // --------------------------------------------------------- converters
+        // this CTA's half: A rows 128 rank .. +127 and B columns 128 rank .. +127
+        const int cw = warp - 6;
+        const int ct = threadIdx.x - 6 * 32;
+        const unsigned pfull0 = map_to_rank(smem_u32(&pfull[0]), 0);
+        const bool exact = flags & FS_EXACT;
+        auto half = [&](FsTile t) {
+            // exact: CTA r converts columns r N/2 .. (r + 1) N/2 - 1 of an
+            // N = fp_cols(cols) wide MMA; else r 128 .. r 128 + 127
+            const int hn = exact ? fp_cols(t.cols) / 2 : FS_BN;
+            t.a += (long long)rank * BM * t.k;
+            t.rows = max(0, min(BM, t.rows - (int)rank * BM));
+            t.b += (int)rank * hn;
+            t.cols = max(0, min(hn, t.cols - (int)rank * hn));
+            return t;
+        };
+        long long lt_ = pair;
+        int lkb = 0;
+        FsTile lti, lnext;
+        if (lt_ < ntiles) lti = half(tiles[lt_]);
+        if (lt_ + npairs < ntiles) lnext = half(tiles[lt_ + npairs]);
+        auto advance = [&]() {
+            if (++lkb < lti.kblocks) return;
+            lkb = 0;
+            lt_ += npairs;
+            lti = lnext;
+            if (lt_ + npairs < ntiles) lnext = half(tiles[lt_ + npairs]);
+        };
+        FsA ra;
+        FsB rb;
+        bool have = lt_ < ntiles;
+        if (have) {
+            fs_load_a(ra, lti, 0, cw, lane);
+            fs_load_b(rb, lti, 0, ct);
+            advance();
+        }
+        bool ok = true;
+        for (long long it = 0; have && !*abort_flag; it++) {
+            const int q = (int)(it % NPB);
+            if (it >= NPB) ok = mbar_wait(smem_u32(&pempty[q]), (unsigned)((it / NPB - 1) & 1), status, 137);
+            if (!ok) break;
+            unsigned char* pa = planes + q * PBUF;
+            fs_convert<P>(ra, rb, pa, pa + P * FS_PLANE, cw, lane, ct);
+            // the tensor core reads the planes through the async proxy
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(pfull0 + (unsigned)(q * 8));
+            have = lt_ < ntiles;
+            if (have) {
+                fs_load_a(ra, lti, lkb, cw, lane);
+                fs_load_b(rb, lti, lkb, ct);
+                advance();
+            }
+        }
+        if (!ok && lane == 0) *abort_flag = 1;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    // neither CTA frees TMEM or exits while the other still signals it
+    cluster_sync_all();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
 }  // namespace tc
 
 // ---------------------------------------------------------------- host side
@@ -2078,6 +2362,8 @@ void preload_gemm_kernels()
     cudaFuncGetAttributes(&a, chai_gemm_fused_split<1, false, true>);
     cudaFuncGetAttributes(&a, chai_gemm_fused_split<3, false, true>);
     cudaFuncGetAttributes(&a, chai_gemm_fused_split<3, true, true>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_pair<1>);
+    cudaFuncGetAttributes(&a, chai_gemm_fused_pair<3>);
 }
 
 int launch_wait_selftest(chai_cuda_ctx* ctx, double limit_ms)
@@ -2305,7 +2591,13 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
     using namespace tc;
     chai_cuda_ctx::GroupedPlan& gp = ctx->gplan;
     cudaStream_t s = ctx->stream;
-    const bool same = gp.dev && gp.S == S && gp.problems.size() == (size_t)count &&
+    // 256 x 256 CTA-pair tiles (GroupedPair) for bf16 / bf16x3 with one
+    // accumulator (every K <= 2048) and B in the converters' registers
+    long long kmax_all = 0;
+    for (int i = 0; i < count; i++) kmax_all = std::max<long long>(kmax_all, (long long)((p[i].k + FS_KB - 1) / FS_KB) * FS_KB);
+    const bool pair = ctx->cfg.grouped_pair && (S == 1 || S == 3) && kmax_all <= 2048 && !ctx->cfg.grouped_tma_b;
+    const int TM = pair ? 2 * BM : BM, TN = pair ? FP_BN : FS_BN;
+    const bool same = gp.dev && gp.S == S && gp.pair == pair && gp.problems.size() == (size_t)count &&
                       memcmp(gp.problems.data(), p, sizeof(chai_gemm_problem) * count) == 0;
     if (!same) {
         std::vector<FusedEntry> g(count);
@@ -2320,10 +2612,10 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
             e.m = q.m;
             e.n = q.n;
             e.k = q.k;
-            e.tiles_n = (q.n + FS_BN - 1) / FS_BN;
+            e.tiles_n = (q.n + TN - 1) / TN;
             e.kblocks = (q.k + FS_KB - 1) / FS_KB;
             e.vec_ok = ((reinterpret_cast<uintptr_t>(q.c) & 15) == 0 && q.n % 4 == 0) ? 1 : 0;
-            tiles += (long long)((q.m + BM - 1) / BM) * e.tiles_n;
+            tiles += (long long)((q.m + TM - 1) / TM) * e.tiles_n;
             kmax = std::max<long long>(kmax, (long long)e.kblocks * FS_KB);
         }
         if (tiles >= (1ll << 31)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "grouped gemm: too large");
@@ -2339,10 +2631,11 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
         if (st) return st;
         FusedEntry* dg = static_cast<FusedEntry*>(ctx->scratch);
         CHAI_CUDA_TRY(ctx, cudaMemcpyAsync(dg, g.data(), g.size() * sizeof(FusedEntry), cudaMemcpyHostToDevice, s));
-        fs_tiles<<<(unsigned)count, 128, 0, s>>>(dg, static_cast<FsTile*>(gp.dev));
+        fs_tiles<<<(unsigned)count, 128, 0, s>>>(dg, static_cast<FsTile*>(gp.dev), TM, TN);
         CHAI_CUDA_TRY(ctx, cudaGetLastError());
         gp.problems.assign(p, p + count);
         gp.S = S;
+        gp.pair = pair;
         gp.tiles = tiles;
         // the same accumulator rule as the prepass path (see launch_gemm_grouped)
         gp.acc2 = S == 6 || kmax > 2048;
@@ -2384,6 +2677,25 @@ static int launch_grouped_fused(chai_cuda_ctx* ctx, int S, const chai_gemm_probl
     cudaEvent_t ev[2];
     ktime_begin(ctx, "gemm_grouped", ev);
     const CUtensorMap* maps = static_cast<const CUtensorMap*>(gp.maps);
+    if (pair) {
+        // clusters of two CTAs, at most one per two SMs
+        const unsigned pgrid = 2 * (unsigned)std::min<long long>(tiles, ctx->sm_count / 2);
+#define CHAI_FP(SS)                                                                                  \
+    do {                                                                                             \
+        auto k = chai_gemm_fused_pair<SS>;                                                           \
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, fs_smem_bytes(SS));    \
+        k<<<pgrid, FS_THREADS, fs_smem_bytes(SS), s>>>(dt, tiles, ctx->status_word, flags);          \
+    } while (0)
+        cudaEvent_t pev[2];
+        ktime_begin(ctx, "gemm_grouped", pev);
+        if (S == 1) CHAI_FP(1);
+        else CHAI_FP(3);
+#undef CHAI_FP
+        CHAI_CUDA_TRY(ctx, cudaGetLastError());
+        ktime_end(ctx, "gemm_grouped", pev);
+        ctx->fused_launches++;
+        return CHAI_OK;
+    }
 #define CHAI_FS(SS, A2, BTV)                                                                         \
     do {                                                                                             \
         auto k = chai_gemm_fused_split<SS, A2, BTV>;                                                 \

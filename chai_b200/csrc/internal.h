@@ -36,6 +36,7 @@ struct Config {
     bool reduce_accum_f32 = false;           // f32 reductions: per-thread partials in f32 (block tree, combine FP64)
     int stencil_rows_per_thread = 1;         // output rows per stencil thread (1, 2 or 4; 4 columns each)
     int stencil_min_blocks = 0;              // __launch_bounds__ minimum blocks per SM for stencil kernels (0: none)
+    bool grouped_pair = true;                // in-kernel split on 256 x 256 CTA-pair tiles (bf16, bf16x3, K <= 2048)
     bool grouped_tma_b = false;              // in-kernel split: B chunks through TMA (bf16, bf16x3; slower, see gemm_tc.cu)
     bool grouped_exact = true;               // in-kernel split: MMAs cover each tile's N and last K (rounded to 16)
     bool grouped_fused = true;               // grouped GEMM splits f32 operands inside the kernel (else prepass planes)
@@ -104,6 +105,7 @@ struct chai_cuda_ctx {
         void* maps = nullptr;        // per-problem B tensor maps (B through TMA)
         size_t map_bytes = 0;
         bool bt = false;             // maps valid for `problems`
+        bool pair = false;           // tile records of 256 x 256 CTA-pair tiles
     } gplan;
     uint64_t fused_launches = 0;
 };

@@ -147,3 +147,23 @@ def test_tma_b_equals_register_b(chai_dev, prec):
         dev.close()
     for i, (a, b) in enumerate(zip(bt, reg)):
         assert np.array_equal(a, b), (i, shapes[i])
+
+
+@pytest.mark.parametrize("prec", [L.GEMM_BF16, L.GEMM_BF16X3])
+def test_pair_tiles_equal_one_cta_kernel(chai_dev, prec):
+    """256 x 256 output tiles on CTA pairs (tcgen05.mma.cta_group::2, each
+    CTA converting half of A's rows and half of B's columns) against the
+    one-CTA kernel's 128 x 128 tiles (GroupedPair=0): the same per-element
+    product sequence, so C is bit-identical -- M and N below, at and past
+    the 256 edge, N of 4, K tails."""
+    import chai_b200.api as ch
+    shapes = problems(60, seed=17) + [(256, 256, 64), (257, 260, 72), (128, 512, 100), (512, 128, 36), (3, 4, 4),
+                                      (300, 4, 200), (8, 520, 8), (264, 8, 512)]
+    _, _, pair = run_grouped(chai_dev, shapes, prec, seed=7)
+    dev = ch.Device(config="GroupedPair=0")
+    try:
+        _, _, one = run_grouped(dev, shapes, prec, seed=7)
+    finally:
+        dev.close()
+    for i, (a, b) in enumerate(zip(pair, one)):
+        assert np.array_equal(a, b), (i, shapes[i])
