@@ -855,7 +855,7 @@ def run_grouped(args, L, ctx, stream):
     t_tc = flops * tensor_mult / (P["bf16_tflops"] * 1e12)
     gbs = alg_bytes / (kern * 1e-3) / 1e9
     common = {"traffic": traffic("gemm_grouped"), "peak_source": kind, "kernel_ms": kern,
-              "kernel": "chai_gemm_fused_split (grouped, operands split in-kernel)",
+              "kernel": "chai_gemm_fused_pair (grouped, operands split in-kernel, 256x256 CTA-pair tiles)",
               "algorithmic_bytes": alg_bytes, "algorithmic_tensor_flops": flops * tensor_mult,
               "tensor_frac": ach / P["bf16_tflops"], "hbm_frac": gbs / P["hbm_gbs"],
               "floor_ms": {"hbm": t_hbm * 1e3, "tensor": t_tc * 1e3}}
