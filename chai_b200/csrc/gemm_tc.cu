@@ -612,11 +612,17 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
 constexpr int PAIR_THREADS = 320;           // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 
 // a pair tile is 256 x BN (BN = 128 or 256): each CTA stages 128 rows of A
-// and BN / 2 rows of B per K block
-template <int ST, int BN>
+// and BN / 2 rows of B per K block.  A stage holds one 64-element K chunk
+// with every distinct plane of both operands (P planes: 1 plain, 2 bf16x3,
+// 3 bf16x6), so a plane that several split products use (a0, b0) crosses
+// from L2 once per chunk, not once per product.  ST counts the smem of ST
+// single-plane blocks; it buys max(2, ST / P) chunk stages.
+template <int ST, int BN, int S = 1>
 struct PairShape {
+    static constexpr int P = S == 1 ? 1 : (S == 3 ? 2 : 3);
     static constexpr int B_STAGE = (BN / 2) * KB_BYTES;
-    static constexpr int SMEM_BYTES = ST * (A_STAGE + B_STAGE) + 1024 + 256;
+    static constexpr int CST = ST / P >= 2 ? ST / P : 2;      // chunk stages
+    static constexpr int SMEM_BYTES = CST * P * (A_STAGE + B_STAGE) + 1024 + 256;
 };
 
 __device__ __forceinline__ unsigned cta_rank()
@@ -707,20 +713,22 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
     constexpr bool SPLIT = S > 1;
     constexpr int BN = BNT;                                    // pair tile columns
     constexpr int HB = BN / 2;                                 // B rows per CTA; accumulator columns per epilogue warp
-    constexpr int PAIR_B_STAGE = PairShape<ST, BN>::B_STAGE;
+    constexpr int PAIR_B_STAGE = PairShape<ST, BN, S>::B_STAGE;
+    constexpr int P = PairShape<ST, BN, S>::P;                 // distinct planes per operand
+    constexpr int CST = PairShape<ST, BN, S>::CST;             // chunk stages
     constexpr unsigned TMEM_COLS = 2 * BN;                     // split: main + corr; plain: two accumulators
     constexpr int NB = SPLIT ? 1 : 2;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char* sa = smem;
-    unsigned char* sb = smem + ST * A_STAGE;
-    unsigned long long* bars = reinterpret_cast<unsigned long long*>(sb + ST * PAIR_B_STAGE);
+    unsigned char* sa = smem;                                  // [CST][P] A planes of a chunk
+    unsigned char* sb = smem + CST * P * A_STAGE;              // [CST][P] B planes of a chunk
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(sb + CST * P * PAIR_B_STAGE);
     unsigned long long* full = bars;
-    unsigned long long* empty = bars + ST;
-    unsigned long long* tfull = bars + 2 * ST;
-    unsigned long long* tempty = bars + 2 * ST + 2;
-    unsigned long long* drain = bars + 2 * ST + 4;
-    unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * ST + 5);
+    unsigned long long* empty = bars + CST;
+    unsigned long long* tfull = bars + 2 * CST;
+    unsigned long long* tempty = bars + 2 * CST + 2;
+    unsigned long long* drain = bars + 2 * CST + 4;
+    unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 2 * CST + 5);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -728,11 +736,9 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
     const bool leader = rank == 0;
     const int pair = (int)cluster_index(), npairs = (int)cluster_count();
     const int ntiles = tg.tiles_m * tg.tiles_n * tg.batch;
-    // K blocks per tile: S product blocks per 64-element chunk
-    const int kblocks = kchunks * S;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < ST; s++) {
+        for (int s = 0; s < CST; s++) {
             mbar_init(smem_u32(&full[s]), 1);
             mbar_init(smem_u32(&empty[s]), 1);
         }
@@ -765,31 +771,29 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
                 int tm, tn, tb;
                 tile_coords(tg, t, tm, tn, tb);
                 const int arow = tm * 256 + (int)rank * 128, brow = tn * BN + (int)rank * HB;
-                for (int kb = 0; kb < kblocks; kb++, it++) {
-                    const int s = (int)(it % ST);
-                    const long long r = it / ST;
+                for (int c = 0; c < kchunks; c++, it++) {
+                    const int s = (int)(it % CST);
+                    const long long r = it / CST;
                     if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (unsigned)((r - 1) & 1), status, 121)) {
                         *abort_flag = 1;
                         break;
                     }
-                    if (leader) mbar_expect_tx(smem_u32(&full[s]), 2 * (A_STAGE + PAIR_B_STAGE));
-                    int xa = kb * kx_mul, xb = xa;
-                    if (SPLIT) {
-                        const int blk = kb % S, chunk = kb / S;
-                        const int sel = S == 3 ? 1 : 2;
-                        xa = kSelA[sel][blk] * tg.plane_k + chunk * kx_mul;
-                        xb = kSelB[sel][blk] * tg.plane_k + chunk * kx_mul;
-                    }
+                    if (leader) mbar_expect_tx(smem_u32(&full[s]), 2 * P * (A_STAGE + PAIR_B_STAGE));
                     const unsigned fb = full0 + (unsigned)(s * 8);
-                    tma_load_3d_pair(smem_u32(sa + s * A_STAGE), &map_a, fb, xa, arow, tb);
-                    tma_load_3d_pair(smem_u32(sb + s * PAIR_B_STAGE), &map_b, fb, xb, brow, tb);
+                    // the chunk's P planes of A and of B (plane p at column p * plane_k)
+#pragma unroll
+                    for (int pl = 0; pl < P; pl++) {
+                        const int x = (SPLIT ? pl * tg.plane_k : 0) + c * kx_mul;
+                        tma_load_3d_pair(smem_u32(sa + (s * P + pl) * A_STAGE), &map_a, fb, x, arow, tb);
+                        tma_load_3d_pair(smem_u32(sb + (s * P + pl) * PAIR_B_STAGE), &map_b, fb, x, brow, tb);
+                    }
                     issued = it + 1;
                 }
             }
             if (leader) {
-                // every copy of both CTAs has landed once the last ST phases completed
-                for (long long j = issued - ST < 0 ? 0 : issued - ST; j < issued; j++)
-                    mbar_wait(smem_u32(&full[j % ST]), (unsigned)((j / ST) & 1), status, 122);
+                // every copy of both CTAs has landed once the last CST phases completed
+                for (long long j = issued - CST < 0 ? 0 : issued - CST; j < issued; j++)
+                    mbar_wait(smem_u32(&full[j % CST]), (unsigned)((j / CST) & 1), status, 122);
             }
             if (*abort_flag) spin_ns(1000000);   // abort: let the peer's copies in flight land
         }
@@ -818,26 +822,31 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
                         }
                         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     }
-                    for (int blk = 0; blk < S; blk++, it++) {
-                        const int s = (int)(it % ST);
-                        if (!mbar_wait(smem_u32(&full[s]), (unsigned)((it / ST) & 1), status, 123)) {
-                            ok = false;
-                            break;
-                        }
-                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                        const unsigned a0 = smem_u32(sa + s * A_STAGE), b0 = smem_u32(sb + s * PAIR_B_STAGE);
+                    const int s = (int)(it % CST);
+                    if (!mbar_wait(smem_u32(&full[s]), (unsigned)((it / CST) & 1), status, 123)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const int sel = S == 3 ? 1 : 2;
+#pragma unroll
+                    for (int blk = 0; blk < S; blk++) {
+                        const int pa = SPLIT ? kSelA[sel][blk] : 0, pb = SPLIT ? kSelB[sel][blk] : 0;
+                        const unsigned a0 = smem_u32(sa + (s * P + pa) * A_STAGE);
+                        const unsigned b0 = smem_u32(sb + (s * P + pb) * PAIR_B_STAGE);
                         const unsigned acc = blk == 0 ? acc_main : acc_corr;
                         const bool first = blk == 0 ? seg_start : (c == 0 && blk == 1);
 #pragma unroll
                         for (int k = 0; k < KB_BYTES / 32; k++)
                             mma_pair<KIND>(acc, smem_desc(a0 + 32 * k), smem_desc(b0 + 32 * k), idesc,
                                            !(first && k == 0));
-                        mma_commit_pair(smem_u32(&empty[s]));        // stage free in both CTAs
                         if (SPLIT && blk == 0 && (c % seg == seg - 1) && c != kchunks - 1) {
                             mma_commit_pair(smem_u32(&tfull[0]));    // segment sum ready to drain
                             seg_no++;
                         }
                     }
+                    mma_commit_pair(smem_u32(&empty[s]));            // stage free in both CTAs
+                    it++;
                 }
                 if (!ok) {
                     *abort_flag = 1;
@@ -2277,7 +2286,7 @@ static int launch_pair(chai_cuda_ctx* ctx, const TcCfg& c, const CUtensorMap& ma
 #define CHAI_PAIR_V(STV, BNV)                                                                               \
     do {                                                                                                    \
         auto k = chai_gemm_pair<KIND, S, STV, BNV>;                                                         \
-        const int sm = PairShape<STV, BNV>::SMEM_BYTES;                                                     \
+        const int sm = PairShape<STV, BNV, S>::SMEM_BYTES;                                                  \
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                          \
         k<<<grid, PAIR_THREADS, sm, ctx->stream>>>(ma, mb, kchunks, seg, tg, ep, ctx->status_word);         \
     } while (0)
