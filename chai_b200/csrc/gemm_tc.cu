@@ -502,7 +502,7 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
         int lt = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
             const int ab = lt % NB;
-            const bool ok = mbar_wait(smem_u32(&tfull[ab]), (unsigned)((lt / NB) & 1), status, 104);
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&tfull[ab]), (unsigned)((lt / NB) & 1), status, 104));   // warp-uniform
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const TileInfo ti = tile_info<GROUPED, BN>(t, tg, ep, kblocks, groups, ngroups);
             const int tn = ti.tn;
@@ -879,7 +879,7 @@ chai_gemm_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant_
             bool ok = true;
             for (int g = 0; g < nseg; g++) {
                 const long long wait_no = SPLIT ? seg_no : (long long)(lt >> 1);
-                ok = mbar_wait(smem_u32(&tfull[ab]), (unsigned)(wait_no & 1), status, 124);
+                ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&tfull[ab]), (unsigned)(wait_no & 1), status, 124));
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const bool last = g == nseg - 1;
                 const bool do_store = ok && !*abort_flag && last;
@@ -1614,9 +1614,12 @@ __device__ __forceinline__ bool fs_bt_step(FsA& ra, bool& have, long long& it, F
 {
     constexpr int PBUF = 2 * P * FS_PLANE;
     const int q = (int)(it % NPB);
-    if (it >= NPB && !mbar_wait(smem_u32(&pempty[q]), (unsigned)((it / NPB - 1) & 1), status, 117)) return false;
+    // the warp leaves the loop together (each lane's bounded wait could end differently)
+    const bool w1 = it < NPB || mbar_wait(smem_u32(&pempty[q]), (unsigned)((it / NPB - 1) & 1), status, 117);
+    if (!__all_sync(0xffffffffu, w1)) return false;
     const int bs = (int)(it % FS_BST);
-    if (!mbar_wait(smem_u32(&bfull[bs]), (unsigned)((it / FS_BST) & 1), status, 120)) return false;
+    const bool w2 = mbar_wait(smem_u32(&bfull[bs]), (unsigned)((it / FS_BST) & 1), status, 120);
+    if (!__all_sync(0xffffffffu, w2)) return false;
     unsigned char* pa = planes + q * PBUF;
     fs_convert_a<P>(ra, pa, cw, lane);
     fs_convert_b_smem<P>(braw + bs * FS_BRAW, pa + P * FS_PLANE, ct);
@@ -1825,7 +1828,7 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
         for (long long t = blockIdx.x; t < ntiles; t += G, lt++) {
             const FsTile ti = tiles[t];                // loaded while the accumulator fills
             const int ab = lt & 1;
-            const bool ok = mbar_wait(smem_u32(&tfull[ab]), (unsigned)((lt >> 1) & 1), status, 114);
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&tfull[ab]), (unsigned)((lt >> 1) & 1), status, 114));   // warp-uniform
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             float* crow = ti.c + (long long)r * ti.n;
             const bool do_store = ok && !*abort_flag && r < ti.rows;
@@ -1943,6 +1946,7 @@ chai_gemm_fused_split(const FsTile* __restrict__ tiles, long long ntiles, int* s
             const int q = (int)(it % NPB);
             // plane buffer q was last read by the MMAs of chunk it - NPB
             if (it >= NPB) ok = mbar_wait(smem_u32(&pempty[q]), (unsigned)((it / NPB - 1) & 1), status, 117);
+            ok = __all_sync(0xffffffffu, ok);         // the warp leaves the loop together
             if (!ok) break;
             unsigned char* pa = planes + q * PBUF;
             fs_convert<P>(ra, rb, pa, pa + P * FS_PLANE, cw, lane, ct);
@@ -2111,7 +2115,7 @@ chai_gemm_fused_pair(const FsTile* __restrict__ tiles, long long ntiles, int* st
         for (long long t = pair; t < ntiles; t += npairs, lt++) {
             const FsTile ti = tiles[t];
             const int ab = lt & 1;
-            const bool ok = mbar_wait(smem_u32(&tfull[ab]), (unsigned)((lt >> 1) & 1), status, 134);
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&tfull[ab]), (unsigned)((lt >> 1) & 1), status, 134));   // warp-uniform
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int rows = max(0, min(BM, ti.rows - (int)rank * BM));
             float* cbase = ti.c + (long long)rank * BM * ti.n;
@@ -2194,10 +2198,14 @@ chai_gemm_fused_pair(const FsTile* __restrict__ tiles, long long ntiles, int* st
         for (long long it = 0; have && !*abort_flag; it++) {
             const int q = (int)(it % NPB);
             if (it >= NPB) ok = mbar_wait(smem_u32(&pempty[q]), (unsigned)((it / NPB - 1) & 1), status, 137);
+            ok = __all_sync(0xffffffffu, ok);         // the warp leaves the loop together
             if (!ok) break;
             unsigned char* pa = planes + q * PBUF;
             fs_convert<P>(ra, rb, pa, pa + P * FS_PLANE, cw, lane, ct);
-            // the tensor core reads the planes through the async proxy
+            // the tensor core reads the planes through the async proxy; each
+            // warp arrives on the leader's barrier (cluster-scope release).
+            // One elected arrival per CTA after a local barrier ran slower
+            // (1.60 against 1.43 ms on the 4096-problem group).
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive_cluster(pfull0 + (unsigned)(q * 8));
