@@ -234,6 +234,10 @@ static bool build_program(const std::vector<std::vector<Node>>& all, int root, d
     }
     p.stride = 4 + (int)p.rng_nodes.size() + (int)p.var_scalars.size();
     auto col_of = [&](const std::vector<int>& v, int i) { return (int)(std::find(v.begin(), v.end(), i) - v.begin()); };
+    // element indices in 32 bits when every trace is shorter than 2^30
+    // elements (the chunk index c = e0 / 4 and its bound then fit an int)
+    bool small = true;
+    for (const auto& tr : all) small = small && (long long)(tr[it].W * tr[it].H) < (1ll << 30);
     std::ostringstream os;
     os << "extern \"C\" __global__ void __launch_bounds__(256) chai_many(const long long* __restrict__ tab, "
           "double* __restrict__ partials)\n{\n  using namespace chai_ops; using namespace chai_rng;\n"
@@ -255,9 +259,10 @@ static bool build_program(const std::vector<std::vector<Node>>& all, int root, d
        << "    const bool flush = next >= t1 || (lo + 1 < ntr && rows[(long long)(lo + 1) * " << p.stride
        << " + 3] <= next);\n"
        << "    for (int sub = 0; sub < " << kManySubs << "; sub++) {\n"
-       << "    const long long c = ((tile - tp[3]) * " << kManySubs << " + sub) * 256 + threadIdx.x;\n"
-       << "    if (c * 4 >= n) break;\n"
-       << "    const long long e0 = c * 4;\n"
+       << (small ? "    const int c = ((int)(tile - tp[3]) * " : "    const long long c = ((tile - tp[3]) * ") << kManySubs
+       << " + sub) * 256 + threadIdx.x;\n"
+       << (small ? "    if (c * 4 >= (int)n) break;\n" : "    if (c * 4 >= n) break;\n")
+       << "    const long long e0 = (long long)c * 4;\n"
        << "    long long xx[4], yy[4]; { const long long y0 = e0 / W, x0 = e0 - y0 * W; "
           "for (int j = 0; j < 4; j++) { xx[j] = x0 + j; yy[j] = y0; } }\n";
     for (int i : body) {
