@@ -580,9 +580,11 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
 //
 // chai_gemm_pair: tcgen05.mma.cta_group::2 over a cluster of two CTAs on two
 // SMs.  A pair tile is 256 x 256: each CTA stages its own 128 rows of A and its
-// own 128 rows (N) of B -- half of B per SM instead of all of it, so a stage is
-// 32 KiB per CTA and each SM's shared-memory reads per MMA fall by a third
-// against the one-CTA 128 x 256 tile.  The even CTA of the pair (the leader)
+// own 128 rows (N) of B -- half of B per SM instead of all of it, so each SM's
+// shared-memory reads per MMA fall by a third against the one-CTA 128 x 256
+// tile.  A stage is one 64-element K chunk with every distinct plane of both
+// operands (PairShape), and the MMA issues all of the chunk's split products
+// from it.  The even CTA of the pair (the leader)
 // issues the MMAs; both CTAs' TMA copies complete on the leader's barrier
 // (.cta_group::2 copies, no multicast), and the MMA commits arrive on both
 // CTAs' barriers (tcgen05.commit multicast).  Each CTA holds its 128 rows of
@@ -604,8 +606,8 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
 // products of the same chunk, into the other accumulator.
 //
 // Barriers (per CTA; the leader's are the ones the MMA and the copies use):
-//   full[s]    leader: expect_tx of both CTAs' bytes + both CTAs' copies
-//   empty[s]   each CTA: the MMA commit of the stage (multicast)
+//   full[s]    leader: expect_tx of both CTAs' bytes + both CTAs' copies (all planes of chunk s)
+//   empty[s]   each CTA: the MMA commit after the chunk's products (multicast)
 //   tfull[b]   each CTA: accumulator (or drain segment) ready (multicast commit)
 //   tempty[b]  leader: 16 epilogue warps (8 per CTA) done with it
 //   drain      leader: every MMA complete before TMEM is freed
