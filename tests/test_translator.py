@@ -105,6 +105,28 @@ def test_kirsch_trace_is_one_kernel_with_gathers():
     assert "% 64)" not in body and "f2x4" not in body
 
 
+def test_stencil_tile_height_follows_shared_memory_and_grid():
+    """Stencil tiles are 64 rows tall when the staged tiles fit the 46 KiB of
+    static shared memory and the image gives every SM four tiles; 32 rows
+    otherwise (f64 sources, small images); StencilRows overrides."""
+    from tests.test_gpu_trace import kirsch_expr
+
+    def src_for(W, H, prec, cfg=None):
+        def build():
+            A = ch._ARR[prec](_raw=([ch._bc(L.BC_MEMORY, buffer=7), ch._sc(1), ch._sc(W), ch._sc(H),
+                                     ch._op(66 if prec == L.F32 else 67)], W, H, 1))
+            arr = ch.Arrayf32 if prec == L.F32 else ch.Arrayf64
+            return A, arr(kirsch_expr(ch, A, W, H))
+        stmts, (A, K) = record(build)
+        st, src = source(stmts, [(K.var, prec, W, H, 1, 0, 8)], cfg)
+        assert st == 0, src
+        return src
+    assert "blockIdx.y * 64" in src_for(8192, 8192, L.F32)
+    assert "blockIdx.y * 32" in src_for(8192, 8192, L.F64)        # (64 + 2) x 136 x 8 B > 46 KiB
+    assert "blockIdx.y * 32" in src_for(256, 256, L.F32)          # 2 x 4 tiles of 64 rows < 4 per SM
+    assert "blockIdx.y * 16" in src_for(8192, 8192, L.F32, "StencilRows=16")
+
+
 def test_flat_kernel_packs_f32_add_sub():
     """Element-wise kernels issue f32 add / sub as f32x2 pairs of neighbouring
     elements (registers of one 16-byte load); PackF32=0 keeps them scalar."""
