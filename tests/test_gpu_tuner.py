@@ -217,20 +217,21 @@ def test_unsupported_tuning_keys_are_rejected(chai_dev):
 
 def test_learned_tuner_gain_over_defaults_and_cold_start(tmp_path):
     """What the trained network gains over the method without it.  Exhaustive
-    sweeps of 600 training keys (M, N, K log-uniform in [64, 2048]; fp32 via
-    bf16x3, bf16, and f32 GEMV) train the cost model on the GPU; on 30
+    sweeps of 1000 training keys (M, N, K log-uniform in [64, 2048]; fp32 via
+    bf16x3, bf16, and f32 GEMV) train the cost model on the GPU; on 40
     held-out keys of the same distribution the learned method (rank the whole
     search space with the model, time the top 3) is judged on each key's own
     exhaustive sweep (per-configuration median of 5 sweeps, so that the
-    exhaustive best is not the luckiest of ~100 single samples).  Asserted: its pick reaches >= 0.95 of the exhaustive
-    best (geometric mean), it beats the fixed default configuration the
-    library uses without tuning, and it tunes >= 10x faster than the
-    exhaustive sweep (wall time of chai_cuda_tune against the sweep)."""
+    exhaustive best is not the luckiest of ~100 single samples).  Asserted:
+    its pick reaches >= 0.95 of the exhaustive best (geometric mean), it beats
+    the configuration the library runs without tuning (TUNE_DEFAULT), and it
+    tunes >= 10x faster than the exhaustive sweep (wall time of
+    chai_cuda_tune against the sweep)."""
     dev = ch.Device(config="TopK=3")
     try:
         ctx = dev.ctx
-        keys = T.shapes(630, seed=29, lo=64, hi=2048)
-        train, held_keys = keys[:600], keys[600:]
+        keys = T.shapes(1040, seed=29, lo=64, hi=2048)
+        train, held_keys = keys[:1000], keys[1000:]
         data, _ = T.collect(ctx, train)
         samples = [(k, c) for k, cs in data for c in cs if c.measured_us < 1e29]
         T.train(ctx, samples, epochs=2500, lr=1e-3, seed=1)
@@ -243,6 +244,7 @@ def test_learned_tuner_gain_over_defaults_and_cold_start(tmp_path):
     pick = gm([r["best_us"] / r["pick_us"] for r in rows])
     dflt = gm([r["best_us"] / r["default_us"] for r in rows])
     speedup = sum(r["exhaustive_s"] for r in rows) / sum(r["learned_s"] for r in rows)
+    print("learned pick %.4f of exhaustive best, defaults %.4f, cold start %.1fx" % (pick, dflt, speedup))
     assert pick >= 0.95, (pick, dflt, speedup)
     assert pick > dflt, (pick, dflt)
     assert speedup >= 10.0, speedup
