@@ -982,17 +982,15 @@ __device__ __forceinline__ void split8(const float (&a)[8], uint4 (&q)[3])
 // distinct planes side by side); each thread splits 8 consecutive elements and
 // writes one 16-byte chunk per plane
 template <int S>
-__global__ void __launch_bounds__(256) split_rows_bf16(const float* __restrict__ x, long long ld, long long sx,
-                                                       int rows, int k, int kpad, __nv_bfloat16* __restrict__ out,
-                                                       long long so)
+__device__ __forceinline__ void split_rows_block(const float* __restrict__ x, long long ld, long long sx, int k,
+                                                 int kpad, __nv_bfloat16* __restrict__ out, long long so, int bx,
+                                                 int gx, int row, int batch)
 {
-    const int batch = blockIdx.z;
-    const int row = blockIdx.y;
     constexpr int P = Planes<S>::P;
     x += batch * sx + (long long)row * ld;
     out += batch * so + (long long)row * P * kpad;
     const bool vec = ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
-    for (int k8 = blockIdx.x * blockDim.x + threadIdx.x; k8 * 8 < kpad; k8 += gridDim.x * blockDim.x) {
+    for (int k8 = bx * blockDim.x + threadIdx.x; k8 * 8 < kpad; k8 += gx * blockDim.x) {
         const int kk = k8 * 8;
         float a[8];
         if (vec && kk + 8 <= k) {
@@ -1010,18 +1008,24 @@ __global__ void __launch_bounds__(256) split_rows_bf16(const float* __restrict__
     }
 }
 
+template <int S>
+__global__ void __launch_bounds__(256) split_rows_bf16(const float* __restrict__ x, long long ld, long long sx,
+                                                       int rows, int k, int kpad, __nv_bfloat16* __restrict__ out,
+                                                       long long so)
+{
+    split_rows_block<S>(x, ld, sx, k, kpad, out, so, blockIdx.x, gridDim.x, blockIdx.y, blockIdx.z);
+}
+
 // B (k x cols, row-major) -> B' (cols x S*kpad bf16) through a 64 x 64 tile:
 // float4 loads along cols, 16-byte stores of 8 consecutive k per column
 template <int S>
-__global__ void __launch_bounds__(256) split_cols_bf16(const float* __restrict__ x, long long ld, long long sx, int k,
-                                                       int cols, int kpad, __nv_bfloat16* __restrict__ out,
-                                                       long long so)
+__device__ __forceinline__ void split_cols_block(const float* __restrict__ x, long long ld, long long sx, int k,
+                                                 int cols, int kpad, __nv_bfloat16* __restrict__ out, long long so,
+                                                 int bx, int by, int batch, float (&tile)[64][65])
 {
-    __shared__ float tile[64][65];
-    const int batch = blockIdx.z;
     x += batch * sx;
     out += batch * so;
-    const int k0 = blockIdx.y * 64, c0 = blockIdx.x * 64;
+    const int k0 = by * 64, c0 = bx * 64;
     const bool vec = ((reinterpret_cast<uintptr_t>(x) & 15) == 0) && (ld % 4 == 0);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // 16 float4 per tile row, 16 rows per pass
     for (int i = ty; i < 64; i += 16) {
@@ -1052,6 +1056,41 @@ __global__ void __launch_bounds__(256) split_cols_bf16(const float* __restrict__
         __nv_bfloat16* o = out + (long long)cc * P * kpad;
 #pragma unroll
         for (int p = 0; p < P; p++) *reinterpret_cast<uint4*>(o + (long long)p * kpad + kk) = q[p];
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) split_cols_bf16(const float* __restrict__ x, long long ld, long long sx, int k,
+                                                       int cols, int kpad, __nv_bfloat16* __restrict__ out,
+                                                       long long so)
+{
+    __shared__ float tile[64][65];
+    split_cols_block<S>(x, ld, sx, k, cols, kpad, out, so, blockIdx.x, blockIdx.y, blockIdx.z, tile);
+}
+
+// Both operands' planes in one launch (one launch fewer per GEMM, and the two
+// small grids of a small product run side by side): blocks [0, nr) take A's
+// row grid (rx x rows x batch, x fastest), the rest B's 64 x 64 tile grid
+// (cx x ky x batch); each block does exactly what it does in the separate
+// kernels.
+template <int S>
+__global__ void __launch_bounds__(256) split_both_bf16(const float* __restrict__ a, long long lda, long long sa, int rows,
+                                                       const float* __restrict__ b, long long ldb, long long sb, int cols,
+                                                       int k, int kpad, __nv_bfloat16* __restrict__ oa, long long soa,
+                                                       __nv_bfloat16* __restrict__ ob, long long sob, int rx, int cx,
+                                                       int ky, long long nr)
+{
+    __shared__ float tile[64][65];
+    const long long bid = blockIdx.x;
+    if (bid < nr) {
+        const int bx = (int)(bid % rx);
+        const long long rest = bid / rx;
+        split_rows_block<S>(a, lda, sa, k, kpad, oa, soa, bx, rx, (int)(rest % rows), (int)(rest / rows));
+    } else {
+        const long long c = bid - nr;
+        const int bx = (int)(c % cx);
+        const long long rest = c / cx;
+        split_cols_block<S>(b, ldb, sb, k, cols, kpad, ob, sob, bx, (int)(rest % ky), (int)(rest / ky), tile);
     }
 }
 
@@ -2371,6 +2410,9 @@ void preload_gemm_kernels()
     cudaFuncGetAttributes(&a, split_cols_bf16<1>);
     cudaFuncGetAttributes(&a, split_cols_bf16<3>);
     cudaFuncGetAttributes(&a, split_cols_bf16<6>);
+    cudaFuncGetAttributes(&a, split_both_bf16<1>);
+    cudaFuncGetAttributes(&a, split_both_bf16<3>);
+    cudaFuncGetAttributes(&a, split_both_bf16<6>);
     cudaFuncGetAttributes(&a, pad_rows_f32);
     cudaFuncGetAttributes(&a, transpose_pad_f32);
     cudaFuncGetAttributes(&a, fs_tiles);
@@ -2497,10 +2539,16 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
         } else {
             __nv_bfloat16* a2 = (__nv_bfloat16*)Ap;
             __nv_bfloat16* b2 = (__nv_bfloat16*)Bp;
+            const long long nr = (long long)rgrid.x * rgrid.y * rgrid.z;
+            const long long nb = (long long)sgrid.x * sgrid.y * sgrid.z;
 #define SPLIT(SS)                                                                                                   \
-    split_rows_bf16<SS><<<rgrid, 256, 0, s>>>(A, d->lda, d->stride_a, (int)M, (int)K, (int)kpad, a2, M * kp);    \
-    if (!b_ready)                                                                                                   \
-        split_cols_bf16<SS><<<sgrid, 256, 0, s>>>(B, d->ldb, d->stride_b, (int)K, (int)N, (int)kpad, b2, N * kp)
+    if (b_ready)                                                                                                    \
+        split_rows_bf16<SS><<<rgrid, 256, 0, s>>>(A, d->lda, d->stride_a, (int)M, (int)K, (int)kpad, a2, M * kp);  \
+    else                                                                                                            \
+        split_both_bf16<SS><<<(unsigned)(nr + nb), 256, 0, s>>>(A, d->lda, d->stride_a, (int)M, B, d->ldb,          \
+                                                                d->stride_b, (int)N, (int)K, (int)kpad, a2, M * kp, \
+                                                                b2, N * kp, (int)rgrid.x, (int)sgrid.x,             \
+                                                                (int)sgrid.y, nr)
             if (S == 1) { SPLIT(1); } else if (S == 3) { SPLIT(3); } else { SPLIT(6); }
 #undef SPLIT
         }
