@@ -199,8 +199,11 @@ def test_tuning_db_and_weights_round_trip(tmp_path):
     finally:
         dev.close()
     text = db.read_text()
-    assert text.startswith("BEST 256 768 512 %d 0 128 %d 128 %d 4 1 1 %d " % (L.GEMM_BF16X3, best.block_n,
-                                                                             best.stages, best.group_m))
+    # the line holds the key and every field of the configuration the sweep
+    # chose (one-CTA or CTA-pair tile, whichever timed best)
+    assert text.startswith("BEST 256 768 512 %d 0 %d %d %d %d %d %d %d %d " % (
+        L.GEMM_BF16X3, best.block_m, best.block_n, best.block_k, best.stages, best.vec_width, best.cluster_m,
+        best.cluster_n, best.group_m))
     dev = ch.Device(config="TuneDB=%s" % db)
     try:
         np.testing.assert_array_equal(T.get_weights(dev.ctx), w)
