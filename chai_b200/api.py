@@ -629,6 +629,30 @@ def matmul(a, b, c=None, alpha=1.0, beta=1.0):
 # ------------------------------------------------------------------ inline OpenCL
 
 _CL_SCALARS = {"unsigned": L.U32, "uint": L.U32, "int": L.I32, "float": L.F32, "double": L.F64}
+_CL_BYTES = {"char": 1, "uchar": 1, "short": 2, "ushort": 2, "int": 4, "uint": 4, "long": 8, "ulong": 8,
+             "float": 4, "double": 8}
+
+
+def _cl_vector_bytes(tok):
+    """Bytes of one element of an OpenCL vector type name (a 3-vector is
+    stored as a 4-vector), or 0 when `tok` names no vector type."""
+    import re
+    m = re.fullmatch(r"(char|uchar|short|ushort|int|uint|long|ulong|float|double)(2|3|4|8|16)", tok)
+    if not m:
+        return 0
+    n = int(m.group(2))
+    return _CL_BYTES[m.group(1)] * (4 if n == 3 else n)
+
+
+def _cl_vector_params(text):
+    """Per kernel, for each parameter: the element bytes of a vector-typed
+    parameter (0 for the others)."""
+    import re
+    out = {}
+    for m in re.finditer(r"\b(?:__kernel|kernel)\s+void\s+(\w+)\s*\(([^)]*)\)", text):
+        out[m.group(1)] = [_max([_cl_vector_bytes(t) for t in p.replace("*", " ").split()] or [0])
+                           for p in m.group(2).split(",") if p.split()]
+    return out
 
 
 def _cl_signatures(text):
@@ -666,6 +690,7 @@ class ProgramCL:
     def __init__(self, text):
         self.text = text if isinstance(text, str) else "\n".join(text)
         self._sigs = _cl_signatures(self.text)
+        self._vbytes = _cl_vector_params(self.text)
 
     def __call__(self, name, *args):
         if name not in self._sigs:
@@ -689,12 +714,18 @@ class _KernelCall:
         if len(sig) != len(self.args):
             raise TypeError("ProgramCL: %s takes %d arguments" % (self.name, len(sig)))
         args = []
-        for (kind, prec), a in zip(sig, self.args):
+        vbytes = self.prog._vbytes.get(self.name, [0] * len(sig))
+        for (kind, prec), vb, a in zip(sig, vbytes, self.args):
             if kind == L.KARG_ARRAY:
                 if not isinstance(a, Array):
                     raise TypeError("ProgramCL: array arguments must be array variables")
                 args.append((kind, a.prec, a.var, a.version - 1, 0.0))
                 _Client.keep.append(a)
+            elif kind == L.KARG_LOCAL and vb:
+                # __local floatN* etc.: the count is in vector elements; passed as 32-bit words
+                args.append((kind, L.U32, 0, 0, float((int(a) * vb + 3) // 4)))
+            elif vb:
+                raise TypeError("ProgramCL: %s: vector-typed scalar arguments are not supported" % self.name)
             else:
                 args.append((kind, prec if prec >= 0 else L.F32, 0, 0, float(a)))
         idx = len(_Client.kernels)

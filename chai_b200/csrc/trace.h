@@ -120,6 +120,6 @@ private:
 
 // OpenCL C program text -> CUDA source (inline_cl.cpp)
 int opencl_to_cuda(const std::string& src, const std::string& name, const std::vector<size_t>& local_bytes,
-                   int work_dim, std::string& out, std::string& err);
+                   int work_dim, std::string& out, std::string& err, std::vector<char>* image_args = nullptr);
 
 }  // namespace chai

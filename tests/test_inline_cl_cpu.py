@@ -1,6 +1,8 @@
 """Inline OpenCL kernels (ProgramCL) on the CPU: the recorded statement, the
 signature parse (api/ProgramCL.cpp:45-176) and the OpenCL C -> CUDA text that
-NVRTC compiles for sm_100a (chai_cuda_trace_source, no device needed)."""
+NVRTC compiles for sm_100a (chai_cuda_trace_source, no device needed): the
+scalar language, and vector types, swizzles, conversions, atomics, work-group
+copies and image2d_t parameters."""
 import ctypes as C
 
 import numpy as np
@@ -103,15 +105,221 @@ def test_local_memory_pointer_is_placed_in_dynamic_shared_memory():
     assert not re.search(r"\b__global\b(?!_)", src.split("// ---- program text")[1])
 
 
-def test_image_arguments_are_rejected():
-    prog = ch.ProgramCL("__kernel void k(image2d_t img, __global float* a) { }")
-    n = 4
+def compile_call(text, name, arrays, extra=()):
+    """Record `prog(name, *arrays, *extra)(64, 16)` over the given
+    (precision, W, H) arrays and compile the trace; (status, source)."""
+    prog = ch.ProgramCL(text)
+    zeros = {L.F32: ch.zeros_f32, L.F64: ch.zeros_f64, L.I32: ch.zeros_i32, L.U32: ch.zeros_u32}
 
     def build():
-        a = ch.Arrayf32(ch.zeros_f32(n))
-        prog("k", a, a)(n, 1)
+        arrs = [ch._ARR[p](zeros[p](w, h)) for p, w, h in arrays]
+        prog(name, *arrs, *extra)(64, 16)
+        return arrs
+    stmts, kernels, arrs = record_with_kernels(build)
+    return source(stmts, kernels)
+
+
+VEC_OPS = """
+__kernel void vec_ops(__global float* a, __global float* out, __global int* iout, uint n)
+{
+    const size_t i = get_global_id(0);
+    if (i >= n) return;
+    float4 v = vload4(i, a);
+    float4 w = (float4)(1.0f, 2.0f, 3.0f, 4.0f);
+    float4 u = v * w + (float4)(0.5f);
+    u.xy = u.yx;
+    u.zw += (float2)(1.0f, -1.0f);
+    u.s0 = u.s3 * 2.0f;
+    float2 lo = u.lo, hi = u.hi;
+    float4 m = mix(u, w, 0.25f);
+    m = clamp(m, -4.0f, 4.0f);
+    m = fmax(m, fmin(u, w));
+    int4 c = u > w;
+    float4 s = select(u, w, c);
+    float d = dot(s.xyz, w.xyz) + length(hi) + distance(lo, hi);
+    float3 cr = cross(s.xyz, w.xyz);
+    float4 nrm = normalize(m);
+    int4 iv = convert_int4_sat_rte(m * 1000.0f);
+    uint4 bits = as_uint4(nrm);
+    vstore4(sqrt(fabs(nrm)) + exp(-fabs(m)) + sin(s) + (float4)(d, cr), i, out);
+    iout[i] = iv.x + iv.y + iv.z + iv.w + (int)(bits.x & 1u) + any(c) + all(c) + popcount(iv.x) + clz(iv.y);
+}
+"""
+
+DVEC_WIDE = """
+#pragma OPENCL EXTENSION cl_khr_fp64 : enable
+__kernel void dvec(__global double* a, __global long* b, uint n)
+{
+    const size_t i = get_global_id(0);
+    double2 v = vload2(i, a);
+    long2 l = convert_long2(v * 10.0);
+    v.even = v.odd;
+    b[i] = l.x + l.y + (long)as_ulong(v.x) + add_sat(l.x, l.y) + mul_hi(l.x, l.y);
+    vstore2(v + convert_double2(l), i, a);
+}
+__kernel void wide(__global float* a, __global uint* u)
+{
+    const size_t i = get_global_id(0);
+    float8 v = vload8(i, a);
+    float16 w = (float16)(v, v.s76543210);
+    uint16 k = convert_uint16_sat(w);
+    v.lo = v.hi * 2.0f;
+    v.s0123 = v.s4567 + 1.0f;
+    w.odd = w.even;
+    vstore8(v + w.lo + w.hi, i, a);
+    u[i] = k.sF + k.s0 + rotate(k.s1, 3u) + hadd(k.s2, k.s3);
+}
+"""
+
+ATOMS = """
+__kernel void hist(__global const uint* x, __global uint* h, __local uint* lh, uint n, uint bins)
+{
+    const uint l = get_local_id(0);
+    for (uint b = l; b < bins; b += get_local_size(0)) lh[b] = 0;
+    barrier(CLK_LOCAL_MEM_FENCE);
+    const size_t g = get_global_id(0);
+    if (g < n) atomic_inc(&lh[x[g] % bins]);
+    barrier(CLK_LOCAL_MEM_FENCE);
+    for (uint b = l; b < bins; b += get_local_size(0)) atomic_add(&h[b], lh[b]);
+}
+__kernel void tile_rev(__global const float4* src, __global float4* dst, __local float4* t)
+{
+    event_t e = async_work_group_copy(t, src + get_group_id(0) * get_local_size(0), get_local_size(0), 0);
+    wait_group_events(1, &e);
+    const uint l = get_local_id(0);
+    dst[get_global_id(0)] = t[get_local_size(0) - 1 - l].wzyx;
+}
+__kernel void atoms(__global int* a, __global ulong* b, __global float* f)
+{
+    atomic_max(&a[0], (int)get_global_id(0));
+    atomic_min(&a[1], -(int)get_global_id(0));
+    atomic_cmpxchg(&a[2], 0, 1);
+    atomic_xchg(&a[3], 7);
+    atomic_or(&a[4], 1 << (get_global_id(0) & 31));
+    atom_add(&b[0], (ulong)get_global_id(0));
+    atomic_add(&f[0], 1.0f);
+    atomic_sub(&a[5], 2);
+    atomic_dec(&a[6]);
+}
+"""
+
+IMAGES = """
+__constant sampler_t smp = CLK_NORMALIZED_COORDS_FALSE | CLK_ADDRESS_CLAMP | CLK_FILTER_NEAREST;
+const sampler_t lin = CLK_NORMALIZED_COORDS_TRUE | CLK_ADDRESS_REPEAT | CLK_FILTER_LINEAR;
+__kernel void img(__read_only image2d_t src, __global float* out, __write_only image2d_t dst)
+{
+    const int x = get_global_id(0), y = get_global_id(1);
+    float4 p = read_imagef(src, smp, (int2)(x - 1, y)) + read_imagef(src, smp, (int2)(x + 1, y));
+    float2 uv = (float2)((x + 0.5f) / get_image_width(src), (y + 0.5f) / get_image_height(src));
+    p += read_imagef(src, lin, uv);
+    vstore4(p, y * get_image_width(src) + x, out);
+    write_imagef(dst, (int2)(x, y), p * 0.5f);
+}
+__kernel void dimg(read_only image2d_t src, __global double* out)
+{
+    const int x = get_global_id(0), y = get_global_id(1);
+    double2 v = as_double2(read_imageui(src, smp, (int2)(x, y)));
+    vstore2(v, y * get_image_width(src) + x, out);
+}
+"""
+
+
+@pytest.mark.parametrize("text,name,arrays,extra", [
+    (VEC_OPS, "vec_ops", [(L.F32, 256, 1), (L.F32, 256, 1), (L.I32, 64, 1)], (np.uint32(64),)),
+    (DVEC_WIDE, "dvec", [(L.F64, 128, 1), (L.F64, 64, 1)], (np.uint32(64),)),
+    (ATOMS, "hist", [(L.U32, 64, 1), (L.U32, 64, 1)], (64, np.uint32(64), np.uint32(64))),
+    (IMAGES, "img", [(L.F32, 32, 16), (L.F32, 512, 1), (L.F32, 32, 16)], ()),
+])
+def test_vector_image_and_atomic_programs_compile(text, name, arrays, extra):
+    st, src = compile_call(text, name, arrays, extra)
+    assert st == 0, src[-3000:]
+    body = src.split("// ---- program text")[-1]
+    assert "chai_cl::vec<" in body
+    assert "float4" not in body.replace("chai_cl::vec<float, 4>", "")
+
+
+def test_vector_rewrites():
+    st, src = compile_call(VEC_OPS, "vec_ops", [(L.F32, 256, 1), (L.F32, 256, 1), (L.I32, 64, 1)],
+                           (np.uint32(64),))
+    assert st == 0
+    body = src.split("// ---- program text")[-1]
+    # literals, assigned and read swizzles, conversions and reinterpretations
+    assert "chai_cl::make<chai_cl::vec<float, 4>>(1.0f, 2.0f, 3.0f, 4.0f)" in body
+    assert "u.chai_swl<0,1>() = u.chai_swr<1,0>();" in body
+    assert "u.chai_swl<2,3>() += chai_cl::make<chai_cl::vec<float, 2>>(1.0f, -1.0f);" in body
+    assert "u.chai_sw1<0>() = u.chai_sw1<3>() * 2.0f;" in body
+    assert "u.chai_lo(), hi = u.chai_hi();" in body
+    assert "chai_cl::convert<int, 4, 1, 1>(m * 1000.0f)" in body
+    assert "chai_cl::as_type<chai_cl::vec<unsigned int, 4>>(nrm)" in body
+    # single x / y / z / w components stay members
+    assert "iv.x + iv.y + iv.z + iv.w" in body
+    st, src = compile_call(DVEC_WIDE, "wide", [(L.F32, 512, 1), (L.U32, 64, 1)])
+    assert st == 0
+    body = src.split("// ---- program text")[-1]
+    assert "w.chai_odd_l() = w.chai_even();" in body
+    assert "v.chai_swl<0,1,2,3>() = v.chai_swr<4,5,6,7>() + 1.0f;" in body
+    assert "k.chai_sw1<15>() + k.chai_sw1<0>()" in body
+
+
+def test_member_names_in_vector_free_programs_are_left_alone():
+    text = """
+    typedef struct { float lo, hi, sa; } range;
+    __kernel void spans(__global float* a)
+    {
+        range r; r.lo = a[0]; r.hi = a[1]; r.sa = r.hi - r.lo;
+        a[get_global_id(0)] = r.sa;
+    }"""
+    st, src = compile_call(text, "spans", [(L.F32, 64, 1)])
+    assert st == 0, src[-2000:]
+    assert "r.lo = a[0]; r.hi = a[1]; r.sa = r.hi - r.lo;" in src
+
+
+def test_image_parameters():
+    st, src = compile_call(IMAGES, "img", [(L.F32, 32, 16), (L.F32, 512, 1), (L.F32, 32, 16)])
+    assert st == 0, src[-2000:]
+    body = src.split("// ---- program text")[-1]
+    # pointer + packed extent per image, rebuilt at the top of the body
+    assert "unsigned char* chai_img_src, long long chai_imgd_src" in body
+    assert "const chai_cl::image2d src = {chai_img_src," in body
+    assert "read_only" not in body and "write_only" not in body
+    # an f64 array: 2 values per texel
+    st, src = compile_call(IMAGES, "dimg", [(L.F64, 16, 4), (L.F64, 64, 1)])
+    assert st == 0, src[-2000:]
+    # rows must be whole 16-byte texels: 6 floats are not
+    st, src = compile_call(IMAGES, "img", [(L.F32, 6, 4), (L.F32, 512, 1), (L.F32, 32, 16)])
+    assert st != 0 and "16-byte texels" in src
+    for bad, word in (("__kernel void k(image3d_t v, __global float* a) { }", "image3d_t"),
+                      ("__kernel void k(sampler_t s, __global float* a) { }", "sampler_t")):
+        prog = ch.ProgramCL(bad)
+        n = 4
+
+        def build():
+            a = ch.Arrayf32(ch.zeros_f32(n))
+            prog("k", 0, a)(n, 1)       # neither parameter kind is an array one
+            return a
+        stmts, kernels, a = record_with_kernels(build)
+        st, src = source(stmts, kernels)
+        assert st != 0 and word in src
+
+
+def test_vector_local_memory_is_sized_in_vector_elements():
+    prog = ch.ProgramCL(ATOMS)
+    assert prog._vbytes["tile_rev"] == [16, 16, 16]
+    assert prog._vbytes["hist"] == [0, 0, 0, 0, 0]
+    st, src = compile_call(ATOMS, "tile_rev", [(L.F32, 256, 1), (L.F32, 256, 1)], (16,))
+    assert st == 0, src[-2000:]
+    assert "t = reinterpret_cast<chai_cl::vec<float, 4>*>(chai_cl_lmem + 0);" in src
+
+    def build():
+        a = ch.Arrayf32(ch.zeros_f32(256))
+        prog("tile_rev", a, a, 16)(64, 16)
         return a
-    stmts, kernels, a = record_with_kernels(build)
-    st, src = source(stmts, kernels, [(a.var, 4, n, 1, 1, 0, 9)])
-    assert st != 0
-    assert "image2d_t" in src
+    _, kernels, _ = record_with_kernels(build)
+    assert kernels[0][2][2] == (L.KARG_LOCAL, L.U32, 0, 0, 64.0)     # 16 float4 = 64 words
+
+
+def test_vector_scalar_arguments_are_rejected():
+    prog = ch.ProgramCL("__kernel void k(__global float* a, float4 v) { }")
+    a = ch.Arrayf32(ch.zeros_f32(4))
+    with pytest.raises(TypeError):
+        prog("k", a, 1.0)(4, 1)
