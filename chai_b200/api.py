@@ -721,10 +721,7 @@ class _KernelCall:
                     raise TypeError("ProgramCL: array arguments must be array variables")
                 args.append((kind, a.prec, a.var, a.version - 1, 0.0))
                 _Client.keep.append(a)
-            elif kind == L.KARG_LOCAL and vb:
-                # __local floatN* etc.: the count is in vector elements; passed as 32-bit words
-                args.append((kind, L.U32, 0, 0, float((int(a) * vb + 3) // 4)))
-            elif vb:
+            elif vb and kind != L.KARG_LOCAL:
                 raise TypeError("ProgramCL: %s: vector-typed scalar arguments are not supported" % self.name)
             else:
                 args.append((kind, prec if prec >= 0 else L.F32, 0, 0, float(a)))

@@ -962,6 +962,26 @@ bool swizzle(const std::string& w, std::vector<int>& idx, std::string& special)
     return true;
 }
 
+// Bytes of one element of a __local parameter's declared type (after the
+// vector rewrite); 0 when the type is not an OpenCL scalar or vector type.
+size_t local_elem_bytes(const std::string& type)
+{
+    static const std::pair<const char*, size_t> scalars[] = {
+        {"char", 1}, {"signed char", 1}, {"uchar", 1}, {"unsigned char", 1}, {"short", 2}, {"ushort", 2},
+        {"unsigned short", 2}, {"int", 4}, {"uint", 4}, {"unsigned", 4}, {"unsigned int", 4}, {"float", 4},
+        {"long", 8}, {"ulong", 8}, {"unsigned long", 8}, {"long long", 8}, {"unsigned long long", 8},
+        {"double", 8}, {"size_t", 8}};
+    for (const auto& e : scalars)
+        if (type == e.first) return e.second;
+    const std::string head = "chai_cl::vec<";
+    if (type.compare(0, head.size(), head) != 0 || type.back() != '>') return 0;
+    const size_t comma = type.rfind(',');
+    if (comma == std::string::npos) return 0;
+    const size_t eb = local_elem_bytes(type.substr(head.size(), comma - head.size()));
+    const int n = std::atoi(type.c_str() + comma + 1);
+    return eb * (size_t)(n == 3 ? 4 : n);
+}
+
 // true when the token after position i starts an assignment (=, op=, ++, --)
 bool assigned_next(const std::vector<Tok>& t, size_t i)
 {
@@ -1041,12 +1061,15 @@ void rewrite_vectors(std::vector<Tok>& t)
 
 }  // namespace
 
-// `local_bytes[i]`: bytes of the i-th argument of kernel `name` when it is a
-// __local pointer (0 otherwise).  `image_args`, when given, receives one flag
-// per parameter of kernel `name`: 1 for an image2d_t parameter, which takes
-// two launch arguments (the texel pointer, then width | height << 32).
-int opencl_to_cuda(const std::string& src, const std::string& name, const std::vector<size_t>& local_bytes,
-                   int work_dim, std::string& out, std::string& err, std::vector<char>* image_args)
+// `local_counts[i]`: elements of the i-th argument of kernel `name` when it is
+// a __local pointer (0 otherwise); each is sized by its declared element type
+// and `*local_bytes`, when given, receives the dynamic shared memory they
+// take.  `image_args`, when given, receives one flag per parameter of kernel
+// `name`: 1 for an image2d_t parameter, which takes two launch arguments (the
+// texel pointer, then width | height << 32).
+int opencl_to_cuda(const std::string& src, const std::string& name, const std::vector<size_t>& local_counts,
+                   int work_dim, std::string& out, std::string& err, std::vector<char>* image_args,
+                   size_t* local_bytes)
 {
     std::vector<Tok> t = tokenize(src);
     rewrite_vectors(t);
@@ -1175,13 +1198,23 @@ int opencl_to_cuda(const std::string& src, const std::string& name, const std::v
                     if (called && image_args) (*image_args)[pi] = 1;
                 }
                 if (local && called) {
-                    const size_t bytes = pi < local_bytes.size() ? local_bytes[pi] : 0;
-                    inject << " " << last_ident << " = reinterpret_cast<" << (type.empty() ? "float" : type)
-                           << "*>(chai_cl_lmem + " << offset << ");";
-                    offset += (bytes + 15) & ~size_t(15);
+                    const size_t count = pi < local_counts.size() ? local_counts[pi] : 0;
+                    const size_t eb = local_elem_bytes(type);
+                    if (eb == 0) {
+                        err = "inline kernel: __local parameter " + last_ident + " has an element type of unknown size";
+                        return -1;
+                    }
+                    if (count > (size_t)227 * 1024) {
+                        err = "inline kernel: __local memory above 227 KB";
+                        return -1;
+                    }
+                    inject << " " << last_ident << " = reinterpret_cast<" << type << "*>(chai_cl_lmem + " << offset
+                           << ");";
+                    offset += (count * eb + 15) & ~size_t(15);
                 }
                 plist_out << (pi ? "," : "") << pout.str();
             }
+            if (called && local_bytes) *local_bytes = offset;
             os << "extern \"C\" __global__ void " << kname << pre << params_before << "(" << plist_out.str() << ")";
             // body: copy up to and including the opening '{', then inject
             while (k < t.size()) {
@@ -1227,23 +1260,24 @@ int Translator::emit_inline(int i)
     }
     const uint64_t lx = k.local_size[0], ly = two_d ? k.local_size[1] : 1;
     if (lx * ly > 1024) return fail(CHAI_ERR_INVALID, "inline kernel: more than 1024 work items per group");
-    std::vector<size_t> lbytes(k.n_args, 0);
+    std::vector<size_t> lcount(k.n_args, 0);
     size_t smem = 0;
     for (uint32_t a = 0; a < k.n_args; a++) {
         const chai_kernel_arg& g = k.args[a];
         if (g.kind == CHAI_KARG_LOCAL) {
-            if (g.value < 0) return fail(CHAI_ERR_INVALID, "inline kernel: negative __local size");
-            lbytes[a] = (size_t)g.value * prec_bytes(g.prec);
-            smem += (lbytes[a] + 15) & ~size_t(15);
+            // an element count; the kernel's declared element type sizes it
+            if (!(g.value >= 0 && g.value <= 227.0 * 1024))
+                return fail(CHAI_ERR_INVALID, "inline kernel: __local size out of range");
+            lcount[a] = (size_t)g.value;
         } else if (g.kind != CHAI_KARG_ARRAY && g.kind != CHAI_KARG_SCALAR) {
             return fail(CHAI_ERR_INVALID, "inline kernel: argument kind");
         }
     }
-    if (smem > 227 * 1024) return fail(CHAI_ERR_INVALID, "inline kernel: __local memory above 227 KB");
     std::string cuda, err;
     std::vector<char> images;
-    if (opencl_to_cuda(k.source, k.name, lbytes, two_d ? 2 : 1, cuda, err, &images))
+    if (opencl_to_cuda(k.source, k.name, lcount, two_d ? 2 : 1, cuda, err, &images, &smem))
         return fail(CHAI_ERR_INVALID, err);
+    if (smem > 227 * 1024) return fail(CHAI_ERR_INVALID, "inline kernel: __local memory above 227 KB");
     // an image2d_t argument: rows of whole 16-byte RGBA texels over one slot
     for (uint32_t a = 0, m = 0; a < k.n_args; a++) {
         if (k.args[a].kind != CHAI_KARG_ARRAY) continue;

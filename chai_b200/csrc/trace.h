@@ -119,7 +119,8 @@ private:
 };
 
 // OpenCL C program text -> CUDA source (inline_cl.cpp)
-int opencl_to_cuda(const std::string& src, const std::string& name, const std::vector<size_t>& local_bytes,
-                   int work_dim, std::string& out, std::string& err, std::vector<char>* image_args = nullptr);
+int opencl_to_cuda(const std::string& src, const std::string& name, const std::vector<size_t>& local_counts,
+                   int work_dim, std::string& out, std::string& err, std::vector<char>* image_args = nullptr,
+                   size_t* local_bytes = nullptr);
 
 }  // namespace chai

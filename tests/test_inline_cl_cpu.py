@@ -302,7 +302,7 @@ def test_image_parameters():
         assert st != 0 and word in src
 
 
-def test_vector_local_memory_is_sized_in_vector_elements():
+def test_local_memory_is_sized_by_the_declared_element_type():
     prog = ch.ProgramCL(ATOMS)
     assert prog._vbytes["tile_rev"] == [16, 16, 16]
     assert prog._vbytes["hist"] == [0, 0, 0, 0, 0]
@@ -315,7 +315,7 @@ def test_vector_local_memory_is_sized_in_vector_elements():
         prog("tile_rev", a, a, 16)(64, 16)
         return a
     _, kernels, _ = record_with_kernels(build)
-    assert kernels[0][2][2] == (L.KARG_LOCAL, L.U32, 0, 0, 64.0)     # 16 float4 = 64 words
+    assert kernels[0][2][2] == (L.KARG_LOCAL, L.F32, 0, 0, 16.0)     # 16 float4: sized by the declared type
 
 
 def test_vector_scalar_arguments_are_rejected():
@@ -323,3 +323,31 @@ def test_vector_scalar_arguments_are_rejected():
     a = ch.Arrayf32(ch.zeros_f32(4))
     with pytest.raises(TypeError):
         prog("k", a, 1.0)(4, 1)
+
+
+def test_local_offsets_follow_the_declared_element_sizes():
+    text = """
+    typedef struct { float a, b, c; } trip;
+    __kernel void k(__local long* a, __local float4* b, __local uchar* c, __global float* out) { }
+    __kernel void s(__local trip* t, __global float* out) { }"""
+    prog = ch.ProgramCL(text)
+
+    def build():
+        out = ch.Arrayf32(ch.zeros_f32(64))
+        prog("k", 3, 2, 5, out)(64, 16)
+        return out
+    stmts, kernels, _ = record_with_kernels(build)
+    st, src = source(stmts, kernels)
+    assert st == 0, src[-2000:]
+    # 3 longs = 24 B -> 32; 2 float4 = 32 B; 5 uchars
+    assert "a = reinterpret_cast<long*>(chai_cl_lmem + 0);" in src
+    assert "b = reinterpret_cast<chai_cl::vec<float, 4>*>(chai_cl_lmem + 32);" in src
+    assert "c = reinterpret_cast<uchar*>(chai_cl_lmem + 64);" in src
+
+    def build_s():
+        out = ch.Arrayf32(ch.zeros_f32(64))
+        prog("s", 4, out)(64, 16)
+        return out
+    stmts, kernels, _ = record_with_kernels(build_s)
+    st, src = source(stmts, kernels)
+    assert st != 0 and "unknown size" in src
