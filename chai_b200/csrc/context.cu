@@ -183,6 +183,10 @@ void parse_config(chai::Config& c, const char* text)
             c.grouped_fused = v != "prepass";
         } else if (k == "PackF32") {
             c.pack_f32 = v != "0" && v != "off";
+        } else if (k == "PackF32Stencil") {
+            c.pack_f32_stencil = v != "0" && v != "off";
+        } else if (k == "StencilBorderTma") {
+            c.stencil_border_tma = v != "0" && v != "off";
         } else if (k == "PlanCache") {
             c.plan_cache = v != "0" && v != "off";
         } else if (k == "PlanGraph") {

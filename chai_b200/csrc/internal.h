@@ -44,6 +44,8 @@ struct Config {
     int gemm_pair_seg = 64;                  // pair kernel, split precisions: K chunks per promotion segment
     int gemm_stages = 0;                     // GEMM pipeline stages (0: tuned or default)
     bool pack_f32 = true;                    // element kernels issue f32 add / sub as packed f32x2 pairs
+    bool pack_f32_stencil = false;           // ... stencil kernels too (slower: re-pairing moves, registers)
+    bool stencil_border_tma = true;          // border stencil tiles staged by TMA + wrapped patch loads
     std::string jit_cache;
 };
 

@@ -424,14 +424,22 @@ int Translator::emit_group(const std::vector<int>& roots)
         os << "  {\n    const bool interior = " << (use_tma ? "true" : "false") << " && tx0 - " << ST_PX
            << " >= 0 && tx0 + " << ST_TX + ST_PX << " <= W && ty0 - " << R << " >= 0 && ty0 + " << ST_TY + R
            << " <= H;\n";
-        os << "    if (interior) {\n      if (threadIdx.x == 0) chai_k::mbar_init(&tbar, 1);\n      __syncthreads();\n"
+        // Border tiles: with StencilBorderTma (an image at least one tile
+        // large) they are staged by the same TMA load, whose rows and columns
+        // outside the image arrive zero-filled, and only those elements are
+        // then replaced by wrapped loads; otherwise every element of a border
+        // tile is a wrapped load.
+        const bool border_tma = use_tma && ctx_->cfg.stencil_border_tma && W >= (uint64_t)SW && H >= (uint64_t)SH;
+        os << "    if (" << (border_tma ? "true" : "interior")
+           << ") {\n      if (threadIdx.x == 0) chai_k::mbar_init(&tbar, 1);\n      __syncthreads();\n"
               "      if (threadIdx.x == 0) {\n        chai_k::mbar_expect_tx(&tbar, " << tile_bytes << "u);\n";
         for (size_t k = 0; k < srcs.size(); k++) {
             const Node& a = nodes_[srcs[k]];
             os << "        chai_k::tma_load_3d(tile" << k << ", &tm" << k << ", &tbar, (int)(tx0 - " << ST_PX
                << "), (int)(ty0 - " << R << "), slot % " << a.slots << ");\n";
         }
-        os << "      }\n      tile_ok = chai_k::mbar_wait_bounded(&tbar, 0, status);\n    } else {\n";
+        os << "      }\n      tile_ok = chai_k::mbar_wait_bounded(&tbar, 0, status);\n";
+        os << (border_tma ? "    }\n    if (!interior && tile_ok) {\n" : "    } else {\n");
         for (size_t k = 0; k < srcs.size(); k++) {
             const Node& a = nodes_[srcs[k]];
             const long long sl = a.slots > 1 ? (long long)(a.W * a.H) : 0;
@@ -439,7 +447,11 @@ int Translator::emit_group(const std::vector<int>& roots)
             for (auto& kv : sten)
                 if (kv.second.src == srcs[k]) { gsrc = kv.first; break; }
             os << "      for (int idx = threadIdx.x; idx < " << SH * SW << "; idx += 256) { const int r = idx / " << SW
-               << ", c = idx - r * " << SW << "; tile" << k << "[idx] = g" << gsrc << "[(long long)(slot % "
+               << ", c = idx - r * " << SW << "; ";
+            if (border_tma)
+                os << "const long long y = ty0 - " << R << " + r, x = tx0 - " << ST_PX
+                   << " + c; if (y >= 0 && y < H && x >= 0 && x < W) continue; ";
+            os << "tile" << k << "[idx] = g" << gsrc << "[(long long)(slot % "
                << a.slots << ") * " << sl << " + chai_k::wrapn(ty0 - " << R << " + r, H) * W + chai_k::wrapn(tx0 - "
                << ST_PX << " + c, W)]; }\n";
         }
@@ -525,12 +537,15 @@ int Translator::emit_group(const std::vector<int>& roots)
                 // fuses a packed mul.rn.f32x2 feeding a packed add / sub into a packed
                 // FMA (one rounding instead of two), which would change results;
                 // scalar mul.rn.f32 results feeding packed add / sub are not fused.
-                // Flat kernels only: a stencil's operands come from windows shifted
-                // by the gather's column offset, whose pairs straddle register
-                // pairs, and the moves that re-pair them cost what packing saves.
-                if (ctx_->cfg.pack_f32 && !mode2d && ar == 2 && nd.prec == CHAI_F32 && (nd.op == 11 || nd.op == 14) &&
-                    nodes_[nd.kids[0]].prec == CHAI_F32 && nodes_[nd.kids[1]].prec == CHAI_F32) {
-                    os << "    f2x4<" << nd.op << ">(v" << nd.kids[0] << ", v" << nd.kids[1] << ", v" << i << ");\n";
+                // In a stencil the operands of a gather whose column offset is odd
+                // relative to its window straddle register pairs and are re-paired
+                // by moves (PackF32Stencil).
+                if (ctx_->cfg.pack_f32 && (!mode2d || ctx_->cfg.pack_f32_stencil) && ar == 2 &&
+                    nd.prec == CHAI_F32 && (nd.op == 11 || nd.op == 14) && nodes_[nd.kids[0]].prec == CHAI_F32 &&
+                    nodes_[nd.kids[1]].prec == CHAI_F32) {
+                    for (int q = 0; q < NV / 4; q++)
+                        os << "    f2x4<" << nd.op << ">(v" << nd.kids[0] << " + " << 4 * q << ", v" << nd.kids[1]
+                           << " + " << 4 * q << ", v" << i << " + " << 4 * q << ");\n";
                     break;
                 }
                 // operand precision: widest operand (fp-only ops at least f32);

@@ -1,8 +1,10 @@
 """Stencil tiles on images of many tiles: interior tiles staged by TMA,
-border tiles by wrapped loads (the periodic wrap of interp/InterpGather.hpp:
-31-44 without a division for coordinates within one period), ragged last
-tile rows and columns, f64 and two-source stencils, for several tile heights
-and register limits.  Bit-exact against the oracle's Kirsch and numpy rolls."""
+border tiles by TMA with the elements outside the image replaced by wrapped
+loads (or, StencilBorderTma=0, entirely by wrapped loads: the periodic wrap
+of interp/InterpGather.hpp:31-44 without a division for coordinates within
+one period), ragged last tile rows and columns, f64 and two-source stencils,
+for several tile heights, register limits and packing options.  Bit-exact
+against the oracle's Kirsch and numpy rolls."""
 import ctypes as C
 
 import numpy as np
@@ -14,7 +16,8 @@ from chai_b200 import _lib as L
 pytestmark = pytest.mark.gpu
 f32 = np.float32
 
-CONFIGS = ["", "StencilRows=16", "StencilRows=8", "StencilRows=64", "StencilMinBlocks=5", "PackF32=0"]
+CONFIGS = ["", "StencilRows=16", "StencilRows=8", "StencilRows=64", "StencilMinBlocks=5", "PackF32=0",
+           "PackF32Stencil=1", "StencilBorderTma=0", "StencilBorderTma=0 StencilRows=16"]
 
 
 def _eval_on(ch, dev, imgs, expr):

@@ -95,6 +95,9 @@ def test_kirsch_trace_is_one_kernel_with_gathers():
     assert src.count("isinf(") == 1 and src.count("f2<13, float>") == 10   # 3 * total, fast, 8 slow
     st0, src0 = source(stmts, [(K.var, 4, 64, 64, 1, 0, 8)], "FuseMaxAffine=0")
     assert st0 == 0 and "isinf(" not in src0
+    # a 64 x 64 image is smaller than one staged tile: its border tiles are
+    # wrapped loads only
+    assert "if (!interior && tile_ok)" not in src
     # two rows x 4 columns per thread: 4 row windows (offsets -1 .. +2) serve both rows
     st2, src2 = source(stmts, [(K.var, 4, 64, 64, 1, 0, 8)], "StencilRowsPerThread=2")
     assert st2 == 0 and src2.count("const float* rowp = tile0") == 4 and src2.count("chai_k::lds_vec(rowp") == 4
@@ -226,3 +229,23 @@ def test_malformed_trace_is_invalid():
     stmts = [(1, 1, [ch._op(11)])]
     st, _ = source(stmts)
     assert st == -1
+
+
+def test_border_tiles_staged_by_tma_with_wrapped_patches():
+    """On an image of at least one staged tile, border tiles take the same TMA
+    load as interior ones (zero fill outside the image) and then replace only
+    the elements outside the image by wrapped loads; StencilBorderTma=0 keeps
+    the all-wrapped staging."""
+    from tests.test_gpu_trace import kirsch_expr
+    W = H = 512
+
+    def build():
+        A = ch._ARR[4](_raw=([ch._bc(L.BC_MEMORY, buffer=7), ch._sc(1), ch._sc(H), ch._sc(W), ch._op(66)], W, H, 1))
+        return A, ch.Arrayf32(kirsch_expr(ch, A, W, H))
+    stmts, (A, K) = record(build)
+    st, src = source(stmts, [(K.var, 4, W, H, 1, 0, 8)])
+    assert st == 0, src
+    assert src.count("tma_load_3d(tile0") == 1 and "if (!interior && tile_ok)" in src
+    assert "if (y >= 0 && y < H && x >= 0 && x < W) continue;" in src
+    st0, src0 = source(stmts, [(K.var, 4, W, H, 1, 0, 8)], "StencilBorderTma=0")
+    assert st0 == 0 and "if (!interior && tile_ok)" not in src0 and "if (interior) {" in src0
