@@ -458,9 +458,46 @@ def run_c1(args, L, ctx, stream):
     dev = ch.Device(config=" ".join(x for x in (args.config, "PlanGraph=1") if x))
     try:
         L.check(L.lib().chai_cuda_set_stream(dev.ctx, C.c_void_p(stream.cuda_stream)), dev.ctx)
-        return _run_c1(args, L, ch, dev, n, stream)
+        out = _run_c1(args, L, ch, dev, n, stream)
     finally:
         dev.close()
+    out["roofline"] = _c1_gemm_roofline(L, ch, ctx, n)
+    return out
+
+
+def _c1_gemm_roofline(L, ch, ctx, n):
+    """The C1 line's roofline: its dominant kernel, the bf16x3 tcgen05 GEMM of
+    the 512^3 product, timed with CUDA events on the bench's main context
+    (kernel timing on) over a few evaluations of the same trace.  Tensor work:
+    three bf16 products, 3 x 2 n^3.  At this size the GEMM is latency-bound,
+    so the fraction is small by construction; the line's time is the six
+    dependent launches of one evaluation."""
+    import torch
+    try:
+        stmts, s_arr = record(ch, lambda: ch.Arrayf32(c1_expr(ch, ch.RNGf32(ch.RNG_PHILOX, 0))))
+        desc, keep = ch.build_desc(stmts)
+        barr = (L.chai_buffer_binding * 1)(L.chai_buffer_binding(s_arr.var, 4, 1, 1, 1, 0, 77202))
+        for _ in range(3):
+            L.check(L.lib().chai_cuda_evaluate(ctx, C.byref(desc), barr, 1), ctx)
+        torch.cuda.synchronize()
+        kstats(L, ctx, "gemm_tc")
+        for _ in range(10):
+            L.check(L.lib().chai_cuda_evaluate(ctx, C.byref(desc), barr, 1), ctx)
+        torch.cuda.synchronize()
+        g_ms, g_n = kstats(L, ctx, "gemm_tc")
+        L.lib().chai_cuda_release(ctx, 77202)
+        if not g_n:
+            return None
+        P, kind = peaks()
+        kern_ms = g_ms / g_n
+        flops = 3 * 2.0 * n ** 3
+        ach = flops / (kern_ms * 1e-3) / 1e12
+        return {"bound": "tensor", "achieved": ach, "peak": P["bf16_tflops"], "unit": "TFLOP/s",
+                "frac": ach / P["bf16_tflops"], "traffic": None, "peak_source": "%s (bf16 dense, burst)" % kind,
+                "kernel": "chai_gemm_tc_kernel (bf16x3, 512^3)", "kernel_ms": kern_ms, "algorithmic_flops": flops,
+                "note": "latency-bound: 32 one-CTA 128x64 tiles, 8 K chunks each"}
+    except Exception:
+        return None
 
 
 def _run_c1(args, L, ch, dev, n, stream):
