@@ -171,6 +171,8 @@ void parse_config(chai::Config& c, const char* text)
             c.gemm_pair = v != "0" && v != "off";
         } else if (k == "GemmPairSeg") {
             c.gemm_pair_seg = std::max(1, atoi(v.c_str()));
+        } else if (k == "GemmSplitK") {
+            c.gemm_split_k = v != "0" && v != "off";
         } else if (k == "GemmStages") {
             c.gemm_stages = std::max(0, atoi(v.c_str()));
         } else if (k == "GroupedPair") {

@@ -274,6 +274,10 @@ struct TileGrid {
     // kernel): CTA 0's producer posts chunk `stall`'s expected bytes but
     // issues no copy, so the MMA's bounded wait on it runs out (-1: off)
     int stall = -1;
+    // K split (one-CTA kernel, batch 1): the batch index of a tile is its
+    // split, which covers K chunks [split * kchunks_split, +kchunks_split)
+    // and stores its partial product in slab `split` of the epilogue output
+    int ksplit = 1, kchunks_split = 0;
 };
 
 // Split precisions store each distinct bf16 plane once per row, side by side
@@ -440,15 +444,17 @@ chai_gemm_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_cons
                         issued = it + 1;
                         continue;
                     }
-                    int xa = kb * kx_mul, xb = xa;
+                    const int c0 = tg.ksplit > 1 ? ti.tb * tg.kchunks_split : 0;   // first K chunk of the split
+                    const int zb = tg.ksplit > 1 ? 0 : ti.tb;                       // operand batch
+                    int xa = (kb + c0) * kx_mul, xb = xa;
                     if (SPLIT || split_s > 1) {
-                        const int blk = kb % split_s, chunk = kb / split_s;
+                        const int blk = kb % split_s, chunk = kb / split_s + c0;
                         const int sel = split_s == 3 ? 1 : 2;
                         xa = kSelA[sel][blk] * tg.plane_k + chunk * kx_mul;
                         xb = kSelB[sel][blk] * tg.plane_k + chunk * kx_mul;
                     }
-                    tma_load_3d(smem_u32(sa + s * A_STAGE), &map_a, fb, xa, ti.arow, ti.tb);
-                    tma_load_3d(smem_u32(sb + s * B_STAGE), &map_b, fb, xb, ti.brow, ti.tb);
+                    tma_load_3d(smem_u32(sa + s * A_STAGE), &map_a, fb, xa, ti.arow, zb);
+                    tma_load_3d(smem_u32(sb + s * B_STAGE), &map_b, fb, xb, ti.brow, zb);
                     issued = it + 1;
                 }
             }
@@ -1095,6 +1101,20 @@ __global__ void __launch_bounds__(256) split_both_bf16(const float* __restrict__
 }
 
 // f32 rows padded to kpad (tf32 operands), optionally transposing
+// K-split partials of a small one-CTA GEMM (ksplit slabs of m x n): C =
+// alpha * (P_0 + P_1 + ...) (+ beta * C), the slabs added in split order
+__global__ void __launch_bounds__(256) splitk_sum(const float* __restrict__ p, int ksplit, int m, int n,
+                                                  float* __restrict__ c, long long ldc, float alpha, float beta)
+{
+    const int col = blockIdx.x * 256 + threadIdx.x, row = blockIdx.y;
+    if (col >= n || row >= m) return;
+    const long long mn = (long long)m * n, i = (long long)row * n + col;
+    float v = p[i];
+    for (int s = 1; s < ksplit; s++) v += p[s * mn + i];
+    float* out = c + (long long)row * ldc + col;
+    *out = beta != 0.0f ? alpha * v + beta * *out : alpha * v;
+}
+
 __global__ void pad_rows_f32(const float* __restrict__ x, long long ld, long long sx, int rows, int k, int kpad,
                              float* __restrict__ out, long long so)
 {
@@ -2502,9 +2522,16 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     const size_t b_off = (a_bytes + 1023) & ~size_t(1023);
     const size_t s_off = (b_off + b_bytes + 255) & ~size_t(255);
     const size_t s_bytes = fp8 ? (size_t)batch * (tiles_m128 + nb128) * 4 : 0;
-    int st = ensure_scratch(ctx, s_off + s_bytes + 1024);
+    // a trace's small matmul may split K over SMs the tiles leave idle: room
+    // for up to four m x n partial slabs after the planes
+    const bool may_split = ctx->trace_gemm && ctx->cfg.gemm_split_k && !cfg_in && !b_planes && batch == 1 &&
+                           !fp8 && M * N <= (1ll << 22);
+    const size_t w_off = (s_off + s_bytes + 255) & ~size_t(255);
+    const size_t w_bytes = may_split ? (size_t)4 * M * N * sizeof(float) : 0;
+    int st = ensure_scratch(ctx, w_off + w_bytes + 1024);
     if (st) return st;
     char* base = static_cast<char*>(ctx->scratch);
+    float* ws = reinterpret_cast<float*>(base + w_off);
     void* Ap = base;
     void* Bp = b_planes && !fp8 && batch == 1 ? const_cast<void*>(b_planes) : base + b_off;
     const bool b_ready = Bp == b_planes;
@@ -2611,16 +2638,44 @@ int launch_gemm_tc_cfg(chai_cuda_ctx* ctx, const chai_gemm_desc* d, int precisio
     tg.group_m = cfg.group_m;
     if (kblocks >= 2 && fault_injected("gemm_stall")) tg.stall = 1;
     tg.plane_k = (int)kpad;
+    // K split (a trace's small matmul): while the tiles fill at most half of
+    // the SMs, double the splits (up to 4) as long as each keeps >= 2 K
+    // chunks; each split's tile stores its partial in a slab of the scratch
+    // and splitk_sum adds the slabs in split order
+    int ksplit = 1, kb_launch = kblocks;
+    EpiArgs epl = ep;
+    if (may_split) {
+        const int kchunks_all = (int)(kpad / kblk);
+        const long long nt = (long long)tg.tiles_m * tg.tiles_n;
+        while (ksplit < 4 && nt * (ksplit * 2) <= ctx->sm_count && kchunks_all % (ksplit * 2) == 0 &&
+               kchunks_all / (ksplit * 2) >= 2)
+            ksplit *= 2;
+        if (ksplit > 1) {
+            tg.batch = ksplit;
+            tg.ksplit = ksplit;
+            tg.kchunks_split = kchunks_all / ksplit;
+            kb_launch = kblocks / ksplit;
+            epl.c = ws;
+            epl.ldc = N;
+            epl.stride_c = M * N;
+            epl.alpha = 1.0f;
+            epl.beta = 0.0f;
+            epl.vec_ok = N % 4 == 0 ? 1 : 0;
+        }
+    }
     const long long ntiles = (long long)tg.tiles_m * tg.tiles_n * tg.batch;
     if (ntiles > (1ll << 30)) return set_error(ctx, CHAI_ERR_UNSUPPORTED, "tc gemm: too many tiles");
     const unsigned grid = (unsigned)std::min<long long>(ntiles, ctx->sm_count);
     cudaEvent_t ev[2];
     ktime_begin(ctx, "gemm_tc", ev);
-    if (tf32) st = launch_variant<KIND_TF32, false, false>(ctx, cfg, grid, ma, mb, kblocks, S, tg, ep, nullptr, 0);
-    else if (fp8) st = launch_variant<KIND_FP8, false, false>(ctx, cfg, grid, ma, mb, kblocks, S, tg, ep, nullptr, 0);
-    else if (S == 1) st = launch_variant<KIND_BF16, false, false>(ctx, cfg, grid, ma, mb, kblocks, S, tg, ep, nullptr, 0);
-    else st = launch_variant<KIND_BF16, true, false>(ctx, cfg, grid, ma, mb, kblocks, S, tg, ep, nullptr, 0);
+    if (tf32) st = launch_variant<KIND_TF32, false, false>(ctx, cfg, grid, ma, mb, kb_launch, S, tg, epl, nullptr, 0);
+    else if (fp8) st = launch_variant<KIND_FP8, false, false>(ctx, cfg, grid, ma, mb, kb_launch, S, tg, epl, nullptr, 0);
+    else if (S == 1) st = launch_variant<KIND_BF16, false, false>(ctx, cfg, grid, ma, mb, kb_launch, S, tg, epl, nullptr, 0);
+    else st = launch_variant<KIND_BF16, true, false>(ctx, cfg, grid, ma, mb, kb_launch, S, tg, epl, nullptr, 0);
     if (st) return st;
+    if (ksplit > 1)
+        splitk_sum<<<dim3((unsigned)((N + 255) / 256), (unsigned)M), 256, 0, s>>>(ws, ksplit, (int)M, (int)N,
+                                                                                  ep.c, ep.ldc, ep.alpha, ep.beta);
     ktime_end(ctx, "gemm_tc", ev);
     CHAI_CUDA_TRY(ctx, cudaGetLastError());
     return CHAI_OK;

@@ -43,6 +43,7 @@ struct Config {
     bool gemm_pair = true;                   // 256-row GEMM tiles on CTA pairs (cta_group::2) where configured
     int gemm_pair_seg = 64;                  // pair kernel, split precisions: K chunks per promotion segment
     int gemm_stages = 0;                     // GEMM pipeline stages (0: tuned or default)
+    bool gemm_split_k = true;                // traced small GEMMs split K over otherwise idle SMs
     bool pack_f32 = true;                    // element kernels issue f32 add / sub as packed f32x2 pairs
     bool pack_f32_stencil = false;           // ... stencil kernels too (slower: re-pairing moves, registers)
     bool stencil_border_tma = true;          // border stencil tiles staged by TMA + wrapped patch loads
@@ -94,6 +95,7 @@ struct chai_cuda_ctx {
     std::unordered_map<uint64_t, PlanGraph> graphs;
     uint64_t graph_launches = 0;
     bool capturing = false;                                 // a plan replay is being captured
+    bool trace_gemm = false;                                // the GEMM being launched is a trace's matmul
     std::mutex capture_mutex;                               // no client-thread stream work during a capture
     // grouped GEMM with the in-kernel split: the device tile records of the
     // last call, reused while the problem array repeats

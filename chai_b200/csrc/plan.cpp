@@ -271,7 +271,11 @@ int Translator::run_step(const Step& s)
             d.a = ptr_of(s.a);
             d.b = ptr_of(s.b);
             d.c = ptr_of(s.c);
-            return launch_gemm(ctx_, &d);
+            // a trace's matmul: a small one may split K (GemmSplitK)
+            ctx_->trace_gemm = true;
+            const int st = launch_gemm(ctx_, &d);
+            ctx_->trace_gemm = false;
+            return st;
         }
         case Step::GEMV:
             return launch_gemv(ctx_, s.prec, s.trans, s.m, s.n, s.alpha, ptr_of(s.a), s.lda, ptr_of(s.b), s.beta,
