@@ -351,3 +351,31 @@ def test_local_offsets_follow_the_declared_element_sizes():
     stmts, kernels, _ = record_with_kernels(build_s)
     st, src = source(stmts, kernels)
     assert st != 0 and "unknown size" in src
+
+
+def test_vector_rewrite_edge_cases_compile():
+    """Swizzles through '->' and on array elements, upper-case hex
+    components, scalar convert_ / as_ names, a literal as a call argument,
+    vector compound assignment and comparisons feeding select()."""
+    text = """
+    typedef struct { float4 p; int n; } item;
+    __kernel void edge(__global item* it, __global float* out, __global uint* u)
+    {
+        const size_t i = get_global_id(0);
+        __global item* q = it + i;
+        float4 v = q->p;
+        q->p.xy = v.zw;
+        float2 w = (&it[i])->p.SAB;
+        v *= (float4)(2.0f);
+        v.hi -= w;
+        int4 m = isgreater(v, (float4)(0.0f)) & (v != v.wzyx);
+        u[i] = as_uint(out[i]) ^ convert_uint_sat(-1.5f) ^ (uint)convert_int_rtn(v.x);
+        out[i] = dot(select((float4)(0.0f), v, m), (float4)(1.0f, 0.5f, 0.25f, 0.125f));
+    }"""
+    st, src = compile_call(text, "edge", [(L.F32, 256, 1), (L.F32, 64, 1), (L.U32, 64, 1)])
+    assert st == 0, src[-3000:]
+    body = src.split("// ---- program text")[-1]
+    assert "q->p.chai_swl<0,1>() = v.chai_swr<2,3>();" in body
+    assert "->p.chai_swr<10,11>();" in body
+    assert "v.chai_hi_l() -= w;" in body
+    assert "chai_cl::as_type<unsigned int>(out[i])" in body and "chai_cl::convert<unsigned int, 1, 1, 0>(-1.5f)" in body
