@@ -644,15 +644,40 @@ def _cl_vector_bytes(tok):
     return _CL_BYTES[m.group(1)] * (4 if n == 3 else n)
 
 
+def _cl_kernel_heads(text):
+    """(name, parameter text) of every `__kernel void NAME(...)`; attributes
+    between `__kernel` and `void` are skipped, as api/ProgramCL.cpp:156-177
+    skips every token up to `void`."""
+    import re
+    out = []
+    for m in re.finditer(r"\b(?:__kernel|kernel)\b", text):
+        i = m.end()
+        while True:
+            while i < len(text) and text[i].isspace():
+                i += 1
+            if not text.startswith("__attribute__", i):
+                break
+            j = text.find("(", i)
+            if j < 0:
+                return out
+            depth = 0
+            for k in range(j, len(text)):
+                depth += {"(": 1, ")": -1}.get(text[k], 0)
+                if depth == 0:
+                    break
+            i = k + 1
+        h = re.match(r"void\s+(\w+)\s*\(([^)]*)\)", text[i:])
+        if h:
+            out.append((h.group(1), h.group(2)))
+    return out
+
+
 def _cl_vector_params(text):
     """Per kernel, for each parameter: the element bytes of a vector-typed
     parameter (0 for the others)."""
-    import re
-    out = {}
-    for m in re.finditer(r"\b(?:__kernel|kernel)\s+void\s+(\w+)\s*\(([^)]*)\)", text):
-        out[m.group(1)] = [_max([_cl_vector_bytes(t) for t in p.replace("*", " ").split()] or [0])
-                           for p in m.group(2).split(",") if p.split()]
-    return out
+    return {name: [_max([_cl_vector_bytes(t) for t in p.replace("*", " ").split()] or [0])
+                   for p in params.split(",") if p.split()]
+            for name, params in _cl_kernel_heads(text)}
 
 
 def _cl_signatures(text):
@@ -661,11 +686,10 @@ def _cl_signatures(text):
     image2d_t parameters are arrays, __local / local ones local memory, the
     rest scalars; the precision is the parameter's uint / unsigned / int /
     float / double keyword."""
-    import re
     sigs = {}
-    for m in re.finditer(r"\b(?:__kernel|kernel)\s+void\s+(\w+)\s*\(([^)]*)\)", text):
+    for name, params in _cl_kernel_heads(text):
         args = []
-        for p in m.group(2).split(","):
+        for p in params.split(","):
             toks = p.replace("*", " ").split()
             if not toks:
                 continue
@@ -677,7 +701,7 @@ def _cl_signatures(text):
                 kind = L.KARG_SCALAR
             prec = next((_CL_SCALARS[t] for t in toks if t in _CL_SCALARS), -1)
             args.append((kind, prec))
-        sigs[m.group(1)] = args
+        sigs[name] = args
     return sigs
 
 

@@ -1094,6 +1094,32 @@ int opencl_to_cuda(const std::string& src, const std::string& name, const std::v
                 return k < t.size() ? (int)k : -1;
             };
             int kv = next_ident(j);
+            // __attribute__((...)) between __kernel and void (dropped), as the
+            // reference's parser skips every token up to "void"
+            // (api/ProgramCL.cpp:156-177)
+            while (kv >= 0 && t[kv].text == "__attribute__") {
+                size_t q = (size_t)kv + 1;
+                int depth = 0;
+                bool opened = false, closed = false;
+                for (; q < t.size() && !closed; q++) {
+                    if (t[q].kind != Tok::OTHER) continue;
+                    const std::string& x = t[q].text;
+                    for (size_t c = 0; c < x.size(); c++) {
+                        if (x[c] == '(') { depth++; opened = true; }
+                        if (x[c] == ')' && --depth == 0 && opened) {
+                            if (x.find_first_not_of(" \t\r\n", c + 1) != std::string::npos) {
+                                err = "inline kernel: unexpected text after __attribute__";
+                                return -1;
+                            }
+                            closed = true;
+                            break;
+                        }
+                    }
+                }
+                if (!closed) { err = "inline kernel: unbalanced __attribute__"; return -1; }
+                j = q;
+                kv = next_ident(j);
+            }
             if (kv < 0 || t[kv].text != "void") { err = "inline kernel: expected void after __kernel"; return -1; }
             j = (size_t)kv + 1;
             int kn = next_ident(j);

@@ -379,3 +379,18 @@ def test_vector_rewrite_edge_cases_compile():
     assert "->p.chai_swr<10,11>();" in body
     assert "v.chai_hi_l() -= w;" in body
     assert "chai_cl::as_type<unsigned int>(out[i])" in body and "chai_cl::convert<unsigned int, 1, 1, 0>(-1.5f)" in body
+
+
+def test_attributes_between_kernel_and_void():
+    """`__kernel __attribute__((...)) void name(...)`: the reference's parser
+    skips every token up to `void` (api/ProgramCL.cpp:156-177); the attribute
+    is dropped from the CUDA text."""
+    text = """
+    __kernel __attribute__((reqd_work_group_size(64, 1, 1))) void scale(__global float* a, float s)
+    { a[get_global_id(0)] *= s; }"""
+    prog = ch.ProgramCL(text)
+    assert prog._sigs["scale"] == [(L.KARG_ARRAY, L.F32), (L.KARG_SCALAR, L.F32)]
+    st, src = compile_call(text, "scale", [(L.F32, 64, 1)], (f32(2.0),))
+    assert st == 0, src[-2000:]
+    assert "__attribute__" not in src.split("// ---- program text")[-1]
+    assert 'extern "C" __global__ void scale(' in src
