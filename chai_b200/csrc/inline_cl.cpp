@@ -782,6 +782,57 @@ template <class T> __device__ __forceinline__ void vstore##N(const chai_cl::vec<
 }
 CHAI_CL_VLOAD(2) CHAI_CL_VLOAD(3) CHAI_CL_VLOAD(4) CHAI_CL_VLOAD(8) CHAI_CL_VLOAD(16)
 #undef CHAI_CL_VLOAD
+// ---- half as a storage format (OpenCL 1.2 without cl_khr_fp16): vload_half*
+// widen IEEE binary16 to float, vstore_half* round float / double to it
+// (_rte the default, _rtz, _rtp, _rtn) with the PTX conversions
+namespace chai_cl {
+struct half_t { unsigned short bits; };
+__device__ __forceinline__ float h2f(unsigned short h) { float f; asm("cvt.f32.f16 %0, %1;" : "=f"(f) : "h"(h)); return f; }
+template <int M> __device__ __forceinline__ unsigned short f2h(float f)
+{
+    unsigned short h;
+    if (M == 2) asm("cvt.rz.f16.f32 %0, %1;" : "=h"(h) : "f"(f));
+    else if (M == 3) asm("cvt.rp.f16.f32 %0, %1;" : "=h"(h) : "f"(f));
+    else if (M == 4) asm("cvt.rm.f16.f32 %0, %1;" : "=h"(h) : "f"(f));
+    else asm("cvt.rn.f16.f32 %0, %1;" : "=h"(h) : "f"(f));
+    return h;
+}
+template <int M> __device__ __forceinline__ unsigned short f2h(double f)
+{
+    unsigned short h;
+    if (M == 2) asm("cvt.rz.f16.f64 %0, %1;" : "=h"(h) : "d"(f));
+    else if (M == 3) asm("cvt.rp.f16.f64 %0, %1;" : "=h"(h) : "d"(f));
+    else if (M == 4) asm("cvt.rm.f16.f64 %0, %1;" : "=h"(h) : "d"(f));
+    else asm("cvt.rn.f16.f64 %0, %1;" : "=h"(h) : "d"(f));
+    return h;
+}
+}  // namespace chai_cl
+typedef chai_cl::half_t half;
+__device__ __forceinline__ float vload_half(size_t i, const half* p) { return chai_cl::h2f(p[i].bits); }
+#define CHAI_CL_VLOAD_HALF(N, A)                                                                         \
+__device__ __forceinline__ chai_cl::vec<float, N> vload##A##_half##N(size_t i, const half* p)            \
+{ chai_cl::vec<float, N> r; _Pragma("unroll") for (int k = 0; k < N; k++) r.c(k) = chai_cl::h2f(p[i * (N == 3 && #A[0] ? 4 : N) + k].bits); return r; }
+CHAI_CL_VLOAD_HALF(2, ) CHAI_CL_VLOAD_HALF(3, ) CHAI_CL_VLOAD_HALF(4, ) CHAI_CL_VLOAD_HALF(8, ) CHAI_CL_VLOAD_HALF(16, )
+CHAI_CL_VLOAD_HALF(2, a) CHAI_CL_VLOAD_HALF(3, a) CHAI_CL_VLOAD_HALF(4, a) CHAI_CL_VLOAD_HALF(8, a) CHAI_CL_VLOAD_HALF(16, a)
+#undef CHAI_CL_VLOAD_HALF
+#define CHAI_CL_VSTORE_HALF1(SUF, M)                                                                     \
+__device__ __forceinline__ void vstore_half##SUF(float d, size_t i, half* p) { p[i].bits = chai_cl::f2h<M>(d); } \
+__device__ __forceinline__ void vstore_half##SUF(double d, size_t i, half* p) { p[i].bits = chai_cl::f2h<M>(d); }
+CHAI_CL_VSTORE_HALF1(, 1) CHAI_CL_VSTORE_HALF1(_rte, 1) CHAI_CL_VSTORE_HALF1(_rtz, 2) CHAI_CL_VSTORE_HALF1(_rtp, 3)
+CHAI_CL_VSTORE_HALF1(_rtn, 4)
+#undef CHAI_CL_VSTORE_HALF1
+#define CHAI_CL_VSTORE_HALFN(N, A, SUF, M)                                                              \
+template <class T> __device__ __forceinline__ void vstore##A##_half##N##SUF(const chai_cl::vec<T, N>& v, size_t i, half* p) \
+{ _Pragma("unroll") for (int k = 0; k < N; k++) p[i * (N == 3 && #A[0] ? 4 : N) + k].bits = chai_cl::f2h<M>(v.c(k)); }
+#define CHAI_CL_VSTORE_HALF_MODES(N, A)                                                                  \
+CHAI_CL_VSTORE_HALFN(N, A, , 1) CHAI_CL_VSTORE_HALFN(N, A, _rte, 1) CHAI_CL_VSTORE_HALFN(N, A, _rtz, 2)   \
+CHAI_CL_VSTORE_HALFN(N, A, _rtp, 3) CHAI_CL_VSTORE_HALFN(N, A, _rtn, 4)
+CHAI_CL_VSTORE_HALF_MODES(2, ) CHAI_CL_VSTORE_HALF_MODES(3, ) CHAI_CL_VSTORE_HALF_MODES(4, )
+CHAI_CL_VSTORE_HALF_MODES(8, ) CHAI_CL_VSTORE_HALF_MODES(16, )
+CHAI_CL_VSTORE_HALF_MODES(2, a) CHAI_CL_VSTORE_HALF_MODES(3, a) CHAI_CL_VSTORE_HALF_MODES(4, a)
+CHAI_CL_VSTORE_HALF_MODES(8, a) CHAI_CL_VSTORE_HALF_MODES(16, a)
+#undef CHAI_CL_VSTORE_HALF_MODES
+#undef CHAI_CL_VSTORE_HALFN
 // ---- program text
 )cl";
 

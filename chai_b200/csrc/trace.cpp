@@ -225,8 +225,28 @@ int Translator::parse(const chai_stmt& s, int& pos)
             v.kind = Node::VAR;
             v.var = kd.args[a].variable;
             v.ver = kd.args[a].version;
-            const int k = resolve_var(v);
+            int k = resolve_var(v);
             if (k < 0) return -1;
+            // the kernel updates this argument in place: when its value is
+            // also another variable's (equal expressions share one node) or
+            // another argument of this kernel, the argument gets a private
+            // copy, so that only this variable sees the update -- as every
+            // chai array has memory of its own in the reference
+            bool shared = std::find(n.kids.begin(), n.kids.end(), k) != n.kids.end();
+            for (const auto& kv : assigned_)
+                if (!shared && kv.second == k && kv.first.first != v.var) shared = true;
+            for (const auto& kv : inputs_)
+                if (!shared && kv.second == k && kv.first != v.var) shared = true;
+            if (shared) {
+                Node c;
+                c.kind = Node::CONVERT;           // same precision: a copy
+                c.prec = nodes_[k].prec;
+                c.W = nodes_[k].W; c.H = nodes_[k].H; c.slots = nodes_[k].slots;
+                c.kids = {k};
+                c.var = v.var;                    // one copy per (variable, version)
+                c.ver = v.ver;
+                k = add(c);
+            }
             n.kids.push_back(k);
         }
         return add(n);

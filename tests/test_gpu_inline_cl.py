@@ -127,3 +127,19 @@ def test_inline_kernel_trace_replays(ch, chai_dev):
     n1 = C.c_uint64()
     L.check(L.lib().chai_cuda_kernel_stats(chai_dev.ctx, b"plan_replay", None, C.byref(n1), 0), chai_dev.ctx)
     assert n1.value - n0.value == 2
+
+
+def test_kernel_arguments_equal_to_other_variables_get_their_own_storage(ch):
+    """Two arrays made by the same expression (one node after deduplication)
+    stay two arrays when a kernel updates them: each argument, and every
+    other variable of that value, keeps its own contents."""
+    n = 128
+    prog = ch.ProgramCL("""
+    __kernel void two(__global float* a, __global float* b) { const size_t i = get_global_id(0); a[i] = 1.0f; b[i] = 2.0f; }
+    __kernel void one(__global float* a) { a[get_global_id(0)] = 5.0f; }""")
+    A, B = ch.Arrayf32(ch.zeros_f32(n)), ch.Arrayf32(ch.zeros_f32(n))
+    prog("two", A, B)(n, 64)
+    assert np.array_equal(A.read1(), np.full(n, 1, f32)) and np.array_equal(B.read1(), np.full(n, 2, f32))
+    C, D = ch.Arrayf32(ch.zeros_f32(n)), ch.Arrayf32(ch.zeros_f32(n))
+    prog("one", C)(n, 64)
+    assert np.array_equal(C.read1(), np.full(n, 5, f32)) and np.array_equal(D.read1(), np.zeros(n, f32))

@@ -283,3 +283,56 @@ def test_image_reads_writes_and_samplers(ch):
     dout = ch.Arrayf64(ch.zeros_f64(2 * iw * 4))
     prog("dimg", ch.make2(d), dout)(iw, 4, 8, 2)
     assert np.array_equal(dout.read1(), d.ravel() * 2.0)
+
+
+HALF = """
+__kernel void halves(__global const float* x, __global half* hn, __global half* hz, __global float* back)
+{
+    const size_t i = get_global_id(0);
+    vstore_half(x[i], i, hn);
+    vstore_half_rtz(x[i], i, hz);
+    back[i] = vload_half(i, hn);
+}
+__kernel void halves4(__global const float* x, __global half* h, __global float* back)
+{
+    const size_t i = get_global_id(0);
+    vstore_half4_rtp(vload4(i, x), i, h);
+    vstore4(vload_half4(i, h), i, back);
+}
+"""
+
+
+def _half_toward(x, direction):
+    """binary16 nearest to x in the given direction (0: toward zero, +1: up)."""
+    h = x.astype(np.float16)
+    hf = h.astype(f32)
+    if direction == 0:
+        fix = np.abs(hf) > np.abs(x)
+        h[fix] = np.nextafter(h[fix], np.float16(0))
+    else:
+        fix = hf < x
+        h[fix] = np.nextafter(h[fix], np.float16(np.inf))
+    return h
+
+
+def test_half_storage_round_trips(ch):
+    n = 256
+    rng = np.random.default_rng(8)
+    x = (rng.uniform(-1, 1, n) * np.logspace(-7, 4.7, n)).astype(f32)      # half subnormals .. 5e4
+    x[:4] = [0.0, -0.0, 1.0 / 3.0, 65504.0]
+    prog = ch.ProgramCL(HALF)
+    X = ch.make1(x)
+    hn, hz = ch.Arrayu32(ch.zeros_u32(n // 2)), ch.Arrayu32(ch.zeros_u32(n // 2))
+    back = ch.Arrayf32(ch.zeros_f32(n))
+    prog("halves", X, hn, hz, back)(n, 64)
+    got_n = hn.read1().view(np.uint16).view(np.float16)
+    got_z = hz.read1().view(np.uint16).view(np.float16)
+    assert np.array_equal(got_n.view(np.uint16), x.astype(np.float16).view(np.uint16))
+    assert np.array_equal(got_z.view(np.uint16), _half_toward(x, 0).view(np.uint16))
+    assert np.array_equal(back.read1(), x.astype(np.float16).astype(f32))
+    h4 = ch.Arrayu32(ch.zeros_u32(n // 2))
+    back4 = ch.Arrayf32(ch.zeros_f32(n))
+    prog("halves4", X, h4, back4)(n // 4, 32)
+    want_p = _half_toward(x, 1)
+    assert np.array_equal(h4.read1().view(np.uint16), want_p.view(np.uint16))
+    assert np.array_equal(back4.read1(), want_p.astype(f32))

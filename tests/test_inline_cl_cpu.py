@@ -394,3 +394,28 @@ def test_attributes_between_kernel_and_void():
     assert st == 0, src[-2000:]
     assert "__attribute__" not in src.split("// ---- program text")[-1]
     assert 'extern "C" __global__ void scale(' in src
+
+
+def test_half_storage_functions_compile():
+    """vload_half* / vstore_half* (all rounding modes, aligned forms, float
+    and double sources) over `half` storage."""
+    text = """
+    __kernel void halves(__global const float* x, __global half* h, __global float* back,
+                         __global const double* d, __global half* hd)
+    {
+        const size_t i = get_global_id(0);
+        vstore_half(x[i], i, h);
+        vstore_half_rtz(x[i], i + 64, h);
+        back[i] = vload_half(i, h) + vload_half(i + 64, h);
+        float4 v = vload4(0, x);
+        vstore_half4_rtp(v, 40, h);
+        vstorea_half3(v.xyz, 20, h);
+        float3 w = vloada_half3(20, h);
+        float8 z = vload_half8(2, h);
+        vstore_half8_rtn(z, 3, h);
+        vstore_half_rte(d[i], i, hd);
+        back[i + 64] = w.x + z.s7 + vload_half2(1, hd).y;
+    }"""
+    st, src = compile_call(text, "halves", [(L.F32, 64, 1), (L.U32, 128, 1), (L.F32, 128, 1), (L.F64, 64, 1),
+                                            (L.U32, 64, 1)])
+    assert st == 0, src[-3000:]
