@@ -419,3 +419,23 @@ def test_half_storage_functions_compile():
     st, src = compile_call(text, "halves", [(L.F32, 64, 1), (L.U32, 128, 1), (L.F32, 128, 1), (L.F64, 64, 1),
                                             (L.U32, 64, 1)])
     assert st == 0, src[-3000:]
+
+
+def test_kernel_head_parser_edge_cases():
+    """Kernel heads as api/ProgramCL.cpp:145-177 finds them: `kernel` or
+    `__kernel`, attributes before `void`, several kernels, and words such as
+    "kernel" in comments or identifiers that head nothing."""
+    text = """
+    // this kernel computes nothing; my_kernel is not a kernel head
+    int my_kernel_helper(int x) { return x; }
+    kernel void a(global float* x) { }
+    __kernel __attribute__((vec_type_hint(float4))) __attribute__((reqd_work_group_size(8, 8, 1)))
+    void b(__global uint* y, __local float2* t, float s) { }
+    """
+    heads = ch._cl_kernel_heads(text)
+    assert [h[0] for h in heads] == ["a", "b"]
+    p = ch.ProgramCL(text)
+    assert p._sigs["a"] == [(L.KARG_ARRAY, L.F32)]
+    # float2 is no scalar keyword of the reference's parser: no precision
+    assert p._sigs["b"] == [(L.KARG_ARRAY, L.U32), (L.KARG_LOCAL, -1), (L.KARG_SCALAR, L.F32)]
+    assert p._vbytes["b"] == [0, 8, 0]
